@@ -1,0 +1,348 @@
+#!/usr/bin/env python3
+"""Benchmark: MO VGL electron-points/s on B200 (config-1 molecule).
+
+One step = one evaluation of AO VGL + MO VGL for every electron point of the
+workload (walkers x electrons), the reference's qmckl_get_mo_basis_mo_vgl.
+
+  value  device-resident throughput: coordinates already in HBM, outputs left
+         in HBM, timed with CUDA events on the evaluation stream, L2 flushed
+         (256 MB write) before every timed step.
+  e2e    the same through the public host API: qmckl_set_electron_coord from
+         pinned host memory + qmckl_get_mo_basis_mo_vgl into pinned host memory
+         (both copies inside the timed region).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--form mixed|fp64]
+  python bench.py --impl reference     # the CPU reference path on host cores
+
+Under torchrun (N > 1) every rank evaluates its own full workload on its own
+GPU (walkers are independent; no collective on the data path): weak scaling,
+value = points of all ranks / max over ranks of the timed region.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MO VGL electron-points/s on 1 B200, mixed vs FP64 form at <=1e-6 rel err"
+WORKLOAD = "config-1 molecule: 80 nuclei (40 C/N/O + 40 H), cc-pVTZ-shaped cartesian basis, 2000 AOs, 160 MOs, 318 electrons x 512 walkers"
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), d.get("bf16_tflops_sustained", 1400.0), "measured"
+    return 6650.0, 1590.0, 1400.0, "fallback"
+
+
+def load_traffic():
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "dram_traffic.txt")
+    out = {}
+    if os.path.exists(p):
+        for line in open(p):
+            line = line.strip()
+            if not line or line.startswith("#"):
+                continue
+            parts = dict(kv.split("=", 1) for kv in line.split() if "=" in kv)
+            if "kernel" in parts and "bytes_per_launch" in parts:
+                out[(parts["kernel"], parts.get("form", ""))] = float(parts["bytes_per_launch"])
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(sysd, seconds=15.0, nthreads=0):
+    """Time the CPU oracle (a restatement of the reference's C HPC path) on a bounded sample."""
+    from oracle import pyoracle as O
+    pts = sysd["elec_coord"].reshape(-1, 3)
+    b = O.Basis(sysd)
+    nthreads = nthreads or os.cpu_count() or 1
+    n = 64
+    done, t_total = 0, 0.0
+    while t_total < seconds and done < pts.shape[0]:
+        chunk = pts[done:done + n]
+        t0 = time.perf_counter()
+        ao = O.ao_vgl(b, chunk, sysd["nucl_coord"], nthreads=nthreads)
+        O.mo_vgl(sysd["mo_coef"], ao, nthreads=nthreads)
+        t_total += time.perf_counter() - t0
+        done += chunk.shape[0]
+        n = min(2 * n, 4096)
+    return {"value": done / t_total, "unit": "electron-points/s", "cores": nthreads, "kind": "port",
+            "sample": f"{done} of {pts.shape[0]} points of the workload, AO VGL + MO VGL, {t_total:.1f} s"}
+
+
+def run_reference(args):
+    import torch.distributed as dist  # noqa: F401  (only for rank detection)
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from qmckl_b200 import gen
+    sysd = gen.config(1)
+    P = sysd["elec_coord"].shape[0] * sysd["elec_coord"].shape[1]
+    vals = []
+    base = None
+    for i in range(args.warmup + args.steps):
+        base = cpu_baseline(sysd, seconds=max(2.0, 20.0 / max(1, args.steps)))
+        if i >= args.warmup:
+            vals.append(base["value"])
+    v = statistics.median(vals)
+    base["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "electron-points/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * P / v, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, qmckl_b200/gen.py)",
+            "config": {"workload": WORKLOAD, "points": P, "form": "reference CPU path"},
+            "cpu_baseline": base,
+            "e2e": {"value": v, "unit": "electron-points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--form", default=os.environ.get("QMCKL_B200_BENCH_FORM", "mixed"), choices=["mixed", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    from qmckl_b200 import gen
+    from qmckl_b200 import qmckl as pq
+    from qmckl_b200.system import make_context
+
+    sysd = gen.config(1)
+    W, E = sysd["elec_coord"].shape[:2]
+    P, A, M = W * E, sysd["ao_num"], sysd["mo_num"]
+    form = pq.FORM_MIXED if args.form == "mixed" else pq.FORM_FP64
+    ctx = make_context(sysd, points=False, form=form)
+    stream = torch.cuda.current_stream()
+    pq.b200_set_stream(ctx, stream.cuda_stream)
+
+    coord_t = np.ascontiguousarray(gen.points(sysd).T)               # [3][P]
+    d_coord = torch.tensor(coord_t, dtype=torch.float64, device="cuda")
+    d_mo = torch.empty(P * 5 * M, dtype=torch.float64, device="cuda")
+    d_ao = torch.empty(P * 5 * A, dtype=torch.float64, device="cuda") if form == pq.FORM_FP64 else None
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        pq.b200_mo_vgl_device(ctx, P, d_coord.data_ptr(), d_mo.data_ptr())
+
+    # accuracy of the timed form against the FP64 form on the same points
+    err = None
+    if form == pq.FORM_MIXED:
+        step()
+        torch.cuda.synchronize()
+        mixed = d_mo.clone()
+        ctx64 = make_context(sysd, points=False, form=pq.FORM_FP64)
+        pq.b200_set_stream(ctx64, stream.cuda_stream)
+        pq.b200_mo_vgl_device(ctx64, P, d_coord.data_ptr(), d_mo.data_ptr())
+        torch.cuda.synchronize()
+        ref = d_mo.view(P, 5, M)
+        diff = (mixed.view(P, 5, M) - ref).abs()
+        err = {"max_abs_over_max_ref": {n: float(diff[:, c, :].max() / ref[:, c, :].abs().max())
+                                         for c, n in enumerate(["value", "grad_x", "grad_y", "grad_z", "laplacian"])},
+               "reference": "FP64 form on the GPU (itself checked against the CPU oracle in tests/)"}
+        pq.context_destroy(ctx64)
+        del mixed, ref, diff
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    launches0 = pq.b200_kernel_launch_count()
+    times = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    launches = pq.b200_kernel_launch_count() - launches0
+    # dominant-kernel timing: the AO kernel alone (same stream, same events)
+    ao_times = []
+    if form == pq.FORM_FP64:
+        for _ in range(max(3, args.steps // 2)):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            pq.b200_ao_vgl_device(ctx, P, d_coord.data_ptr(), d_ao.data_ptr())
+            e1.record(stream)
+            e1.synchronize()
+            ao_times.append(e0.elapsed_time(e1))
+    clocks = sampler.stop()
+    ms = statistics.mean(times)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+
+    # end to end through the public host API (pinned host buffers)
+    h_coord = torch.from_numpy(np.ascontiguousarray(sysd["elec_coord"].reshape(-1))).pin_memory()
+    h_out = torch.empty(P * 5 * M, dtype=torch.float64).pin_memory()
+    ctx_e = make_context(sysd, points=True, form=form)
+    pq.b200_set_stream(ctx_e, stream.cuda_stream)
+    lib = pq.lib()
+    import ctypes as C
+
+    def e2e_step():
+        rc = lib.qmckl_set_electron_coord(C.c_int64(ctx_e), C.c_char(b"N"), C.c_int64(W),
+                                          C.c_void_p(h_coord.data_ptr()), C.c_int64(P * 3))
+        assert rc == 0, pq.last_error(ctx_e)
+        rc = lib.qmckl_get_mo_basis_mo_vgl(C.c_int64(ctx_e), C.c_void_p(h_out.data_ptr()), C.c_int64(P * 5 * M))
+        assert rc == 0, pq.last_error(ctx_e)
+
+    for _ in range(2):
+        e2e_step()
+    e2e_times = []
+    for _ in range(max(3, args.steps // 2)):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        e2e_step()
+        e1.record(stream)
+        e1.synchronize()
+        e2e_times.append(e0.elapsed_time(e1))
+    e2e_ms = statistics.mean(e2e_times)
+    pq.context_destroy(ctx_e)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+
+    hbm, bf16, bf16_sus, peak_src = load_peaks()
+    traffic = load_traffic()
+    if form == pq.FORM_FP64:
+        ao_ms = statistics.mean(ao_times)
+        algo_bytes = 5.0 * P * A * 8 + 24.0 * P      # dense ao_vgl write + coordinates
+        achieved = algo_bytes / (ao_ms * 1e-3) / 1e9
+        roofline = {"kernel": "ao_f64_kernel<5> (AO VGL, FP64)", "bound": "hbm", "achieved": achieved,
+                    "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_source": peak_src,
+                    "traffic": traffic.get(("ao_f64_kernel", "fp64")), "ms_per_launch": ao_ms,
+                    "algorithmic_bytes_per_launch": algo_bytes,
+                    "other_kernel": {"kernel": "dgemm_kernel (MO VGL, FP64 mma.sync m8n8k4)",
+                                     "ms_per_launch": ms - ao_ms,
+                                     "tflops": 2.0 * 5 * P * A * M / ((ms - ao_ms) * 1e-3) / 1e12}}
+    else:
+        flops = 2.0 * 5 * P * A * M
+        pieces = 3
+        executed = flops * (6 if pieces == 3 else 3)
+        achieved = executed / (ms * 1e-3) / 1e12
+        roofline = {"kernel": "split-BF16 tcgen05 MO contraction (whole step)", "bound": "tensor",
+                    "achieved": achieved, "peak": bf16, "unit": "TFLOP/s", "frac": achieved / bf16,
+                    "peak_source": peak_src, "traffic": traffic.get(("mo_tc", "mixed")),
+                    "dense_equivalent_tflops": flops / (ms * 1e-3) / 1e12}
+
+    value = world * P / (ms * 1e-3)
+    line = {
+        "metric": METRIC, "value": value, "unit": "electron-points/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if form == pq.FORM_FP64 else "f32/bf16x3",
+        "data": "synthetic (seeded generator qmckl_b200/gen.py, no dataset)",
+        "config": {"workload": WORKLOAD, "points": P, "ao_num": A, "mo_num": M,
+                   "form": args.form, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "flushed (256 MB write) before every timed step; AO matrix >> L2"},
+        "e2e": {"value": world * P / (e2e_ms * 1e-3), "unit": "electron-points/s",
+                "h2d_bytes_per_step": int(P * 3 * 8), "d2h_bytes_per_step": int(P * 5 * M * 8),
+                "ms_per_step": e2e_ms},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "roofline": roofline,
+    }
+    if err is not None:
+        line["error_vs_fp64"] = err
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(sysd)
+    pq.context_destroy(ctx)
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,72 @@
+/*
+ * qmckl_b200.h -- B200 extensions beside the unchanged qmckl.h surface.
+ *
+ * The reference library has no device interface; these entry points have no
+ * counterpart in it.  They give callers that keep their electron coordinates
+ * and results in GPU memory a way to run the same evaluation without host
+ * copies, and expose the knobs of the device implementation.  Every function
+ * returns a qmckl_exit_code and records failures with qmckl_failwith, like
+ * the reference's own functions (org/qmckl_error.org:539-598).
+ */
+#ifndef QMCKL_B200_H
+#define QMCKL_B200_H
+
+#include "qmckl.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Arithmetic form of the device kernels.
+ *  AUTO : FP64 when the context precision is > 26 bits, else MIXED.  The
+ *         threshold is where the reference switches its MO contraction to
+ *         single precision (org/qmckl_mo.org:2028-2039).
+ *  FP64 : all arithmetic in FP64 (parity form).
+ *  MIXED: FP32 AO arithmetic (FP64 displacements, r^2, tight exponents and the
+ *         Laplacian radial factor) and the MO contraction on tcgen05 tensor
+ *         cores as split-BF16 products accumulated in FP32. */
+#define QMCKL_B200_FORM_AUTO  0
+#define QMCKL_B200_FORM_FP64  1
+#define QMCKL_B200_FORM_MIXED 2
+
+qmckl_exit_code qmckl_b200_set_form(qmckl_context context, const int32_t form);
+qmckl_exit_code qmckl_b200_get_form(const qmckl_context context, int32_t* const form);
+
+/* Number of bfloat16 pieces in the mixed MO contraction: 2 (3 products,
+ * hi*hi + hi*lo + lo*hi) or 3 (6 products, all pairs of total order <= 2).
+ * Default 3. */
+qmckl_exit_code qmckl_b200_set_split_terms(qmckl_context context, const int32_t pieces);
+
+/* The CUDA device and stream (cudaStream_t passed as void*) the context uses.
+ * Default: the current device at the first evaluation, and a stream owned by
+ * the context.  Set before the first evaluation. */
+qmckl_exit_code qmckl_b200_set_device(qmckl_context context, const int32_t device);
+qmckl_exit_code qmckl_b200_set_stream(qmckl_context context, void* stream);
+qmckl_exit_code qmckl_b200_synchronize(qmckl_context context);
+
+/* Device-resident evaluation.  d_coord is device memory holding point_num
+ * points as [3][point_num] (the 'T' layout of qmckl_set_point); outputs are
+ * device memory in the reference layouts ao_vgl[point][5][ao],
+ * ao_value[point][ao], mo_vgl[point][5][mo], mo_value[point][mo].  The basis
+ * and MO coefficients come from the context.  Work is enqueued on the
+ * context's stream; the call returns without synchronizing. */
+qmckl_exit_code qmckl_b200_ao_vgl_device(qmckl_context context, const int64_t point_num,
+                                         const double* d_coord, double* d_ao_vgl);
+qmckl_exit_code qmckl_b200_ao_value_device(qmckl_context context, const int64_t point_num,
+                                           const double* d_coord, double* d_ao_value);
+qmckl_exit_code qmckl_b200_mo_vgl_device(qmckl_context context, const int64_t point_num,
+                                         const double* d_coord, double* d_mo_vgl);
+qmckl_exit_code qmckl_b200_mo_value_device(qmckl_context context, const int64_t point_num,
+                                           const double* d_coord, double* d_mo_value);
+
+/* Number of kernels this library launched since the process started. */
+int64_t qmckl_b200_kernel_launch_count(void);
+
+/* Fault-injection hook for tests: make the n-th next allocation (host
+ * registry or device) fail with QMCKL_ALLOCATION_FAILED; n < 0 disables. */
+void qmckl_b200_inject_alloc_failure(const int64_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QMCKL_B200_H */

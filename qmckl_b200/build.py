@@ -1,0 +1,72 @@
+"""Build recipe of the product library libqmckl_b200.so (sm_100a).
+
+    python -m qmckl_b200.build        # -> qmckl_b200/_lib/libqmckl_b200.so
+
+The library is plain nvcc + g++ output with a C ABI (include/qmckl.h and
+include/qmckl_b200.h); it does not depend on PyTorch.
+"""
+import concurrent.futures as cf
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+OUT_DIR = os.path.join(HERE, "_lib")
+OBJ_DIR = os.path.join(ROOT, "_build", "qmckl_b200")
+LIB = os.path.join(OUT_DIR, "libqmckl_b200.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+INC = ["-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
+CU_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", *ARCH, *INC]
+CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-I/usr/local/cuda/include", *INC]
+
+
+def _sources():
+    return sorted(f for f in os.listdir(CSRC) if f.endswith((".cu", ".cpp")))
+
+
+def _headers():
+    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    inc = os.path.join(ROOT, "include")
+    hs += [os.path.join(inc, f) for f in os.listdir(inc)]
+    return hs
+
+
+def _compile(src, verbose):
+    obj = os.path.join(OBJ_DIR, src + ".o")
+    path = os.path.join(CSRC, src)
+    newest_dep = max([os.path.getmtime(path)] + [os.path.getmtime(h) for h in _headers()])
+    if os.path.exists(obj) and os.path.getmtime(obj) >= newest_dep:
+        return obj
+    if src.endswith(".cu"):
+        cmd = [NVCC, *CU_FLAGS, "-c", path, "-o", obj]
+    else:
+        cmd = ["g++", *CXX_FLAGS, "-c", path, "-o", obj]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    return obj
+
+
+def build(verbose=False, force=False):
+    os.makedirs(OUT_DIR, exist_ok=True)
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    if force:
+        for f in os.listdir(OBJ_DIR):
+            os.remove(os.path.join(OBJ_DIR, f))
+    srcs = _sources()
+    with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
+        objs = list(ex.map(lambda s: _compile(s, verbose), srcs))
+    if not force and os.path.exists(LIB) and all(os.path.getmtime(LIB) >= os.path.getmtime(o) for o in objs):
+        return LIB
+    cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs, "-Xlinker", "-soname=libqmckl_b200.so"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose=True, force="--force" in sys.argv))

@@ -1,0 +1,312 @@
+// AO kernels: FP64 AO VGL / AO value, the primitive and shell VGL getters, and
+// the mixed-precision AO VGL kernel that feeds the tensor-core MO contraction.
+//
+// Arithmetic follows the reference's production kernel
+// qmckl_compute_ao_vgl_hpc_gaussian (org/qmckl_ao.org:8601-8973):
+//   * nucleus screened when r^2 > cutoff * nucleus_range          (8707)
+//   * per nucleus, primitives sorted by exponent; a primitive and all
+//     following ones are skipped once a*r^2 > cutoff                (8756-8766)
+//   * radial VGL: e = exp(-a r^2), f = -2 a e,
+//     (e, f x, f y, f z, f (3 - 2 a r^2)) contracted with the merged
+//     normalized coefficients                                         (8798-8828)
+//   * shell skipped when its contracted value is exactly zero         (8850)
+//   * product rule with the cartesian monomials of
+//     qmckl_ao_polynomial_transp_vgl_hpc (6624-6914), 1e-20 shift on the value.
+//
+// Work decomposition (B200): one warp evaluates one (point, nucleus block)
+// pair.  Lanes first form the displacements of the block's nuclei, then the
+// radial VGL of the block's shells into shared memory, then sweep the block's
+// contiguous AO range with consecutive lanes on consecutive AOs, so every
+// store of ao_vgl[point][comp][k] is a 256-byte coalesced row segment.
+#include <cuda_bf16.h>
+
+#include "kernels.cuh"
+
+namespace qb {
+
+namespace {
+
+constexpr int kWarps = 8;
+constexpr double kShift = 1.e-20;
+
+__device__ __forceinline__ double ipow(double x, int n) {
+  double r = 1.0;
+  for (int i = 0; i < n; ++i) r = r * x;
+  return r;
+}
+
+// Cartesian monomial x^a y^b z^c with gradient and Laplacian, as formed by the
+// reference's HPC polynomial routine (l >= 2 branch; l <= 1 handled by caller).
+template <typename R>
+__device__ __forceinline__ void monomial_vgl(int a, int b, int c, R x, R y, R z, R out[5]) {
+  const R pa = (R)ipow(x, a), pb = (R)ipow(y, b), pc = (R)ipow(z, c);
+  const R pa1 = a >= 1 ? (R)ipow(x, a - 1) : R(1), pb1 = b >= 1 ? (R)ipow(y, b - 1) : R(1),
+          pc1 = c >= 1 ? (R)ipow(z, c - 1) : R(1);
+  const R pa2 = a >= 2 ? (R)ipow(x, a - 2) : R(1), pb2 = b >= 2 ? (R)ipow(y, b - 2) : R(1),
+          pc2 = c >= 2 ? (R)ipow(z, c - 2) : R(1);
+  R xy = pa * pb, yz = pb * pc, xz = pa * pc;
+  out[0] = xy * pc + R(kShift);
+  xy *= R(c);
+  xz *= R(b);
+  yz *= R(a);
+  out[1] = pa1 * yz;
+  out[2] = pb1 * xz;
+  out[3] = pc1 * xy;
+  out[4] = R(a - 1) * pa2 * yz + R(b - 1) * pb2 * xz + R(c - 1) * pc2 * xy;
+}
+
+struct WarpSmem {
+  double rad[kBlockSlots][5];   // radial VGL of the block's shells
+  double nuc[kBlockNuc][4];     // x, y, z displacement, r^2 (negative when screened out)
+};
+
+// Radial part of one shell (slot) for one point; FP64 throughout.
+template <int COMPS>
+__device__ __forceinline__ void shell_radial(const DevTables& T, int slot, int nucl, double x, double y,
+                                             double z, double r2, double cutoff, bool dp_exp,
+                                             double out[5]) {
+  double acc[5] = {0., 0., 0., 0., 0.};
+  const int2 cr = T.slot_coef[slot];
+  const int p0 = T.nuc_prim_start[nucl];
+  for (int j = cr.x; j < cr.y; ++j) {
+    const int ip = T.coef_prim[j];
+    const double a = T.expo[p0 + ip];
+    const double ar2 = a * r2;
+    if (ar2 > cutoff) break;   // primitives are sorted by exponent
+    const double e = dp_exp ? exp(-ar2) : (double)expf(-(float)ar2);
+    const double cv = T.coef_val[j];
+    acc[0] += cv * e;
+    if (COMPS == 5) {
+      double f = a * e;
+      f = -f - f;
+      acc[1] += cv * (f * x);
+      acc[2] += cv * (f * y);
+      acc[3] += cv * (f * z);
+      acc[4] += cv * (f * (3.0 - 2.0 * ar2));
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 5; ++c) out[c] = acc[c];
+}
+
+// Stages 1 and 2 of a (point, block) item: displacements and radial VGL in smem.
+template <int COMPS>
+__device__ __forceinline__ void stage_block(const DevTables& T, WarpSmem& sm, const int4 blk,
+                                            const int2 slots, double px, double py, double pz,
+                                            double cutoff, bool dp_exp, int lane) {
+  const int nn = blk.y - blk.x;
+  if (lane < nn) {
+    const int n = blk.x + lane;
+    const int N = T.nucl_num;
+    const double x = px - T.nucl_coord[n];
+    const double y = py - T.nucl_coord[n + N];
+    const double z = pz - T.nucl_coord[n + 2 * N];
+    const double r2 = x * x + y * y + z * z;
+    const bool in = !(r2 > cutoff * T.nucleus_range[n]);
+    sm.nuc[lane][0] = x;
+    sm.nuc[lane][1] = y;
+    sm.nuc[lane][2] = z;
+    sm.nuc[lane][3] = in ? r2 : -1.0;
+  }
+  __syncwarp();
+  for (int s = slots.x + lane; s < slots.y; s += 32) {
+    const int nucl = T.slot_nuc[s];
+    const int nl = nucl - blk.x;
+    const double r2 = sm.nuc[nl][3];
+    double out[5] = {0., 0., 0., 0., 0.};
+    if (r2 >= 0.0)
+      shell_radial<COMPS>(T, s, nucl, sm.nuc[nl][0], sm.nuc[nl][1], sm.nuc[nl][2], r2, cutoff, dp_exp, out);
+    const int ls = s - slots.x;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) sm.rad[ls][c] = out[c];
+  }
+  __syncwarp();
+}
+
+// FP64 AO VGL (COMPS = 5) or AO value (COMPS = 1).
+template <int COMPS>
+__global__ void __launch_bounds__(kWarps * 32)
+ao_f64_kernel(const DevTables T, const int64_t point_num, const double* __restrict__ coord,
+              const double cutoff, const bool dp_exp, double* __restrict__ out) {
+  __shared__ WarpSmem smem[kWarps];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  WarpSmem& sm = smem[warp];
+  const int64_t A = T.ao_num;
+  const int64_t items = point_num * (int64_t)T.nblock;
+  const int64_t stride = (int64_t)gridDim.x * kWarps;
+  for (int64_t it = (int64_t)blockIdx.x * kWarps + warp; it < items; it += stride) {
+    const int64_t p = it / T.nblock;
+    const int b = (int)(it - p * T.nblock);
+    const int4 blk = T.block[b];
+    const int2 slots = T.block_slots[b];
+    const double px = coord[p], py = coord[p + point_num], pz = coord[p + 2 * point_num];
+    stage_block<COMPS>(T, sm, blk, slots, px, py, pz, cutoff, dp_exp, lane);
+    double* __restrict__ row = out + p * COMPS * A;
+    for (int k = blk.z + lane; k < blk.w; k += 32) {
+      const int code = T.ao_code[k];
+      const int a = code & 15, bb = (code >> 4) & 15, c = (code >> 8) & 15, l = (code >> 12) & 15;
+      const int slot = (code >> 16) & 255, nl = (code >> 24) & 31;
+      double v[5] = {0., 0., 0., 0., 0.};
+      const double s1 = sm.rad[slot][0];
+      if (sm.nuc[nl][3] >= 0.0 && s1 != 0.0) {
+        const double f = T.ao_factor[k];
+        const double s2 = sm.rad[slot][1], s3 = sm.rad[slot][2], s4 = sm.rad[slot][3], s5 = sm.rad[slot][4];
+        if (l == 0) {
+          v[0] = s1 * f; v[1] = s2 * f; v[2] = s3 * f; v[3] = s4 * f; v[4] = s5 * f;
+        } else {
+          double P[5];
+          const double x = sm.nuc[nl][0], y = sm.nuc[nl][1], z = sm.nuc[nl][2];
+          if (l == 1) {
+            P[0] = (a ? x : (bb ? y : z)) + kShift;
+            P[1] = (double)a; P[2] = (double)bb; P[3] = (double)c; P[4] = 0.0;
+          } else {
+            monomial_vgl<double>(a, bb, c, x, y, z, P);
+          }
+          v[0] = P[0] * s1 * f;
+          if (COMPS == 5) {
+            v[1] = (P[1] * s1 + P[0] * s2) * f;
+            v[2] = (P[2] * s1 + P[0] * s3) * f;
+            v[3] = (P[3] * s1 + P[0] * s4) * f;
+            if (l == 1)
+              v[4] = (P[0] * s5 + 2.0 * (P[1] * s2 + P[2] * s3 + P[3] * s4)) * f;
+            else
+              v[4] = (P[4] * s1 + P[0] * s5 + 2.0 * (P[1] * s2 + P[2] * s3 + P[3] * s4)) * f;
+          }
+        }
+      }
+      row[k] = v[0];
+      if (COMPS == 5) {
+        row[A + k] = v[1];
+        row[2 * A + k] = v[2];
+        row[3 * A + k] = v[3];
+        row[4 * A + k] = v[4];
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// qmckl_compute_ao_basis_primitive_gaussian_vgl (org/qmckl_ao.org:4468-4520):
+// one thread per (point, primitive), primitive fastest for coalesced stores.
+__global__ void primitive_vgl_kernel(const DevTables T, const int64_t point_num,
+                                     const double* __restrict__ coord, const double cutoff,
+                                     double* __restrict__ out) {
+  const int64_t Pn = T.prim_num;
+  const int64_t total = point_num * Pn;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = i / Pn;
+    const int64_t q = i - p * Pn;
+    const int n = T.prim_nuc[q];
+    const int N = T.nucl_num;
+    const double x = coord[p] - T.nucl_coord[n];
+    const double y = coord[p + point_num] - T.nucl_coord[n + N];
+    const double z = coord[p + 2 * point_num] - T.nucl_coord[n + 2 * N];
+    const double r2 = x * x + y * y + z * z;
+    const double a = T.prim_expo[q];
+    const double ar2 = a * r2;
+    double* o = out + p * 5 * Pn + q;
+    if (ar2 > cutoff) {
+      o[0] = 0.0; o[Pn] = 0.0; o[2 * Pn] = 0.0; o[3 * Pn] = 0.0; o[4 * Pn] = 0.0;
+      continue;
+    }
+    const double v = exp(-ar2);
+    const double two_a = -2.0 * a * v;
+    o[0] = v;
+    o[Pn] = two_a * x;
+    o[2 * Pn] = two_a * y;
+    o[3 * Pn] = two_a * z;
+    o[4 * Pn] = two_a * (3.0 - 2.0 * ar2);
+  }
+}
+
+// qmckl_compute_ao_basis_shell_gaussian_vgl (org/qmckl_ao.org:4769-4868):
+// one thread per (point, shell); primitives in the user's order.
+__global__ void shell_vgl_kernel(const DevTables T, const int64_t point_num,
+                                 const double* __restrict__ coord, const double cutoff,
+                                 double* __restrict__ out) {
+  const int64_t S = T.shell_num;
+  const int64_t total = point_num * S;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = i / S;
+    const int64_t s = i - p * S;
+    const int n = T.shell_nuc[s];
+    const int N = T.nucl_num;
+    const double x = coord[p] - T.nucl_coord[n];
+    const double y = coord[p + point_num] - T.nucl_coord[n + N];
+    const double z = coord[p + 2 * point_num] - T.nucl_coord[n + 2 * N];
+    const double r2 = x * x + y * y + z * z;
+    double acc[5] = {0., 0., 0., 0., 0.};
+    if (!(r2 > cutoff * T.nucleus_range[n])) {
+      const int2 pr = T.shell_prims[s];
+      for (int q = pr.x; q < pr.y; ++q) {
+        const double a = T.prim_expo[q];
+        const double ar2 = a * r2;
+        if (ar2 > cutoff) continue;
+        const double v = T.prim_coef[q] * exp(-ar2);
+        const double two_a = -2.0 * a * v;
+        acc[0] += v;
+        acc[1] += two_a * x;
+        acc[2] += two_a * y;
+        acc[3] += two_a * z;
+        acc[4] += two_a * (3.0 - 2.0 * ar2);
+      }
+    }
+    double* o = out + p * 5 * S + s;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) o[c * S] = acc[c];
+  }
+}
+
+int grid_for(int64_t items_per_warp_unit) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t want = (items_per_warp_unit + kWarps - 1) / kWarps;
+  const int64_t cap = (int64_t)sms * 8;
+  return (int)(want < cap ? (want > 0 ? want : 1) : cap);
+}
+
+}  // namespace
+
+cudaError_t launch_ao_vgl_f64(const DevTables& T, int64_t point_num, const double* coord,
+                              double cutoff, bool dp_exp, double* ao_vgl, cudaStream_t s) {
+  if (point_num <= 0) return cudaSuccess;
+  const int grid = grid_for(point_num * T.nblock);
+  ao_f64_kernel<5><<<grid, kWarps * 32, 0, s>>>(T, point_num, coord, cutoff, dp_exp, ao_vgl);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ao_value_f64(const DevTables& T, int64_t point_num, const double* coord,
+                                double cutoff, bool dp_exp, double* ao_value, cudaStream_t s) {
+  if (point_num <= 0) return cudaSuccess;
+  const int grid = grid_for(point_num * T.nblock);
+  ao_f64_kernel<1><<<grid, kWarps * 32, 0, s>>>(T, point_num, coord, cutoff, dp_exp, ao_value);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_primitive_vgl(const DevTables& T, int64_t point_num, const double* coord,
+                                 double cutoff, double* prim_vgl, cudaStream_t s) {
+  if (point_num <= 0) return cudaSuccess;
+  const int64_t total = point_num * T.prim_num;
+  const int grid = (int)std::min<int64_t>((total + 255) / 256, 148 * 16);
+  primitive_vgl_kernel<<<grid, 256, 0, s>>>(T, point_num, coord, cutoff, prim_vgl);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_shell_vgl(const DevTables& T, int64_t point_num, const double* coord,
+                             double cutoff, double* shell_vgl, cudaStream_t s) {
+  if (point_num <= 0) return cudaSuccess;
+  const int64_t total = point_num * T.shell_num;
+  const int grid = (int)std::min<int64_t>((total + 255) / 256, 148 * 16);
+  shell_vgl_kernel<<<grid, 256, 0, s>>>(T, point_num, coord, cutoff, shell_vgl);
+  count_launch();
+  return cudaGetLastError();
+}
+
+}  // namespace qb

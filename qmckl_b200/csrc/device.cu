@@ -1,0 +1,676 @@
+// Device state of a context and the providers of the computed arrays.
+//
+// The DeviceState hangs off the context's extension pointer (the reference's
+// qmckl_extra hook, org/qmckl_context.org:183-198).  Providers mirror the
+// reference's date-stamped lazy caches (org/qmckl_ao.org:9035-9225,
+// org/qmckl_mo.org:1762-1877): an array is recomputed only when
+// ctx->point.date is newer than its date, and its date is then set to
+// ctx->date.  Inputs are uploaded when their host version changed: points on
+// every new point date, nuclear coordinates on every qmckl_set_nucleus_coord,
+// basis tables on every finalization, MO coefficients on every
+// finalize_mo_basis / rescale.  The host getters copy the device result into
+// the caller's buffer; the qmckl_b200_*_device entry points leave it on the GPU.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+#include "kernels.cuh"
+#include "mo_tc.cuh"
+#include "qmckl_b200.h"
+
+namespace qb {
+
+static std::atomic<int64_t> g_launches{0};
+void count_launch(int n) { g_launches += n; }
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+struct DeviceState {
+  int device = -1;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  // basis tables
+  uint64_t basis_version = 0;
+  DevBuf tables;
+  DevTables T{};
+  std::vector<char> host_tables;
+  uint64_t nucl_version = ~0ull;
+  DevBuf nucl;
+  // points
+  uint64_t coord_date = ~0ull;
+  int64_t coord_num = -1;
+  DevBuf coord;
+  // outputs
+  DevBuf prim_vgl, shell_vgl, ao_vgl, ao_value, mo_vgl, mo_value;
+  // MO coefficients (FP64 transpose [ao][mo])
+  uint64_t coef_version = ~0ull;
+  DevBuf coef_t;
+  // mixed form: split-bf16 coefficient pieces and the A-matrix scratch
+  TcPlan tc;
+  uint64_t tc_coef_version = ~0ull;
+  int tc_pieces = 0;
+  DevBuf tc_coef, tc_a;
+  int32_t split_pieces = 3;
+};
+
+namespace {
+
+qmckl_exit_code cuda_fail(qmckl_context context, cudaError_t e, const char* where) {
+  char msg[QMCKL_MAX_MSG_LEN];
+  std::snprintf(msg, sizeof msg, "CUDA error: %s", cudaGetErrorString(e));
+  return qmckl_failwith(context, QMCKL_FAILURE, where, msg);
+}
+
+#define QB_CUDA(expr, where)                                  \
+  do {                                                        \
+    cudaError_t e_ = (expr);                                  \
+    if (e_ != cudaSuccess) return cuda_fail(context, e_, where); \
+  } while (0)
+
+qmckl_exit_code ensure(qmckl_context context, DevBuf& b, size_t bytes, const char* where) {
+  if (b.cap >= bytes && b.p != nullptr) return QMCKL_SUCCESS;
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.cap = 0;
+  if (alloc_should_fail()) return qmckl_failwith(context, QMCKL_ALLOCATION_FAILED, where, "device allocation");
+  cudaError_t e = cudaMalloc(&b.p, std::max<size_t>(bytes, 256));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    b.p = nullptr;
+    char msg[QMCKL_MAX_MSG_LEN];
+    std::snprintf(msg, sizeof msg, "device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    return qmckl_failwith(context, QMCKL_ALLOCATION_FAILED, where, msg);
+  }
+  b.cap = std::max<size_t>(bytes, 256);
+  return QMCKL_SUCCESS;
+}
+
+void release(DevBuf& b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.cap = 0;
+}
+
+double cutoff_of(const Context* ctx) {
+  // org/qmckl_ao.org:7814
+  return std::log((double)(((uint64_t)1) << (ctx->precision - 1)));
+}
+
+bool use_mixed(const Context* ctx) {
+  if (ctx->form == QMCKL_B200_FORM_MIXED) return true;
+  if (ctx->form == QMCKL_B200_FORM_FP64) return false;
+  return ctx->precision <= 26;
+}
+
+// Pack the finalized basis into one device allocation.
+qmckl_exit_code upload_tables(qmckl_context context, DeviceState* ds) {
+  Context* ctx = ctx_of(context);
+  const AoBasisRec& B = ctx->ao_basis;
+  const AoDerived& d = B.d;
+  const int64_t N = ctx->nucleus.num, S = B.shell_num, Pn = B.prim_num, A = B.ao_num;
+
+  // nucleus blocks
+  std::vector<int4> blocks;
+  std::vector<int2> block_slots;
+  std::vector<int32_t> slot_nuc;
+  std::vector<int2> slot_coef;
+  std::vector<int32_t> ao_code(A, 0);
+  for (int64_t n = 0; n < N; ++n) {
+    if (B.nucleus_shell_num[n] > kBlockSlots)
+      return qmckl_failwith(context, QMCKL_FAILURE, "qmckl_b200_upload_basis",
+                            "more than 64 shells on one nucleus is not supported");
+  }
+  int64_t n = 0;
+  while (n < N) {
+    const int nb = (int)n;
+    int slots = 0;
+    const int slot_begin = (int)slot_nuc.size();
+    int64_t ao_begin = -1, ao_end = -1;
+    while (n < N && (n - nb) < kBlockNuc && slots + B.nucleus_shell_num[n] <= kBlockSlots) {
+      for (int64_t s = B.nucleus_index[n]; s < B.nucleus_index[n] + B.nucleus_shell_num[n]; ++s) {
+        const int slot = (int)slot_nuc.size() - slot_begin;
+        slot_nuc.push_back((int32_t)n);
+        slot_coef.push_back(make_int2(d.shell_coef_start[s], d.shell_coef_start[s + 1]));
+        const int l = B.shell_ang_mom[s];
+        const int64_t k0 = d.ao_index[s];
+        int64_t k = k0;
+        for (int a = l; a >= 0; --a)
+          for (int b = l - a; b >= 0; --b) {
+            const int c = l - a - b;
+            ao_code[k] = a | (b << 4) | (c << 8) | (l << 12) | (slot << 16) | ((int)(n - nb) << 24);
+            ++k;
+          }
+        if (ao_begin < 0 || k0 < ao_begin) ao_begin = k0;
+        if (k > ao_end) ao_end = k;
+        ++slots;
+      }
+      ++n;
+    }
+    if (ao_begin < 0) { ao_begin = 0; ao_end = 0; }
+    blocks.push_back(make_int4(nb, (int)n, (int)ao_begin, (int)ao_end));
+    block_slots.push_back(make_int2(slot_begin, (int)slot_nuc.size()));
+  }
+  // AO ranges of consecutive blocks must tile [0, A): true when the shells of
+  // each nucleus are numbered consecutively, which the AO numbering implies.
+  {
+    int64_t expect = 0;
+    for (auto& b4 : blocks) {
+      if (b4.z != expect && b4.w > b4.z)
+        return qmckl_failwith(context, QMCKL_FAILURE, "qmckl_b200_upload_basis", "AOs are not ordered by nucleus");
+      if (b4.w > b4.z) expect = b4.w;
+    }
+  }
+  std::vector<int32_t> prim_nuc(Pn, 0);
+  for (int64_t m = 0; m < N; ++m)
+    for (int64_t q = d.nucleus_prim_index[m]; q < d.nucleus_prim_index[m + 1] && q < Pn; ++q) prim_nuc[q] = (int32_t)m;
+  std::vector<int32_t> shell_nuc(S, 0);
+  std::vector<int2> shell_prims(S);
+  for (int64_t m = 0; m < N; ++m)
+    for (int64_t s = B.nucleus_index[m]; s < B.nucleus_index[m] + B.nucleus_shell_num[m]; ++s) shell_nuc[s] = (int32_t)m;
+  for (int64_t s = 0; s < S; ++s)
+    shell_prims[s] = make_int2((int)B.shell_prim_index[s], (int)(B.shell_prim_index[s] + B.shell_prim_num[s]));
+  // prim_nuc for primitives via their shells (covers any ordering)
+  for (int64_t s = 0; s < S; ++s)
+    for (int64_t q = B.shell_prim_index[s]; q < B.shell_prim_index[s] + B.shell_prim_num[s]; ++q) prim_nuc[q] = shell_nuc[s];
+
+  // layout: [offset of each array, 256-byte aligned]
+  std::vector<char>& H = ds->host_tables;
+  H.clear();
+  auto put = [&](const void* src, size_t bytes) -> size_t {
+    size_t off = (H.size() + 255) & ~size_t(255);
+    H.resize(off + std::max<size_t>(bytes, 1));
+    if (bytes) std::memcpy(H.data() + off, src, bytes);
+    return off;
+  };
+  const size_t o_range = put(d.nucleus_range.data(), sizeof(double) * N);
+  const size_t o_nps = put(d.nuc_prim_start.data(), sizeof(int32_t) * (N + 1));
+  const size_t o_expo = put(d.expo_sorted.data(), sizeof(double) * d.expo_sorted.size());
+  const size_t o_block = put(blocks.data(), sizeof(int4) * blocks.size());
+  const size_t o_bslot = put(block_slots.data(), sizeof(int2) * block_slots.size());
+  const size_t o_snuc = put(slot_nuc.data(), sizeof(int32_t) * slot_nuc.size());
+  const size_t o_scoef = put(slot_coef.data(), sizeof(int2) * slot_coef.size());
+  const size_t o_cprim = put(d.coef_prim.data(), sizeof(int32_t) * d.coef_prim.size());
+  const size_t o_cval = put(d.coef_val.data(), sizeof(double) * d.coef_val.size());
+  const size_t o_code = put(ao_code.data(), sizeof(int32_t) * A);
+  const size_t o_fac = put(B.ao_factor.data(), sizeof(double) * A);
+  const size_t o_pnuc = put(prim_nuc.data(), sizeof(int32_t) * Pn);
+  const size_t o_pexp = put(B.exponent.data(), sizeof(double) * Pn);
+  const size_t o_pcoef = put(d.coefficient_normalized.data(), sizeof(double) * Pn);
+  const size_t o_shnuc = put(shell_nuc.data(), sizeof(int32_t) * S);
+  const size_t o_shpr = put(shell_prims.data(), sizeof(int2) * S);
+  qmckl_exit_code rc = ensure(context, ds->tables, H.size(), "qmckl_b200_upload_basis");
+  if (rc != QMCKL_SUCCESS) return rc;
+  QB_CUDA(cudaMemcpyAsync(ds->tables.p, H.data(), H.size(), cudaMemcpyHostToDevice, ds->stream), "qmckl_b200_upload_basis");
+  char* base = (char*)ds->tables.p;
+  DevTables& T = ds->T;
+  T.nucl_num = (int32_t)N;
+  T.shell_num = (int32_t)S;
+  T.prim_num = (int32_t)Pn;
+  T.ao_num = (int32_t)A;
+  T.nblock = (int32_t)blocks.size();
+  T.nslot = (int32_t)slot_nuc.size();
+  T.nucleus_range = (const double*)(base + o_range);
+  T.nuc_prim_start = (const int32_t*)(base + o_nps);
+  T.expo = (const double*)(base + o_expo);
+  T.block = (const int4*)(base + o_block);
+  T.block_slots = (const int2*)(base + o_bslot);
+  T.slot_nuc = (const int32_t*)(base + o_snuc);
+  T.slot_coef = (const int2*)(base + o_scoef);
+  T.coef_prim = (const int32_t*)(base + o_cprim);
+  T.coef_val = (const double*)(base + o_cval);
+  T.ao_code = (const int32_t*)(base + o_code);
+  T.ao_factor = (const double*)(base + o_fac);
+  T.prim_nuc = (const int32_t*)(base + o_pnuc);
+  T.prim_expo = (const double*)(base + o_pexp);
+  T.prim_coef = (const double*)(base + o_pcoef);
+  T.shell_nuc = (const int32_t*)(base + o_shnuc);
+  T.shell_prims = (const int2*)(base + o_shpr);
+  ds->basis_version = B.basis_version;
+  ds->nucl_version = ~0ull;   // re-point the nuclear coordinates below
+  return QMCKL_SUCCESS;
+}
+
+qmckl_exit_code sync_inputs(qmckl_context context, DeviceState* ds, bool need_points) {
+  Context* ctx = ctx_of(context);
+  if (ds->basis_version != ctx->ao_basis.basis_version || ds->tables.p == nullptr) {
+    qmckl_exit_code rc = upload_tables(context, ds);
+    if (rc != QMCKL_SUCCESS) return rc;
+  }
+  if (ds->nucl_version != ctx->nucleus.coord_version) {
+    const int64_t N = ctx->nucleus.num;
+    if ((int64_t)ctx->nucleus.coord.size() < 3 * N)
+      return qmckl_failwith(context, QMCKL_NOT_PROVIDED, "qmckl_b200_upload_nucleus", "nuclear coordinates are not set");
+    qmckl_exit_code rc = ensure(context, ds->nucl, sizeof(double) * 3 * N, "qmckl_b200_upload_nucleus");
+    if (rc != QMCKL_SUCCESS) return rc;
+    QB_CUDA(cudaMemcpyAsync(ds->nucl.p, ctx->nucleus.coord.data(), sizeof(double) * 3 * N,
+                            cudaMemcpyHostToDevice, ds->stream), "qmckl_b200_upload_nucleus");
+    ds->nucl_version = ctx->nucleus.coord_version;
+  }
+  ds->T.nucl_coord = (const double*)ds->nucl.p;
+  if (need_points && (ds->coord_date != ctx->point.date || ds->coord_num != ctx->point.num)) {
+    const int64_t P = ctx->point.num;
+    qmckl_exit_code rc = ensure(context, ds->coord, sizeof(double) * 3 * std::max<int64_t>(P, 1), "qmckl_b200_upload_points");
+    if (rc != QMCKL_SUCCESS) return rc;
+    if (P > 0)
+      QB_CUDA(cudaMemcpyAsync(ds->coord.p, ctx->point.coord.data(), sizeof(double) * 3 * P,
+                              cudaMemcpyHostToDevice, ds->stream), "qmckl_b200_upload_points");
+    ds->coord_date = ctx->point.date;
+    ds->coord_num = P;
+  }
+  return QMCKL_SUCCESS;
+}
+
+qmckl_exit_code sync_coef(qmckl_context context, DeviceState* ds) {
+  Context* ctx = ctx_of(context);
+  if (ds->coef_version == ctx->mo_basis.coef_version && ds->coef_t.p) return QMCKL_SUCCESS;
+  const int64_t A = ctx->ao_basis.ao_num, M = ctx->mo_basis.mo_num;
+  qmckl_exit_code rc = ensure(context, ds->coef_t, sizeof(double) * A * M, "qmckl_b200_upload_mo");
+  if (rc != QMCKL_SUCCESS) return rc;
+  QB_CUDA(cudaMemcpyAsync(ds->coef_t.p, ctx->mo_basis.coefficient_t.data(), sizeof(double) * A * M,
+                          cudaMemcpyHostToDevice, ds->stream), "qmckl_b200_upload_mo");
+  ds->coef_version = ctx->mo_basis.coef_version;
+  return QMCKL_SUCCESS;
+}
+
+qmckl_exit_code copy_out(qmckl_context context, DeviceState* ds, double* host, const void* dev, size_t bytes,
+                         const char* where) {
+  if (host != nullptr && bytes > 0)
+    QB_CUDA(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, ds->stream), where);
+  QB_CUDA(cudaStreamSynchronize(ds->stream), where);
+  return QMCKL_SUCCESS;
+}
+
+DeviceState* state(qmckl_context context) { return ctx_of(context)->extra; }
+
+// ---- compute steps on the device (no date logic) ----
+
+qmckl_exit_code run_ao_vgl(qmckl_context context, DeviceState* ds, int64_t P, const double* coord, double* out) {
+  Context* ctx = ctx_of(context);
+  QB_CUDA(launch_ao_vgl_f64(ds->T, P, coord, cutoff_of(ctx), ctx->precision > 23, out, ds->stream), "qmckl_b200_ao_vgl");
+  return QMCKL_SUCCESS;
+}
+
+qmckl_exit_code run_ao_value(qmckl_context context, DeviceState* ds, int64_t P, const double* coord, double* out) {
+  Context* ctx = ctx_of(context);
+  QB_CUDA(launch_ao_value_f64(ds->T, P, coord, cutoff_of(ctx), ctx->precision > 23, out, ds->stream), "qmckl_b200_ao_value");
+  return QMCKL_SUCCESS;
+}
+
+qmckl_exit_code run_mo_mixed(qmckl_context context, DeviceState* ds, int64_t P, const double* coord,
+                             double* out, int comps) {
+  Context* ctx = ctx_of(context);
+  const int64_t A = ctx->ao_basis.ao_num, M = ctx->mo_basis.mo_num;
+  const int pieces = ds->split_pieces;
+  // coefficient pieces
+  if (ds->tc_coef_version != ctx->mo_basis.coef_version || ds->tc_pieces != pieces || !ds->tc_coef.p) {
+    TcPlan plan = tc_plan(A, M, pieces);
+    qmckl_exit_code rc = ensure(context, ds->tc_coef, plan.coef_bytes, "qmckl_b200_mo_mixed");
+    if (rc != QMCKL_SUCCESS) return rc;
+    QB_CUDA(tc_prepare_coef(plan, ctx->mo_basis.coefficient.data(), ds->tc_coef.p, ds->stream), "qmckl_b200_mo_mixed");
+    ds->tc = plan;
+    ds->tc_coef_version = ctx->mo_basis.coef_version;
+    ds->tc_pieces = pieces;
+  }
+  const int64_t rows = (int64_t)comps * P;
+  const size_t abytes = tc_a_bytes(ds->tc, rows);
+  qmckl_exit_code rc = ensure(context, ds->tc_a, abytes, "qmckl_b200_mo_mixed");
+  if (rc != QMCKL_SUCCESS) return rc;
+  QB_CUDA(tc_run(ds->T, ds->tc, P, comps, coord, cutoff_of(ctx), ds->tc_coef.p, ds->tc_a.p, out, ds->stream),
+          "qmckl_b200_mo_mixed");
+  return QMCKL_SUCCESS;
+}
+
+qmckl_exit_code run_mo(qmckl_context context, DeviceState* ds, int64_t P, const double* coord,
+                       double* ao_scratch, double* out, int comps) {
+  Context* ctx = ctx_of(context);
+  const int64_t A = ctx->ao_basis.ao_num, M = ctx->mo_basis.mo_num;
+  if (use_mixed(ctx)) return run_mo_mixed(context, ds, P, coord, out, comps);
+  qmckl_exit_code rc = sync_coef(context, ds);
+  if (rc != QMCKL_SUCCESS) return rc;
+  rc = comps == 5 ? run_ao_vgl(context, ds, P, coord, ao_scratch) : run_ao_value(context, ds, P, coord, ao_scratch);
+  if (rc != QMCKL_SUCCESS) return rc;
+  QB_CUDA(launch_gemm_f64(comps * P, M, A, ao_scratch, A, (const double*)ds->coef_t.p, M, out, M, ds->stream),
+          "qmckl_b200_mo");
+  return QMCKL_SUCCESS;
+}
+
+}  // namespace
+
+qmckl_exit_code dev_attach(qmckl_context context) {
+  Context* ctx = ctx_of(context);
+  if (ctx->extra) {
+    if (ctx->extra->device >= 0) QB_CUDA(cudaSetDevice(ctx->extra->device), "qmckl_b200_attach");
+    return QMCKL_SUCCESS;
+  }
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return qmckl_failwith(context, QMCKL_FAILURE, "qmckl_b200_attach",
+                          "no CUDA device: qmckl_b200 computes on the GPU only");
+  }
+  DeviceState* ds = new DeviceState();
+  QB_CUDA(cudaGetDevice(&ds->device), "qmckl_b200_attach");
+  ctx->extra = ds;
+  return QMCKL_SUCCESS;
+}
+
+static qmckl_exit_code ensure_stream(qmckl_context context, DeviceState* ds) {
+  if (ds->stream != nullptr) return QMCKL_SUCCESS;
+  QB_CUDA(cudaStreamCreateWithFlags(&ds->stream, cudaStreamNonBlocking), "qmckl_b200_attach");
+  ds->own_stream = true;
+  return QMCKL_SUCCESS;
+}
+
+static qmckl_exit_code attach_all(qmckl_context context) {
+  qmckl_exit_code rc = dev_attach(context);
+  if (rc != QMCKL_SUCCESS) return rc;
+  return ensure_stream(context, state(context));
+}
+
+void dev_detach(Context* ctx) {
+  DeviceState* ds = ctx->extra;
+  if (!ds) return;
+  if (ds->device >= 0) cudaSetDevice(ds->device);
+  if (ds->stream) cudaStreamSynchronize(ds->stream);
+  for (DevBuf* b : {&ds->tables, &ds->nucl, &ds->coord, &ds->prim_vgl, &ds->shell_vgl, &ds->ao_vgl, &ds->ao_value,
+                    &ds->mo_vgl, &ds->mo_value, &ds->coef_t, &ds->tc_coef, &ds->tc_a})
+    release(*b);
+  if (ds->own_stream && ds->stream) cudaStreamDestroy(ds->stream);
+  delete ds;
+  ctx->extra = nullptr;
+}
+
+qmckl_exit_code dev_invalidate_mo(qmckl_context context) {
+  DeviceState* ds = state(context);
+  if (ds) { ds->coef_version = ~0ull; ds->tc_coef_version = ~0ull; }
+  return QMCKL_SUCCESS;
+}
+
+qmckl_exit_code dev_provide_primitive_vgl(qmckl_context context, double* host_out) {
+  qmckl_exit_code rc = attach_all(context);
+  if (rc != QMCKL_SUCCESS) return rc;
+  Context* ctx = ctx_of(context);
+  DeviceState* ds = state(context);
+  rc = sync_inputs(context, ds, true);
+  if (rc != QMCKL_SUCCESS) return rc;
+  const int64_t P = ctx->point.num, n = ctx->ao_basis.prim_num;
+  const size_t bytes = sizeof(double) * 5 * n * P;
+  // The reference recomputes this array on every call (its provider stamps
+  // shell_vgl_date instead, org/qmckl_ao.org:4606-4616); recomputed here too.
+  rc = ensure(context, ds->prim_vgl, bytes, "qmckl_provide_ao_basis_primitive_vgl");
+  if (rc != QMCKL_SUCCESS) return rc;
+  QB_CUDA(launch_primitive_vgl(ds->T, P, (const double*)ds->coord.p, cutoff_of(ctx), (double*)ds->prim_vgl.p, ds->stream),
+          "qmckl_provide_ao_basis_primitive_vgl");
+  ctx->ao_basis.primitive_vgl_date = ctx->date;
+  return copy_out(context, ds, host_out, ds->prim_vgl.p, bytes, "qmckl_get_ao_basis_primitive_vgl");
+}
+
+qmckl_exit_code dev_provide_shell_vgl(qmckl_context context, double* host_out) {
+  qmckl_exit_code rc = attach_all(context);
+  if (rc != QMCKL_SUCCESS) return rc;
+  Context* ctx = ctx_of(context);
+  DeviceState* ds = state(context);
+  const int64_t P = ctx->point.num, n = ctx->ao_basis.shell_num;
+  const size_t bytes = sizeof(double) * 5 * n * P;
+  if (ctx->point.date > ctx->ao_basis.shell_vgl_date || ds->shell_vgl.cap < bytes) {
+    rc = sync_inputs(context, ds, true);
+    if (rc != QMCKL_SUCCESS) return rc;
+    rc = ensure(context, ds->shell_vgl, bytes, "qmckl_provide_ao_basis_shell_vgl");
+    if (rc != QMCKL_SUCCESS) return rc;
+    QB_CUDA(launch_shell_vgl(ds->T, P, (const double*)ds->coord.p, cutoff_of(ctx), (double*)ds->shell_vgl.p, ds->stream),
+            "qmckl_provide_ao_basis_shell_vgl");
+    ctx->ao_basis.shell_vgl_date = ctx->date;
+  }
+  return copy_out(context, ds, host_out, ds->shell_vgl.p, bytes, "qmckl_get_ao_basis_shell_vgl");
+}
+
+qmckl_exit_code dev_provide_ao_vgl(qmckl_context context, double* host_out) {
+  qmckl_exit_code rc = attach_all(context);
+  if (rc != QMCKL_SUCCESS) return rc;
+  Context* ctx = ctx_of(context);
+  DeviceState* ds = state(context);
+  if (ctx->ao_basis.type != 'G')
+    return qmckl_failwith(context, QMCKL_FAILURE, "qmckl_provide_ao_basis_ao_vgl", "only Gaussian basis sets are implemented");
+  const int64_t P = ctx->point.num, A = ctx->ao_basis.ao_num;
+  const size_t bytes = sizeof(double) * 5 * A * P;
+  if (ctx->point.date > ctx->ao_basis.ao_vgl_date || ds->ao_vgl.cap < bytes) {
+    rc = sync_inputs(context, ds, true);
+    if (rc != QMCKL_SUCCESS) return rc;
+    rc = ensure(context, ds->ao_vgl, bytes, "qmckl_provide_ao_basis_ao_vgl");
+    if (rc != QMCKL_SUCCESS) return rc;
+    rc = run_ao_vgl(context, ds, P, (const double*)ds->coord.p, (double*)ds->ao_vgl.p);
+    if (rc != QMCKL_SUCCESS) return rc;
+    ctx->ao_basis.ao_vgl_date = ctx->date;
+  }
+  return copy_out(context, ds, host_out, ds->ao_vgl.p, bytes, "qmckl_get_ao_basis_ao_vgl");
+}
+
+qmckl_exit_code dev_provide_ao_value(qmckl_context context, double* host_out) {
+  qmckl_exit_code rc = attach_all(context);
+  if (rc != QMCKL_SUCCESS) return rc;
+  Context* ctx = ctx_of(context);
+  DeviceState* ds = state(context);
+  if (ctx->ao_basis.type != 'G')
+    return qmckl_failwith(context, QMCKL_FAILURE, "qmckl_provide_ao_basis_ao_value", "only Gaussian basis sets are implemented");
+  const int64_t P = ctx->point.num, A = ctx->ao_basis.ao_num;
+  const size_t bytes = sizeof(double) * A * P;
+  if (ctx->point.date > ctx->ao_basis.ao_value_date || ds->ao_value.cap < bytes) {
+    rc = sync_inputs(context, ds, true);
+    if (rc != QMCKL_SUCCESS) return rc;
+    rc = ensure(context, ds->ao_value, bytes, "qmckl_provide_ao_basis_ao_value");
+    if (rc != QMCKL_SUCCESS) return rc;
+    rc = run_ao_value(context, ds, P, (const double*)ds->coord.p, (double*)ds->ao_value.p);
+    if (rc != QMCKL_SUCCESS) return rc;
+    ctx->ao_basis.ao_value_date = ctx->date;
+  }
+  return copy_out(context, ds, host_out, ds->ao_value.p, bytes, "qmckl_get_ao_basis_ao_value");
+}
+
+qmckl_exit_code dev_provide_mo_vgl(qmckl_context context, double* host_out) {
+  qmckl_exit_code rc = attach_all(context);
+  if (rc != QMCKL_SUCCESS) return rc;
+  Context* ctx = ctx_of(context);
+  DeviceState* ds = state(context);
+  if (ctx->ao_basis.type != 'G')
+    return qmckl_failwith(context, QMCKL_FAILURE, "qmckl_provide_mo_basis_mo_vgl", "only Gaussian basis sets are implemented");
+  if (!ctx->ao_basis.provided)
+    return qmckl_failwith(context, QMCKL_NOT_PROVIDED, "qmckl_ao_basis", NULL);
+  const int64_t P = ctx->point.num, A = ctx->ao_basis.ao_num, M = ctx->mo_basis.mo_num;
+  const size_t bytes = sizeof(double) * 5 * M * P;
+  if (ctx->point.date > ctx->mo_basis.mo_vgl_date || ds->mo_vgl.cap < bytes) {
+    rc = sync_inputs(context, ds, true);
+    if (rc != QMCKL_SUCCESS) return rc;
+    rc = ensure(context, ds->mo_vgl, bytes, "qmckl_provide_mo_basis_mo_vgl");
+    if (rc != QMCKL_SUCCESS) return rc;
+    if (use_mixed(ctx)) {
+      rc = run_mo_mixed(context, ds, P, (const double*)ds->coord.p, (double*)ds->mo_vgl.p, 5);
+    } else {
+      // FP64 form: the AO array is materialised (and cached) as in the reference
+      rc = sync_coef(context, ds);
+      if (rc != QMCKL_SUCCESS) return rc;
+      const size_t abytes = sizeof(double) * 5 * A * P;
+      if (ctx->point.date > ctx->ao_basis.ao_vgl_date || ds->ao_vgl.cap < abytes) {
+        rc = ensure(context, ds->ao_vgl, abytes, "qmckl_provide_ao_basis_ao_vgl");
+        if (rc != QMCKL_SUCCESS) return rc;
+        rc = run_ao_vgl(context, ds, P, (const double*)ds->coord.p, (double*)ds->ao_vgl.p);
+        if (rc != QMCKL_SUCCESS) return rc;
+        ctx->ao_basis.ao_vgl_date = ctx->date;
+      }
+      QB_CUDA(launch_gemm_f64(5 * P, M, A, (const double*)ds->ao_vgl.p, A, (const double*)ds->coef_t.p, M,
+                              (double*)ds->mo_vgl.p, M, ds->stream), "qmckl_provide_mo_basis_mo_vgl");
+    }
+    if (rc != QMCKL_SUCCESS) return rc;
+    ctx->mo_basis.mo_vgl_date = ctx->date;
+  }
+  return copy_out(context, ds, host_out, ds->mo_vgl.p, bytes, "qmckl_get_mo_basis_mo_vgl");
+}
+
+qmckl_exit_code dev_provide_mo_value(qmckl_context context, double* host_out) {
+  qmckl_exit_code rc = attach_all(context);
+  if (rc != QMCKL_SUCCESS) return rc;
+  Context* ctx = ctx_of(context);
+  DeviceState* ds = state(context);
+  if (ctx->ao_basis.type != 'G')
+    return qmckl_failwith(context, QMCKL_FAILURE, "qmckl_provide_mo_basis_mo_value", "only Gaussian basis sets are implemented");
+  const int64_t P = ctx->point.num, A = ctx->ao_basis.ao_num, M = ctx->mo_basis.mo_num;
+  const size_t bytes = sizeof(double) * M * P;
+  if (ctx->point.date > ctx->mo_basis.mo_value_date || ds->mo_value.cap < bytes) {
+    rc = ensure(context, ds->mo_value, bytes, "qmckl_provide_mo_basis_mo_value");
+    if (rc != QMCKL_SUCCESS) return rc;
+    if (ctx->mo_basis.mo_vgl_date == ctx->point.date && ds->mo_vgl.p != nullptr &&
+        ds->mo_vgl.cap >= sizeof(double) * 5 * M * P) {
+      // mo_vgl is current: take its value rows (org/qmckl_mo.org:1186-1198)
+      QB_CUDA(cudaMemcpy2DAsync(ds->mo_value.p, sizeof(double) * M, ds->mo_vgl.p, sizeof(double) * 5 * M,
+                                sizeof(double) * M, P, cudaMemcpyDeviceToDevice, ds->stream),
+              "qmckl_provide_mo_basis_mo_value");
+    } else {
+      rc = sync_inputs(context, ds, true);
+      if (rc != QMCKL_SUCCESS) return rc;
+      if (use_mixed(ctx)) {
+        rc = run_mo_mixed(context, ds, P, (const double*)ds->coord.p, (double*)ds->mo_value.p, 1);
+      } else {
+        rc = sync_coef(context, ds);
+        if (rc != QMCKL_SUCCESS) return rc;
+        const size_t abytes = sizeof(double) * A * P;
+        if (ctx->point.date > ctx->ao_basis.ao_value_date || ds->ao_value.cap < abytes) {
+          rc = ensure(context, ds->ao_value, abytes, "qmckl_provide_ao_basis_ao_value");
+          if (rc != QMCKL_SUCCESS) return rc;
+          rc = run_ao_value(context, ds, P, (const double*)ds->coord.p, (double*)ds->ao_value.p);
+          if (rc != QMCKL_SUCCESS) return rc;
+          ctx->ao_basis.ao_value_date = ctx->date;
+        }
+        QB_CUDA(launch_gemm_f64(P, M, A, (const double*)ds->ao_value.p, A, (const double*)ds->coef_t.p, M,
+                                (double*)ds->mo_value.p, M, ds->stream), "qmckl_provide_mo_basis_mo_value");
+      }
+      if (rc != QMCKL_SUCCESS) return rc;
+    }
+    ctx->mo_basis.mo_value_date = ctx->date;
+  }
+  return copy_out(context, ds, host_out, ds->mo_value.p, bytes, "qmckl_get_mo_basis_mo_value");
+}
+
+}  // namespace qb
+
+using namespace qb;
+
+extern "C" {
+
+int64_t qmckl_b200_kernel_launch_count(void) { return g_launches.load(); }
+
+qmckl_exit_code qmckl_b200_set_split_terms(qmckl_context context, const int32_t pieces) {
+  if (qmckl_context_check(context) == QMCKL_NULL_CONTEXT) return QMCKL_INVALID_CONTEXT;
+  if (pieces != 2 && pieces != 3)
+    return qmckl_failwith(context, QMCKL_INVALID_ARG_2, "qmckl_b200_set_split_terms", "pieces must be 2 or 3");
+  qmckl_exit_code rc = dev_attach(context);
+  if (rc != QMCKL_SUCCESS) return rc;
+  if (state(context)->split_pieces != pieces) {
+    state(context)->split_pieces = pieces;
+    qmckl_context_touch(context);
+  }
+  return QMCKL_SUCCESS;
+}
+
+qmckl_exit_code qmckl_b200_set_device(qmckl_context context, const int32_t device) {
+  if (qmckl_context_check(context) == QMCKL_NULL_CONTEXT) return QMCKL_INVALID_CONTEXT;
+  Context* ctx = ctx_of(context);
+  if (ctx->extra && (ctx->extra->tables.p || ctx->extra->stream))
+    return qmckl_failwith(context, QMCKL_ALREADY_SET, "qmckl_b200_set_device", "set the device before the first evaluation");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    cudaGetLastError();
+    return qmckl_failwith(context, QMCKL_INVALID_ARG_2, "qmckl_b200_set_device", "no such device");
+  }
+  qmckl_exit_code rc = dev_attach(context);
+  if (rc != QMCKL_SUCCESS) return rc;
+  ctx->extra->device = device;
+  QB_CUDA(cudaSetDevice(device), "qmckl_b200_set_device");
+  return QMCKL_SUCCESS;
+}
+
+qmckl_exit_code qmckl_b200_set_stream(qmckl_context context, void* stream) {
+  if (qmckl_context_check(context) == QMCKL_NULL_CONTEXT) return QMCKL_INVALID_CONTEXT;
+  qmckl_exit_code rc = dev_attach(context);
+  if (rc != QMCKL_SUCCESS) return rc;
+  DeviceState* ds = state(context);
+  if (ds->own_stream && ds->stream) {
+    cudaStreamSynchronize(ds->stream);
+    cudaStreamDestroy(ds->stream);
+  }
+  ds->stream = (cudaStream_t)stream;
+  ds->own_stream = false;
+  if (ds->stream == nullptr) return ensure_stream(context, ds);
+  return QMCKL_SUCCESS;
+}
+
+qmckl_exit_code qmckl_b200_synchronize(qmckl_context context) {
+  if (qmckl_context_check(context) == QMCKL_NULL_CONTEXT) return QMCKL_INVALID_CONTEXT;
+  DeviceState* ds = state(context);
+  if (!ds || !ds->stream) return QMCKL_SUCCESS;
+  QB_CUDA(cudaStreamSynchronize(ds->stream), "qmckl_b200_synchronize");
+  return QMCKL_SUCCESS;
+}
+
+static qmckl_exit_code device_entry(qmckl_context context, const char* fname, int64_t point_num,
+                                    const double* d_coord, void* d_out, bool need_mo) {
+  if (qmckl_context_check(context) == QMCKL_NULL_CONTEXT) return QMCKL_INVALID_CONTEXT;
+  Context* ctx = ctx_of(context);
+  if (!ctx->ao_basis.provided) return qmckl_failwith(context, QMCKL_NOT_PROVIDED, fname, "AO basis not provided");
+  if (need_mo && !ctx->mo_basis.provided) return qmckl_failwith(context, QMCKL_NOT_PROVIDED, fname, "MO basis not provided");
+  if (ctx->ao_basis.type != 'G') return qmckl_failwith(context, QMCKL_FAILURE, fname, "only Gaussian basis sets are implemented");
+  if (point_num < 0) return qmckl_failwith(context, QMCKL_INVALID_ARG_2, fname, "point_num < 0");
+  if (point_num > 0 && d_coord == nullptr) return qmckl_failwith(context, QMCKL_INVALID_ARG_3, fname, "NULL pointer");
+  if (point_num > 0 && d_out == nullptr) return qmckl_failwith(context, QMCKL_INVALID_ARG_4, fname, "NULL pointer");
+  qmckl_exit_code rc = attach_all(context);
+  if (rc != QMCKL_SUCCESS) return rc;
+  return sync_inputs(context, state(context), false);
+}
+
+qmckl_exit_code qmckl_b200_ao_vgl_device(qmckl_context context, const int64_t point_num, const double* d_coord,
+                                         double* d_ao_vgl) {
+  qmckl_exit_code rc = device_entry(context, "qmckl_b200_ao_vgl_device", point_num, d_coord, d_ao_vgl, false);
+  if (rc != QMCKL_SUCCESS) return rc;
+  return run_ao_vgl(context, state(context), point_num, d_coord, d_ao_vgl);
+}
+
+qmckl_exit_code qmckl_b200_ao_value_device(qmckl_context context, const int64_t point_num, const double* d_coord,
+                                           double* d_ao_value) {
+  qmckl_exit_code rc = device_entry(context, "qmckl_b200_ao_value_device", point_num, d_coord, d_ao_value, false);
+  if (rc != QMCKL_SUCCESS) return rc;
+  return run_ao_value(context, state(context), point_num, d_coord, d_ao_value);
+}
+
+static qmckl_exit_code mo_device(qmckl_context context, const char* fname, int64_t point_num, const double* d_coord,
+                                 double* d_out, int comps) {
+  qmckl_exit_code rc = device_entry(context, fname, point_num, d_coord, d_out, true);
+  if (rc != QMCKL_SUCCESS) return rc;
+  Context* ctx = ctx_of(context);
+  DeviceState* ds = state(context);
+  if (use_mixed(ctx)) return run_mo_mixed(context, ds, point_num, d_coord, d_out, comps);
+  const size_t abytes = sizeof(double) * comps * ctx->ao_basis.ao_num * point_num;
+  DevBuf& scratch = comps == 5 ? ds->ao_vgl : ds->ao_value;
+  rc = ensure(context, scratch, abytes, fname);
+  if (rc != QMCKL_SUCCESS) return rc;
+  // the AO scratch no longer holds the context's cached points
+  if (comps == 5) ctx->ao_basis.ao_vgl_date = 0; else ctx->ao_basis.ao_value_date = 0;
+  return run_mo(context, ds, point_num, d_coord, (double*)scratch.p, d_out, comps);
+}
+
+qmckl_exit_code qmckl_b200_mo_vgl_device(qmckl_context context, const int64_t point_num, const double* d_coord,
+                                         double* d_mo_vgl) {
+  return mo_device(context, "qmckl_b200_mo_vgl_device", point_num, d_coord, d_mo_vgl, 5);
+}
+
+qmckl_exit_code qmckl_b200_mo_value_device(qmckl_context context, const int64_t point_num, const double* d_coord,
+                                           double* d_mo_value) {
+  return mo_device(context, "qmckl_b200_mo_value_device", point_num, d_coord, d_mo_value, 1);
+}
+
+}  // extern "C"

@@ -1,0 +1,182 @@
+// FP64 MO contraction: C[M][N] = A[M][K] * B[K][N] (row-major).
+//
+// For MO VGL, A is ao_vgl viewed as a (5*point_num) x ao_num matrix, B is
+// coefficient_t [ao][mo] and C is mo_vgl viewed as (5*point_num) x mo_num; for
+// MO value the same with ao_value / mo_value.  This is the dense form of
+// qmckl_compute_mo_basis_mo_vgl_hpc (org/qmckl_mo.org:2015-2163): the
+// reference skips AOs whose value is exactly zero, whose products are exact
+// zeros, so only the summation order differs.
+//
+// The FP64 form runs on the FP64 tensor pipe (mma.sync m8n8k4 f64, the only
+// FP64 MMA on sm_100a; tcgen05 has no FP64 kind).  CTA tile 128 x (8*NT*2),
+// BK = 16, 8 warps as 4 (M) x 2 (N), each warp 32 x 8*NT, operands staged in
+// shared memory by a 3-stage cp.async pipeline with zero-filled edges.
+#include <algorithm>
+
+#include "kernels.cuh"
+
+namespace qb {
+namespace {
+
+constexpr int BM = 128, BK = 16, STAGES = 3;
+constexpr int LDA_S = BK + 4;  // padded smem row stride (doubles) of the A tile
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(bytes));
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src, int bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(bytes));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+template <int NT, int VA, int VB>
+__global__ void __launch_bounds__(256)
+dgemm_kernel(int64_t M, int64_t N, int64_t K, const double* __restrict__ A, int64_t lda,
+             const double* __restrict__ B, int64_t ldb, double* __restrict__ C, int64_t ldc) {
+  constexpr int BN = 16 * NT;
+  constexpr int LDB_S = BN + 4;
+  extern __shared__ __align__(16) double smem[];
+  double* As = smem;                               // [STAGES][BM][LDA_S]
+  double* Bs = smem + STAGES * BM * LDA_S;         // [STAGES][BK][LDB_S]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp & 3, wn = warp >> 2;
+  const int g = lane >> 2, t = lane & 3;
+  const int64_t n0 = (int64_t)blockIdx.x * BN;
+  const int ktiles = (int)((K + BK - 1) / BK);
+
+  for (int64_t mt = blockIdx.y; mt * BM < M; mt += gridDim.y) {
+    const int64_t m0 = mt * BM;
+    double acc[4][NT][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+    auto load_tile = [&](int kt, int st) {
+      const int64_t k0 = (int64_t)kt * BK;
+      double* as = As + st * BM * LDA_S;
+      double* bs = Bs + st * BK * LDB_S;
+      // A tile: BM x BK
+      constexpr int ACH = BM * BK / VA;
+#pragma unroll
+      for (int i = 0; i < ACH / 256; ++i) {
+        const int c = tid + i * 256;
+        const int row = c / (BK / VA), col = (c % (BK / VA)) * VA;
+        const int64_t gm = m0 + row, gk = k0 + col;
+        int bytes = 0;
+        if (gm < M && gk < K) bytes = (int)((K - gk) < VA ? (K - gk) : VA) * 8;
+        const double* src = bytes ? A + gm * lda + gk : A;
+        if (VA == 2) cp_async16(as + row * LDA_S + col, src, bytes);
+        else cp_async8(as + row * LDA_S + col, src, bytes);
+      }
+      // B tile: BK x BN
+      constexpr int BCH = BK * BN / VB;
+      for (int c = tid; c < BCH; c += 256) {
+        const int row = c / (BN / VB), col = (c % (BN / VB)) * VB;
+        const int64_t gk = k0 + row, gn = n0 + col;
+        int bytes = 0;
+        if (gk < K && gn < N) bytes = (int)((N - gn) < VB ? (N - gn) : VB) * 8;
+        const double* src = bytes ? B + gk * ldb + gn : B;
+        if (VB == 2) cp_async16(bs + row * LDB_S + col, src, bytes);
+        else cp_async8(bs + row * LDB_S + col, src, bytes);
+      }
+    };
+
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; ++s) {
+      if (s < ktiles) load_tile(s, s);
+      cp_commit();
+    }
+    for (int kt = 0; kt < ktiles; ++kt) {
+      cp_wait<STAGES - 2>();
+      __syncthreads();
+      const int nk = kt + STAGES - 1;
+      if (nk < ktiles) load_tile(nk, nk % STAGES);
+      cp_commit();
+      const double* as = As + (kt % STAGES) * BM * LDA_S + (wm * 32) * LDA_S;
+      const double* bs = Bs + (kt % STAGES) * BK * LDB_S + wn * (8 * NT);
+#pragma unroll
+      for (int kk = 0; kk < BK; kk += 4) {
+        double af[4], bf[NT];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) af[i] = as[(i * 8 + g) * LDA_S + kk + t];
+#pragma unroll
+        for (int j = 0; j < NT; ++j) bf[j] = bs[(kk + t) * LDB_S + j * 8 + g];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < NT; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+      }
+    }
+    cp_wait<0>();
+    __syncthreads();
+    // epilogue: each thread owns rows g of 8-row tiles, columns 2t, 2t+1
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int64_t m = m0 + wm * 32 + i * 8 + g;
+      if (m >= M) continue;
+      double* crow = C + m * ldc;
+#pragma unroll
+      for (int j = 0; j < NT; ++j) {
+        const int64_t n = n0 + wn * (8 * NT) + j * 8 + 2 * t;
+        if (n + 1 < N && ((ldc & 1) == 0)) {
+          *reinterpret_cast<double2*>(crow + n) = make_double2(acc[i][j][0], acc[i][j][1]);
+        } else {
+          if (n < N) crow[n] = acc[i][j][0];
+          if (n + 1 < N) crow[n + 1] = acc[i][j][1];
+        }
+      }
+    }
+  }
+}
+
+template <int NT, int VA, int VB>
+cudaError_t run(int64_t M, int64_t N, int64_t K, const double* A, int64_t lda, const double* B,
+                int64_t ldb, double* C, int64_t ldc, cudaStream_t s) {
+  constexpr int BN = 16 * NT;
+  const size_t smem = sizeof(double) * STAGES * (BM * LDA_S + BK * (BN + 4));
+  auto kern = dgemm_kernel<NT, VA, VB>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int64_t mt = (M + BM - 1) / BM;
+  dim3 grid((unsigned)((N + BN - 1) / BN), (unsigned)std::min<int64_t>(mt, 65535));
+  kern<<<grid, 256, smem, s>>>(M, N, K, A, lda, B, ldb, C, ldc);
+  count_launch();
+  return cudaGetLastError();
+}
+
+template <int NT>
+cudaError_t run_nt(int64_t M, int64_t N, int64_t K, const double* A, int64_t lda, const double* B,
+                   int64_t ldb, double* C, int64_t ldc, cudaStream_t s) {
+  const bool va = (lda % 2 == 0) && ((uintptr_t)A % 16 == 0);
+  const bool vb = (ldb % 2 == 0) && ((uintptr_t)B % 16 == 0);
+  if (va && vb) return run<NT, 2, 2>(M, N, K, A, lda, B, ldb, C, ldc, s);
+  if (va) return run<NT, 2, 1>(M, N, K, A, lda, B, ldb, C, ldc, s);
+  if (vb) return run<NT, 1, 2>(M, N, K, A, lda, B, ldb, C, ldc, s);
+  return run<NT, 1, 1>(M, N, K, A, lda, B, ldb, C, ldc, s);
+}
+
+}  // namespace
+
+cudaError_t launch_gemm_f64(int64_t M, int64_t N, int64_t K, const double* A, int64_t lda,
+                            const double* B, int64_t ldb, double* C, int64_t ldc, cudaStream_t s) {
+  if (M <= 0 || N <= 0) return cudaSuccess;
+  // pick the N tile (64 or 80 columns) that wastes fewer padded columns
+  const int64_t w64 = ((N + 63) / 64) * 64 - N, w80 = ((N + 79) / 80) * 80 - N;
+  if (w80 < w64) return run_nt<5>(M, N, K, A, lda, B, ldb, C, ldc, s);
+  return run_nt<4>(M, N, K, A, lda, B, ldb, C, ldc, s);
+}
+
+}  // namespace qb

@@ -1,0 +1,68 @@
+// Device-side tables and kernel launchers of the orbital-evaluation path.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace qb {
+
+// Limits of the per-warp shared-memory staging in the AO kernels.  A nucleus
+// block holds at most kBlockNuc nuclei and kBlockSlots shells; finalization
+// rejects a basis with more than kBlockSlots shells on one nucleus.
+constexpr int kBlockNuc = 32;
+constexpr int kBlockSlots = 64;
+
+// Basis tables in device memory (one allocation; see device.cu).
+//
+// Nuclei are grouped into blocks of consecutive nuclei.  A block's AOs are
+// contiguous ([ao_begin, ao_end)) because AOs are numbered nucleus by nucleus.
+// The block's shells are its "slots" (block-local shell numbering) and each AO
+// carries its slot, its block-local nucleus and its cartesian powers.
+struct DevTables {
+  int32_t nucl_num, shell_num, prim_num, ao_num, nblock, nslot;
+  const double* nucl_coord;       // [3][nucl]
+  const double* nucleus_range;    // [nucl]
+  const int32_t* nuc_prim_start;  // [nucl+1] into expo (sorted, de-duplicated per nucleus)
+  const double* expo;             // [sum of unique primitives]
+  const int4* block;              // [nblock] (nuc_begin, nuc_end, ao_begin, ao_end)
+  const int2* block_slots;        // [nblock] (slot_begin, slot_end)
+  const int32_t* slot_nuc;        // [nslot] global nucleus of a slot
+  const int2* slot_coef;          // [nslot] (begin, end) into coef_prim / coef_val
+  const int32_t* coef_prim;       // nucleus-local index of the sorted primitive
+  const double* coef_val;         // normalized, merged coefficient
+  const int32_t* ao_code;         // [ao] a | b<<4 | c<<8 | l<<12 | slot<<16 | nuc_local<<24
+  const double* ao_factor;        // [ao]
+  // tables of the primitive / shell getters (unsorted, as set by the user)
+  const int32_t* prim_nuc;        // [prim]
+  const double* prim_expo;        // [prim]
+  const double* prim_coef;        // [prim] normalized coefficient
+  const int32_t* shell_nuc;       // [shell]
+  const int2* shell_prims;        // [shell] (prim_begin, prim_end)
+};
+
+// Global count of kernels launched by this library.
+void count_launch(int n = 1);
+
+// AO kernels (ao_kernels.cu).  coord is [3][point_num].  All return
+// cudaGetLastError() after the launch.
+cudaError_t launch_ao_vgl_f64(const DevTables& T, int64_t point_num, const double* coord,
+                              double cutoff, bool dp_exp, double* ao_vgl, cudaStream_t s);
+cudaError_t launch_ao_value_f64(const DevTables& T, int64_t point_num, const double* coord,
+                                double cutoff, bool dp_exp, double* ao_value, cudaStream_t s);
+cudaError_t launch_primitive_vgl(const DevTables& T, int64_t point_num, const double* coord,
+                                 double cutoff, double* prim_vgl, cudaStream_t s);
+cudaError_t launch_shell_vgl(const DevTables& T, int64_t point_num, const double* coord,
+                             double cutoff, double* shell_vgl, cudaStream_t s);
+
+// Mixed-form AO kernel: writes the AO matrix A[(point,comp)][k] as `pieces`
+// bfloat16 matrices (A = sum of pieces), each [5*point_num][lda], lda >= ao_num,
+// pieces at stride piece_stride elements.
+cudaError_t launch_ao_vgl_split(const DevTables& T, int64_t point_num, const double* coord,
+                                double cutoff, int pieces, void* a_pieces, int64_t lda,
+                                int64_t piece_stride, cudaStream_t s);
+
+// FP64 GEMM C[M][N] = A[M][K] * B[K][N], row-major with leading dimensions (gemm_f64.cu).
+cudaError_t launch_gemm_f64(int64_t M, int64_t N, int64_t K, const double* A, int64_t lda,
+                            const double* B, int64_t ldb, double* C, int64_t ldc, cudaStream_t s);
+
+}  // namespace qb

@@ -1,0 +1,36 @@
+// Mixed-precision MO contraction on tcgen05 tensor cores (mo_tc.cu).
+//
+// A (the AO matrix, rows = (point, component), columns = AOs) and C (the MO
+// coefficients) are split into `pieces` bfloat16 matrices whose sum is the
+// FP32 value; the products of total order < pieces are accumulated in FP32 in
+// tensor memory (pieces = 2: hi*hi + hi*lo + lo*hi; pieces = 3: the six
+// products of order <= 2).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+
+#include "kernels.cuh"
+
+namespace qb {
+
+struct TcPlan {
+  int64_t ao_num = 0, mo_num = 0;
+  int pieces = 3;
+  int64_t k_pad = 0;     // AO count padded to the K block (64)
+  int64_t n_pad = 0;     // MO count padded to a multiple of 16 (one tile <= 256)
+  int n_tiles = 0;       // number of N tiles of n_tile columns
+  int n_tile = 0;
+  size_t coef_bytes = 0; // pieces * n_pad * k_pad bfloat16
+};
+
+TcPlan tc_plan(int64_t ao_num, int64_t mo_num, int pieces);
+size_t tc_a_bytes(const TcPlan& plan, int64_t rows);
+// coefficient [mo][ao] (host, FP64) -> split bf16 pieces on the device
+cudaError_t tc_prepare_coef(const TcPlan& plan, const double* coefficient_host, void* d_coef, cudaStream_t s);
+// AO (mixed) -> A pieces -> tensor-core GEMM -> out[(point*comps + c)][mo] FP64
+cudaError_t tc_run(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps, const double* coord,
+                   double cutoff, const void* d_coef, void* d_a, double* out, cudaStream_t s);
+
+}  // namespace qb
