@@ -189,7 +189,8 @@ def main():
     P, A, M = W * E, sysd["ao_num"], sysd["mo_num"]
     form = pq.FORM_MIXED if args.form == "mixed" else pq.FORM_FP64
     ctx = make_context(sysd, points=False, form=form)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()          # evaluation stream shared by torch and the library
+    torch.cuda.set_stream(stream)
     pq.b200_set_stream(ctx, stream.cuda_stream)
 
     coord_t = np.ascontiguousarray(gen.points(sysd).T)               # [3][P]

@@ -38,8 +38,9 @@ qmckl_exit_code qmckl_b200_get_form(const qmckl_context context, int32_t* const 
 qmckl_exit_code qmckl_b200_set_split_terms(qmckl_context context, const int32_t pieces);
 
 /* The CUDA device and stream (cudaStream_t passed as void*) the context uses.
- * Default: the current device at the first evaluation, and a stream owned by
- * the context.  Set before the first evaluation. */
+ * Default: the current device at the first evaluation, and a non-blocking
+ * stream owned by the context.  A stream handle of 0 selects the legacy
+ * default stream.  Set the device before the first evaluation. */
 qmckl_exit_code qmckl_b200_set_device(qmckl_context context, const int32_t device);
 qmckl_exit_code qmckl_b200_set_stream(qmckl_context context, void* stream);
 qmckl_exit_code qmckl_b200_synchronize(qmckl_context context);

@@ -36,6 +36,7 @@ struct DeviceState {
   int device = -1;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  bool stream_given = false;     // set by qmckl_b200_set_stream (0 = the legacy default stream)
   // basis tables
   uint64_t basis_version = 0;
   DevBuf tables;
@@ -363,7 +364,7 @@ qmckl_exit_code dev_attach(qmckl_context context) {
 }
 
 static qmckl_exit_code ensure_stream(qmckl_context context, DeviceState* ds) {
-  if (ds->stream != nullptr) return QMCKL_SUCCESS;
+  if (ds->stream != nullptr || ds->stream_given) return QMCKL_SUCCESS;
   QB_CUDA(cudaStreamCreateWithFlags(&ds->stream, cudaStreamNonBlocking), "qmckl_b200_attach");
   ds->own_stream = true;
   return QMCKL_SUCCESS;
@@ -581,7 +582,7 @@ qmckl_exit_code qmckl_b200_set_split_terms(qmckl_context context, const int32_t 
 qmckl_exit_code qmckl_b200_set_device(qmckl_context context, const int32_t device) {
   if (qmckl_context_check(context) == QMCKL_NULL_CONTEXT) return QMCKL_INVALID_CONTEXT;
   Context* ctx = ctx_of(context);
-  if (ctx->extra && (ctx->extra->tables.p || ctx->extra->stream))
+  if (ctx->extra && (ctx->extra->tables.p || ctx->extra->stream || ctx->extra->stream_given))
     return qmckl_failwith(context, QMCKL_ALREADY_SET, "qmckl_b200_set_device", "set the device before the first evaluation");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
@@ -606,7 +607,7 @@ qmckl_exit_code qmckl_b200_set_stream(qmckl_context context, void* stream) {
   }
   ds->stream = (cudaStream_t)stream;
   ds->own_stream = false;
-  if (ds->stream == nullptr) return ensure_stream(context, ds);
+  ds->stream_given = true;
   return QMCKL_SUCCESS;
 }
 

@@ -1,21 +1,559 @@
-// Mixed-precision MO contraction (placeholder until the tcgen05 kernel lands).
+// Mixed-precision MO contraction on tcgen05 tensor cores.
+//
+// mo[(p,c)][i] = sum_k A[(p,c)][k] * C[i][k], with A = ao_vgl viewed as a
+// (comps*point_num) x ao_num matrix (qmckl_compute_mo_basis_mo_vgl_hpc,
+// org/qmckl_mo.org:2015-2163, in dense form) and C = coefficient[mo][ao].
+//
+// Both operands are split into bfloat16 pieces, X = X1 + X2 (+ X3), the
+// pieces of A produced by the mixed AO kernel and those of C once per
+// coefficient update.  Products X_i*Y_j with i + j < pieces are accumulated
+// in FP32 in tensor memory: 3 products for 2 pieces (error ~2^-16 relative),
+// 6 products for 3 pieces (~2^-24, below the FP32 rounding of the AOs).
+//
+// GEMM kernel (one 128 x n_tile output tile per CTA):
+//   warp 4      TMA producer: all A and C pieces of a 64-wide K block into a
+//               stage (128B-swizzled, K-major), completion on full[stage]
+//   warp 5      allocates TMEM, then one thread issues the tcgen05.mma chain
+//               (4 K steps x products) and commits to empty[stage]; after the
+//               last K block it commits to acc_full
+//   warps 0..3  epilogue: tcgen05.ld 32 lanes each, FP32 -> FP64, staged in
+//               shared memory and written as contiguous output rows
+// Every mbarrier wait is bounded by a %globaltimer deadline; a timeout sets an
+// error word that the host turns into QMCKL_FAILURE, and the CTA still frees
+// its TMEM and exits.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
 #include "mo_tc.cuh"
 
 namespace qb {
 
+namespace {
+
+constexpr int BM = 128;          // rows per tile (tcgen05 M)
+constexpr int BK = 64;           // K per stage: one 128-byte swizzle row of bf16
+constexpr int UMMA_K = 16;       // K per tcgen05.mma of kind::f16
+constexpr int kEpiWarps = 4;
+constexpr int kThreads = 32 * (kEpiWarps + 2);
+constexpr uint64_t kWaitNs = 2000000000ull;   // 2 s bound on any barrier wait
+
+// ------------------------------------------------------------ PTX helpers
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ uint64_t globaltimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: returns false (and records `code`) when the deadline passes
+// or another thread of the grid already failed.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer();
+  uint32_t spins = 0;
+  while (true) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((++spins & 255u) == 0) {
+      if (*(volatile int*)err != 0) return false;
+      if (globaltimer() - t0 > kWaitNs) {
+        atomicCAS(err, 0, code);
+        return false;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1, int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
+      ::"r"(smem_addr(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_addr(bar)), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// K-major operand tile, rows of 128 bytes, 128B swizzle, 8-row groups 1024 B apart.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+      ::"r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(acc)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// ------------------------------------------------------------ GEMM kernel
+
+template <int PIECES, int STAGES>
+__global__ void __launch_bounds__(kThreads, 1)
+tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+               const int64_t M, const int n_out, const int n_tile, const int kblocks,
+               double* __restrict__ out, const int64_t ldo, int* __restrict__ err) {
+  constexpr int NPROD = PIECES == 3 ? 6 : 3;
+  constexpr int A_TILE = BM * BK * 2;             // bytes of one A piece tile
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  // 1024-byte aligned base for the swizzled tiles
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const int B_TILE = n_tile * BK * 2;
+  const int STAGE = PIECES * (A_TILE + B_TILE);
+  uint64_t* full = (uint64_t*)(smem + STAGES * STAGE);
+  uint64_t* empty = full + STAGES;
+  uint64_t* acc_full = empty + STAGES;
+  uint32_t* tmem_slot = (uint32_t*)(acc_full + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t m0 = (int64_t)blockIdx.x * BM;
+  const int n0 = blockIdx.y * n_tile;
+  uint32_t tmem_cols = 32;
+  while ((int)tmem_cols < n_tile) tmem_cols <<= 1;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(acc_full, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == kEpiWarps + 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
+                 "r"(tmem_cols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == kEpiWarps) {
+    // ---------------- TMA producer
+    if (lane == 0) {
+      for (int kb = 0; kb < kblocks; ++kb) {
+        const int s = kb % STAGES;
+        const uint32_t phase = (uint32_t)(kb / STAGES) & 1u;
+        if (!mbar_wait(&empty[s], phase ^ 1u, err, 1)) break;
+        uint8_t* st = smem + s * STAGE;
+        mbar_expect_tx(&full[s], (uint32_t)STAGE);
+        for (int p = 0; p < PIECES; ++p) {
+          tma_load_3d(st + p * A_TILE, &tmA, &full[s], kb * BK, (int)m0, p);
+          tma_load_3d(st + PIECES * A_TILE + p * B_TILE, &tmB, &full[s], kb * BK, n0, p);
+        }
+      }
+    }
+  } else if (warp == kEpiWarps + 1) {
+    // ---------------- MMA issuer
+    if (lane == 0) {
+      const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n_tile >> 3) << 17) |
+                             ((uint32_t)(BM >> 4) << 24);
+      // products (i, j) with i + j < PIECES, smallest terms first
+      constexpr int pa3[6] = {2, 1, 0, 1, 0, 0}, pb3[6] = {0, 1, 2, 0, 1, 0};
+      constexpr int pa2[3] = {1, 0, 0}, pb2[3] = {0, 1, 0};
+      bool ok = true;
+      for (int kb = 0; kb < kblocks && ok; ++kb) {
+        const int s = kb % STAGES;
+        const uint32_t phase = (uint32_t)(kb / STAGES) & 1u;
+        if (!mbar_wait(&full[s], phase, err, 2)) { ok = false; break; }
+        tc_fence_after();
+        const uint32_t base = smem_addr(smem + s * STAGE);
+        for (int kk = 0; kk < BK / UMMA_K; ++kk) {
+#pragma unroll
+          for (int t = 0; t < NPROD; ++t) {
+            const int ia = PIECES == 3 ? pa3[t] : pa2[t];
+            const int ib = PIECES == 3 ? pb3[t] : pb2[t];
+            const uint32_t a_addr = base + ia * A_TILE + kk * UMMA_K * 2;
+            const uint32_t b_addr = base + PIECES * A_TILE + ib * B_TILE + kk * UMMA_K * 2;
+            umma_bf16(tmem, smem_desc(a_addr), smem_desc(b_addr), idesc, (kb | kk | t) != 0);
+          }
+        }
+        umma_commit(&empty[s]);
+      }
+      umma_commit(acc_full);
+    }
+  } else {
+    // ---------------- epilogue (warps 0..3, TMEM lanes 32*warp ..)
+    bool ok = mbar_wait(acc_full, 0, err, 3);
+    ok = __all_sync(0xffffffffu, ok && *(volatile int*)err == 0);   // warp-uniform for tcgen05.ld
+    tc_fence_after();
+    if (ok) {
+      double* stage = (double*)smem + warp * 32 * 16;     // [32 rows][16 cols] per warp; stages are idle now
+      const int row_base = warp * 32;
+      for (int c0 = 0; c0 < n_tile; c0 += 16) {
+        uint32_t r[16];
+        tmem_ld16(tmem + ((uint32_t)row_base << 16) + (uint32_t)c0, r);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) stage[lane * 16 + ((j + lane) & 15)] = (double)__uint_as_float(r[j]);
+        __syncwarp();
+        // two rows per pass: lanes 0-15 row 2q, lanes 16-31 row 2q+1
+        for (int q = 0; q < 16; ++q) {
+          const int rr = 2 * q + (lane >> 4);
+          const int cc = lane & 15;
+          const int64_t row = m0 + row_base + rr;
+          const int col = n0 + c0 + cc;
+          if (row < M && col < n_out) out[row * ldo + col] = stage[rr * 16 + ((cc + rr) & 15)];
+        }
+        __syncwarp();
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == kEpiWarps + 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols));
+  }
+}
+
+// ------------------------------------------------------------ A pieces
+
+// bf16 round-to-nearest split of an FP32 value into `pieces` terms.
+template <int PIECES>
+__device__ __forceinline__ void split_bf16(float v, __nv_bfloat16 (&o)[3]) {
+  const __nv_bfloat16 h = __float2bfloat16_rn(v);
+  o[0] = h;
+  float r = v - __bfloat162float(h);
+  const __nv_bfloat16 m = __float2bfloat16_rn(r);
+  o[1] = m;
+  if (PIECES == 3) {
+    r = r - __bfloat162float(m);
+    o[2] = __float2bfloat16_rn(r);
+  }
+}
+
+constexpr int kAoWarps = 8;
+
+struct MixSmem {
+  float rad[kBlockSlots][5];
+  double nuc[kBlockNuc][4];
+};
+
+// Mixed-form AO VGL: radial part with FP64 displacement, r^2, exponent
+// argument, radial Laplacian factor and FP64 accumulation (FP32 exponential
+// when a r^2 <= 30, FP64 above); monomials and the product rule in FP32; the
+// five components of each AO written as bf16 pieces of rows p*comps + c.
+template <int PIECES, int COMPS>
+__global__ void __launch_bounds__(kAoWarps * 32)
+ao_split_kernel(const DevTables T, const int64_t point_num, const double* __restrict__ coord, const double cutoff,
+                __nv_bfloat16* __restrict__ a, const int64_t lda, const int64_t piece_stride) {
+  __shared__ MixSmem smem[kAoWarps];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  MixSmem& sm = smem[warp];
+  const int64_t items = point_num * (int64_t)T.nblock;
+  const int64_t stride = (int64_t)gridDim.x * kAoWarps;
+  for (int64_t it = (int64_t)blockIdx.x * kAoWarps + warp; it < items; it += stride) {
+    const int64_t p = it / T.nblock;
+    const int b = (int)(it - p * T.nblock);
+    const int4 blk = T.block[b];
+    const int2 slots = T.block_slots[b];
+    const double px = coord[p], py = coord[p + point_num], pz = coord[p + 2 * point_num];
+    const int nn = blk.y - blk.x;
+    if (lane < nn) {
+      const int n = blk.x + lane;
+      const int N = T.nucl_num;
+      const double x = px - T.nucl_coord[n];
+      const double y = py - T.nucl_coord[n + N];
+      const double z = pz - T.nucl_coord[n + 2 * N];
+      const double r2 = x * x + y * y + z * z;
+      sm.nuc[lane][0] = x;
+      sm.nuc[lane][1] = y;
+      sm.nuc[lane][2] = z;
+      sm.nuc[lane][3] = (r2 > cutoff * T.nucleus_range[n]) ? -1.0 : r2;
+    }
+    __syncwarp();
+    for (int s = slots.x + lane; s < slots.y; s += 32) {
+      const int nucl = T.slot_nuc[s];
+      const int nl = nucl - blk.x;
+      const double r2 = sm.nuc[nl][3];
+      double acc[5] = {0., 0., 0., 0., 0.};
+      if (r2 >= 0.0) {
+        const double x = sm.nuc[nl][0], y = sm.nuc[nl][1], z = sm.nuc[nl][2];
+        const int2 cr = T.slot_coef[s];
+        const int p0 = T.nuc_prim_start[nucl];
+        for (int j = cr.x; j < cr.y; ++j) {
+          const double al = T.expo[p0 + T.coef_prim[j]];
+          const double ar2 = al * r2;
+          if (ar2 > cutoff) break;
+          const double e = ar2 > 30.0 ? exp(-ar2) : (double)expf(-(float)ar2);
+          const double cv = T.coef_val[j];
+          acc[0] += cv * e;
+          if (COMPS == 5) {
+            const double f = -2.0 * al * e;
+            acc[1] += cv * (f * x);
+            acc[2] += cv * (f * y);
+            acc[3] += cv * (f * z);
+            acc[4] += cv * (f * (3.0 - 2.0 * ar2));
+          }
+        }
+      }
+      const int ls = s - slots.x;
+#pragma unroll
+      for (int c = 0; c < 5; ++c) sm.rad[ls][c] = (float)acc[c];
+    }
+    __syncwarp();
+    for (int k = blk.z + lane; k < blk.w; k += 32) {
+      const int code = T.ao_code[k];
+      const int ax = code & 15, by = (code >> 4) & 15, cz = (code >> 8) & 15, l = (code >> 12) & 15;
+      const int slot = (code >> 16) & 255, nl = (code >> 24) & 31;
+      float v[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+      const float s1 = sm.rad[slot][0];
+      if (sm.nuc[nl][3] >= 0.0 && s1 != 0.0f) {
+        const float f = (float)T.ao_factor[k];
+        const float s2 = sm.rad[slot][1], s3 = sm.rad[slot][2], s4 = sm.rad[slot][3], s5 = sm.rad[slot][4];
+        if (l == 0) {
+          v[0] = s1 * f; v[1] = s2 * f; v[2] = s3 * f; v[3] = s4 * f; v[4] = s5 * f;
+        } else {
+          const float x = (float)sm.nuc[nl][0], y = (float)sm.nuc[nl][1], z = (float)sm.nuc[nl][2];
+          float P0, P1, P2, P3, P4;
+          if (l == 1) {
+            P0 = ax ? x : (by ? y : z);
+            P1 = (float)ax; P2 = (float)by; P3 = (float)cz; P4 = 0.f;
+          } else {
+            float pa = 1.f, pb = 1.f, pc = 1.f, pa1 = 1.f, pb1 = 1.f, pc1 = 1.f, pa2 = 1.f, pb2 = 1.f, pc2 = 1.f;
+            for (int i = 0; i < ax; ++i) { pa2 = pa1; pa1 = pa; pa *= x; }
+            for (int i = 0; i < by; ++i) { pb2 = pb1; pb1 = pb; pb *= y; }
+            for (int i = 0; i < cz; ++i) { pc2 = pc1; pc1 = pc; pc *= z; }
+            if (ax < 2) pa2 = 1.f;
+            if (by < 2) pb2 = 1.f;
+            if (cz < 2) pc2 = 1.f;
+            float xy = pa * pb, yz = pb * pc, xz = pa * pc;
+            P0 = xy * pc;
+            xy *= (float)cz; xz *= (float)by; yz *= (float)ax;
+            P1 = pa1 * yz; P2 = pb1 * xz; P3 = pc1 * xy;
+            P4 = (float)(ax - 1) * pa2 * yz + (float)(by - 1) * pb2 * xz + (float)(cz - 1) * pc2 * xy;
+          }
+          v[0] = P0 * s1 * f;
+          v[1] = (P1 * s1 + P0 * s2) * f;
+          v[2] = (P2 * s1 + P0 * s3) * f;
+          v[3] = (P3 * s1 + P0 * s4) * f;
+          v[4] = (P4 * s1 + P0 * s5 + 2.f * (P1 * s2 + P2 * s3 + P3 * s4)) * f;
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < COMPS; ++c) {
+        __nv_bfloat16 pcs[3];
+        split_bf16<PIECES>(v[c], pcs);
+        const int64_t off = (p * COMPS + c) * lda + k;
+#pragma unroll
+        for (int q = 0; q < PIECES; ++q) a[q * piece_stride + off] = pcs[q];
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// ------------------------------------------------------------ host side
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  return fn;
+}
+
+// 3-D bf16 map {K, rows, pieces}, box {64, box_rows, 1}, 128B swizzle.
+bool make_map(CUtensorMap* map, const void* base, int64_t k, int64_t rows, int64_t ld, int pieces, int64_t piece_stride,
+              int box_rows) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[3] = {(cuuint64_t)k, (cuuint64_t)rows, (cuuint64_t)pieces};
+  cuuint64_t strides[2] = {(cuuint64_t)(ld * 2), (cuuint64_t)(piece_stride * 2)};
+  cuuint32_t box[3] = {(cuuint32_t)BK, (cuuint32_t)box_rows, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+int sm_count() {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
+}
+
+// One error word per device, allocated on first use and kept for the process.
+int* err_word() {
+  static int* words[64] = {nullptr};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  if (!words[dev]) {
+    int* d = nullptr;
+    if (cudaMalloc(&d, sizeof(int)) != cudaSuccess) return nullptr;
+    if (cudaMemset(d, 0, sizeof(int)) != cudaSuccess) return nullptr;
+    words[dev] = d;
+  }
+  return words[dev];
+}
+
+template <int PIECES, int STAGES>
+cudaError_t launch_gemm(const CUtensorMap& ta, const CUtensorMap& tb, int64_t M, int n_out, int n_tile, int n_tiles,
+                        int kblocks, double* out, int64_t ldo, int* err, cudaStream_t s) {
+  const size_t stage = (size_t)PIECES * (BM * BK * 2 + (size_t)n_tile * BK * 2);
+  const size_t smem = 1024 + STAGES * stage + (2 * STAGES + 1) * 8 + 16;
+  auto kern = tc_gemm_kernel<PIECES, STAGES>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid((unsigned)((M + BM - 1) / BM), (unsigned)n_tiles);
+  kern<<<grid, kThreads, smem, s>>>(ta, tb, M, n_out, n_tile, kblocks, out, ldo, err);
+  count_launch();
+  return cudaGetLastError();
+}
+
+}  // namespace
+
 TcPlan tc_plan(int64_t ao_num, int64_t mo_num, int pieces) {
   TcPlan p;
-  p.ao_num = ao_num; p.mo_num = mo_num; p.pieces = pieces;
-  p.k_pad = (ao_num + 63) / 64 * 64;
-  p.n_pad = (mo_num + 15) / 16 * 16;
+  p.ao_num = ao_num;
+  p.mo_num = mo_num;
+  p.pieces = pieces;
+  p.k_pad = (ao_num + BK - 1) / BK * BK;
+  // N tiles of at most 256 columns (one tcgen05.mma N), multiples of 16
+  p.n_tiles = (int)((mo_num + 255) / 256);
+  const int64_t per = (mo_num + p.n_tiles - 1) / p.n_tiles;
+  p.n_tile = (int)((per + 15) / 16 * 16);
+  // the pipeline stages (pieces x (A 16 KB + B n_tile*128 B), 2 stages for 3
+  // pieces, 3 for 2) must fit in 227 KB of shared memory: n_tile <= 160
+  while (p.n_tile > 160) {
+    p.n_tiles += 1;
+    const int64_t q = (mo_num + p.n_tiles - 1) / p.n_tiles;
+    p.n_tile = (int)((q + 15) / 16 * 16);
+  }
+  p.n_pad = (int64_t)p.n_tile * p.n_tiles;
   p.coef_bytes = (size_t)pieces * p.n_pad * p.k_pad * 2;
   return p;
 }
-size_t tc_a_bytes(const TcPlan& plan, int64_t rows) { return (size_t)plan.pieces * rows * plan.k_pad * 2; }
-cudaError_t tc_prepare_coef(const TcPlan&, const double*, void*, cudaStream_t) { return cudaErrorNotSupported; }
-cudaError_t tc_run(const DevTables&, const TcPlan&, int64_t, int, const double*, double, const void*, void*, double*,
-                   cudaStream_t) {
-  return cudaErrorNotSupported;
+
+size_t tc_a_bytes(const TcPlan& plan, int64_t rows) { return (size_t)plan.pieces * (size_t)rows * plan.k_pad * 2; }
+
+cudaError_t tc_prepare_coef(const TcPlan& plan, const double* coefficient_host, void* d_coef, cudaStream_t s) {
+  const int64_t A = plan.ao_num, M = plan.mo_num, KP = plan.k_pad, NP = plan.n_pad;
+  std::vector<uint16_t> h((size_t)plan.pieces * NP * KP, 0);
+  auto to_bf16 = [](double x) -> uint16_t {   // round to nearest even of the FP32 rounding
+    float f = (float)x;
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    if ((u & 0x7f800000u) == 0x7f800000u) return (uint16_t)(u >> 16);
+    u += 0x7fffu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+  };
+  auto from_bf16 = [](uint16_t b) -> double {
+    uint32_t u = (uint32_t)b << 16;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return (double)f;
+  };
+  for (int64_t i = 0; i < M; ++i)
+    for (int64_t k = 0; k < A; ++k) {
+      double r = coefficient_host[i * A + k];
+      for (int p = 0; p < plan.pieces; ++p) {
+        const uint16_t b = to_bf16(r);
+        h[((size_t)p * NP + i) * KP + k] = b;
+        r -= from_bf16(b);
+      }
+    }
+  cudaError_t e = cudaMemcpyAsync(d_coef, h.data(), h.size() * 2, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return e;
+  return cudaStreamSynchronize(s);   // the host staging buffer goes out of scope
+}
+
+cudaError_t tc_run(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps, const double* coord,
+                   double cutoff, const void* d_coef, void* d_a, double* out, cudaStream_t s) {
+  if (point_num <= 0) return cudaSuccess;
+  const int64_t rows = (int64_t)comps * point_num;
+  const int64_t lda = plan.k_pad;
+  const int64_t pstride = rows * lda;
+  __nv_bfloat16* a = (__nv_bfloat16*)d_a;
+  // 1) AO pieces
+  {
+    const int64_t items = point_num * T.nblock;
+    const int grid = (int)std::min<int64_t>((items + kAoWarps - 1) / kAoWarps, (int64_t)sm_count() * 8);
+    if (plan.pieces == 3) {
+      if (comps == 5) ao_split_kernel<3, 5><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, a, lda, pstride);
+      else ao_split_kernel<3, 1><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, a, lda, pstride);
+    } else {
+      if (comps == 5) ao_split_kernel<2, 5><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, a, lda, pstride);
+      else ao_split_kernel<2, 1><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, a, lda, pstride);
+    }
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  // 2) tensor-core contraction
+  CUtensorMap ta, tb;
+  if (!make_map(&ta, a, plan.ao_num, rows, lda, plan.pieces, pstride, BM)) return cudaErrorInvalidValue;
+  if (!make_map(&tb, d_coef, plan.ao_num, plan.n_pad, plan.k_pad, plan.pieces, plan.n_pad * plan.k_pad, plan.n_tile))
+    return cudaErrorInvalidValue;
+  int* err = err_word();
+  if (!err) return cudaErrorMemoryAllocation;
+  const int kblocks = (int)((plan.ao_num + BK - 1) / BK);
+  cudaError_t e;
+  if (plan.pieces == 3)
+    e = launch_gemm<3, 2>(ta, tb, rows, (int)plan.mo_num, plan.n_tile, plan.n_tiles, kblocks, out, plan.mo_num, err, s);
+  else
+    e = launch_gemm<2, 3>(ta, tb, rows, (int)plan.mo_num, plan.n_tile, plan.n_tiles, kblocks, out, plan.mo_num, err, s);
+  if (e != cudaSuccess) return e;
+  // surface a timed-out barrier wait as an error (the word is cleared for the next call)
+  int h = 0;
+  e = cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e != cudaSuccess) return e;
+  e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return e;
+  if (h != 0) {
+    cudaMemsetAsync(err, 0, sizeof(int), s);
+    return cudaErrorLaunchTimeout;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace qb

@@ -1,0 +1,99 @@
+"""Mixed form (FP32 AOs, split-BF16 tcgen05 MO contraction) against the FP64 oracle (GPU)."""
+import numpy as np
+import pytest
+
+from conftest import comp_error
+from oracle import pyoracle as O
+from qmckl_b200 import gen
+from qmckl_b200 import qmckl as pq
+from qmckl_b200.system import make_context
+
+pytestmark = pytest.mark.gpu
+
+MIXED_TOL = 1e-6       # max |mixed - fp64| / max |fp64| per component, 3 bf16 pieces
+MIXED2_TOL = 1e-4      # same bar for 2 pieces (3 products): ~2^-16 representation error
+
+
+def _mo_ref(d):
+    ao = O.ao_vgl(O.Basis(d), gen.points(d), d["nucl_coord"])
+    return O.mo_vgl(d["mo_coef"], ao), ao
+
+
+@pytest.mark.parametrize("pieces,tol", [(3, MIXED_TOL), (2, MIXED2_TOL)])
+def test_mixed_mo_vgl_chbrclf(chbrclf, pieces, tol):
+    ctx = make_context(chbrclf, form=pq.FORM_MIXED)
+    pq.b200_set_split_terms(ctx, pieces)
+    P, M = 136, 224
+    mo = pq.get_mo_basis_mo_vgl(ctx, P * 5 * M).reshape(P, 5, M)
+    ref, _ = _mo_ref(chbrclf)
+    err = comp_error(mo, ref)
+    assert max(err) < tol, err
+    pq.context_destroy(ctx)
+
+
+def test_mixed_mo_value_chbrclf(chbrclf):
+    ctx = make_context(chbrclf, form=pq.FORM_MIXED)
+    P, M = 136, 224
+    mv = pq.get_mo_basis_mo_value(ctx, P * M).reshape(P, M)
+    ref, _ = _mo_ref(chbrclf)
+    assert np.abs(mv - ref[:, 0, :]).max() / np.abs(ref[:, 0, :]).max() < MIXED_TOL
+    pq.context_destroy(ctx)
+
+
+@pytest.mark.parametrize("cid,walkers", [(0, 64), (1, 4)])
+def test_mixed_configs(cid, walkers):
+    d = gen.config(cid, walk_num=walkers)
+    ctx = make_context(d, form=pq.FORM_MIXED)
+    P = d["elec_coord"].shape[0] * d["elec_coord"].shape[1]
+    M = d["mo_num"]
+    mo = pq.get_mo_basis_mo_vgl(ctx, P * 5 * M).reshape(P, 5, M)
+    ref, _ = _mo_ref(d)
+    err = comp_error(mo, ref)
+    assert max(err) < MIXED_TOL, err
+    pq.context_destroy(ctx)
+
+
+def test_mixed_matches_fp64_gpu_on_config1_walkers():
+    """Mixed vs the FP64 GPU form on 32 walkers of the config-1 molecule (10,176 points)."""
+    d = gen.config(1, walk_num=32)
+    P = d["elec_coord"].shape[0] * d["elec_coord"].shape[1]
+    M = d["mo_num"]
+    c64 = make_context(d, form=pq.FORM_FP64)
+    c32 = make_context(d, form=pq.FORM_MIXED)
+    a = pq.get_mo_basis_mo_vgl(c64, P * 5 * M).reshape(P, 5, M)
+    b = pq.get_mo_basis_mo_vgl(c32, P * 5 * M).reshape(P, 5, M)
+    assert max(comp_error(b, a)) < MIXED_TOL
+    pq.context_destroy(c64)
+    pq.context_destroy(c32)
+
+
+def test_mixed_device_entry_and_ragged_rows(chbrclf):
+    """Point counts whose 5*P rows end mid-tile (128-row tiles) and N tiles of the 224 MOs."""
+    import torch
+    ctx = make_context(chbrclf, points=False, form=pq.FORM_MIXED)
+    for npts in (1, 25, 26, 131):
+        pts = gen.points(chbrclf)[:npts]
+        dc = torch.tensor(np.ascontiguousarray(pts.T), dtype=torch.float64, device="cuda")
+        mo = torch.full((npts * 5 * 224,), float("nan"), dtype=torch.float64, device="cuda")
+        pq.b200_mo_vgl_device(ctx, npts, dc.data_ptr(), mo.data_ptr())
+        pq.b200_synchronize(ctx)
+        got = mo.cpu().numpy().reshape(npts, 5, 224)
+        ao = O.ao_vgl(O.Basis(chbrclf), pts, chbrclf["nucl_coord"])
+        ref = O.mo_vgl(chbrclf["mo_coef"], ao)
+        assert np.isfinite(got).all()
+        assert max(comp_error(got, ref)) < MIXED_TOL
+    pq.context_destroy(ctx)
+
+
+def test_auto_form_follows_precision(chbrclf):
+    """AUTO: FP64 at precision 53, mixed at precision <= 26."""
+    P, M = 136, 224
+    c1 = make_context(chbrclf)
+    m1 = pq.get_mo_basis_mo_vgl(c1, P * 5 * M).reshape(P, 5, M)
+    c2 = make_context(chbrclf, precision=26)
+    m2 = pq.get_mo_basis_mo_vgl(c2, P * 5 * M).reshape(P, 5, M)
+    ref, _ = _mo_ref(chbrclf)
+    assert max(comp_error(m1, ref)) < 1e-13
+    assert 1e-13 < max(comp_error(m2, ref)) < 1e-4
+    pq.context_destroy(c1)
+    pq.context_destroy(c2)
