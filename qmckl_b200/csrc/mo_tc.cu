@@ -9,6 +9,10 @@
 // coefficient update.  Products X_i*Y_j with i + j < pieces are accumulated
 // in FP32 in tensor memory: 3 products for 2 pieces (error ~2^-16 relative),
 // 6 products for 3 pieces (~2^-24, below the FP32 rounding of the AOs).
+// The rounding of the FP32 accumulation grows with the number of
+// accumulation steps, so the leading product A1*C1 is accumulated in two
+// accumulators (first and second half of K) and the correction products,
+// 2^-8 smaller, in a third; the epilogue adds the three in FP64.
 //
 // GEMM kernel (one 128 x n_tile output tile per CTA):
 //   warp 4      TMA producer: all A and C pieces of a 64-wide K block into a
@@ -149,8 +153,10 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t m0 = (int64_t)blockIdx.x * BM;
   const int n0 = blockIdx.y * n_tile;
+  // three accumulators of n_tile columns: A1*C1 (first half of K), A1*C1
+  // (second half), corrections
   uint32_t tmem_cols = 32;
-  while ((int)tmem_cols < n_tile) tmem_cols <<= 1;
+  while ((int)tmem_cols < 3 * n_tile) tmem_cols <<= 1;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
@@ -208,7 +214,12 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
             const int ib = PIECES == 3 ? pb3[t] : pb2[t];
             const uint32_t a_addr = base + ia * A_TILE + kk * UMMA_K * 2;
             const uint32_t b_addr = base + PIECES * A_TILE + ib * B_TILE + kk * UMMA_K * 2;
-            umma_bf16(tmem, smem_desc(a_addr), smem_desc(b_addr), idesc, (kb | kk | t) != 0);
+            const bool lead = (t == NPROD - 1);                 // A1*C1
+            const bool second = lead && (2 * kb >= kblocks);
+            const uint32_t d = tmem + (uint32_t)((lead ? (second ? 1 : 0) : 2) * n_tile);
+            const bool first_use = lead ? (second ? (kb == (kblocks + 1) / 2 && kk == 0) : (kb == 0 && kk == 0))
+                                        : (kb == 0 && kk == 0 && t == 0);
+            umma_bf16(d, smem_desc(a_addr), smem_desc(b_addr), idesc, first_use ? 0u : 1u);
           }
         }
         umma_commit(&empty[s]);
@@ -223,11 +234,19 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     if (ok) {
       double* stage = (double*)smem + warp * 32 * 16;     // [32 rows][16 cols] per warp; stages are idle now
       const int row_base = warp * 32;
+      const bool has_second = kblocks >= 2;
       for (int c0 = 0; c0 < n_tile; c0 += 16) {
-        uint32_t r[16];
-        tmem_ld16(tmem + ((uint32_t)row_base << 16) + (uint32_t)c0, r);
+        uint32_t r0[16], r1[16], r2[16];
+        const uint32_t ta = tmem + ((uint32_t)row_base << 16) + (uint32_t)c0;
+        tmem_ld16(ta, r0);
+        tmem_ld16(ta + (uint32_t)n_tile, r1);
+        tmem_ld16(ta + (uint32_t)(2 * n_tile), r2);
 #pragma unroll
-        for (int j = 0; j < 16; ++j) stage[lane * 16 + ((j + lane) & 15)] = (double)__uint_as_float(r[j]);
+        for (int j = 0; j < 16; ++j) {
+          double v = (double)__uint_as_float(r0[j]) + (double)__uint_as_float(r2[j]);
+          if (has_second) v += (double)__uint_as_float(r1[j]);
+          stage[lane * 16 + ((j + lane) & 15)] = v;
+        }
         __syncwarp();
         // two rows per pass: lanes 0-15 row 2q, lanes 16-31 row 2q+1
         for (int q = 0; q < 16; ++q) {
