@@ -60,6 +60,37 @@ qmckl_exit_code qmckl_b200_mo_vgl_device(qmckl_context context, const int64_t po
 qmckl_exit_code qmckl_b200_mo_value_device(qmckl_context context, const int64_t point_num,
                                            const double* d_coord, double* d_mo_value);
 
+/* Mixed-form MO VGL that allocates no device memory.  No counterpart in the
+ * reference library.
+ *
+ * For callers that cannot allocate device memory when they evaluate the
+ * orbitals: codes whose device memory is held by a pool allocator that has
+ * already reserved the free memory (cudaMalloc would fail), work issued from
+ * a CUDA host callback (where allocating CUDA calls are not permitted), or
+ * time-step loops that cannot take the device synchronization of
+ * cudaMalloc/cudaFree.  Same arguments, result and arithmetic as
+ * qmckl_b200_mo_vgl_device in the mixed form (it always evaluates the mixed
+ * form, whatever qmckl_b200_set_form says), but the scratch it needs lives in
+ * one fixed 32 MiB array inside the library, held by every GPU that loads the
+ * library until the process exits.  The caller passes the coordinates and the
+ * output buffer (device memory).
+ *   - Limit: point_num * 5 rows of the AO matrix in 3 (or 2) bfloat16 pieces
+ *     of ao_num rounded up to 64 columns must fit in the 32 MiB; larger
+ *     point_num is rejected with QMCKL_INVALID_ARG_2 and a message giving the
+ *     largest point count for the basis (546 points for 2000 AOs, 3 pieces).
+ *   - The basis tables and the split MO coefficients must already be on the
+ *     device: run one regular mixed-form evaluation of the context first (that
+ *     one allocates); otherwise QMCKL_NOT_PROVIDED.
+ *   - The first call on a device looks up the array's device address (once
+ *     per device); make that first call before any stream capture.
+ *   - Every call uses the same array and it keeps the previous call's
+ *     contents; the timeout word is cleared at the start of each call.  Calls
+ *     whose GPU work overlaps (other streams, other host threads, other
+ *     contexts) race on the array: order them on one stream.
+ *   - The call synchronizes the context's stream before returning. */
+qmckl_exit_code qmckl_b200_mo_vgl_device_noalloc(qmckl_context context, const int64_t point_num,
+                                                 const double* d_coord, double* d_mo_vgl);
+
 /* Number of kernels this library launched since the process started. */
 int64_t qmckl_b200_kernel_launch_count(void);
 

@@ -389,6 +389,37 @@ void dev_detach(Context* ctx) {
   ctx->extra = nullptr;
 }
 
+// The device data a fixed-scratch evaluation needs, without allocating: the
+// basis tables and split coefficients must already be on the device (any
+// regular mixed evaluation of the context puts them there); nuclear
+// coordinates moved since then are copied into their existing buffer.
+qmckl_exit_code dev_prepared_mixed(qmckl_context context, PreparedMixed* out) {
+  Context* ctx = ctx_of(context);
+  DeviceState* ds = ctx->extra;
+  const char* fname = "qmckl_b200_mo_vgl_device_noalloc";
+  if (ds == nullptr || ds->tables.p == nullptr || ds->basis_version != ctx->ao_basis.basis_version ||
+      ds->tc_coef.p == nullptr || ds->tc_coef_version != ctx->mo_basis.coef_version ||
+      ds->tc_pieces != ds->split_pieces || (ds->stream == nullptr && !ds->stream_given))
+    return qmckl_failwith(context, QMCKL_NOT_PROVIDED, fname,
+                          "basis or MO coefficients not on the device yet: run one regular mixed-form "
+                          "evaluation of this context first");
+  if (ds->device >= 0) QB_CUDA(cudaSetDevice(ds->device), fname);
+  if (ds->nucl_version != ctx->nucleus.coord_version) {
+    const size_t bytes = sizeof(double) * 3 * ctx->nucleus.num;
+    if (ds->nucl.p == nullptr || ds->nucl.cap < bytes)
+      return qmckl_failwith(context, QMCKL_NOT_PROVIDED, fname, "nuclear coordinates not on the device yet");
+    QB_CUDA(cudaMemcpyAsync(ds->nucl.p, ctx->nucleus.coord.data(), bytes, cudaMemcpyHostToDevice, ds->stream), fname);
+    ds->nucl_version = ctx->nucleus.coord_version;
+  }
+  out->T = ds->T;
+  out->T.nucl_coord = (const double*)ds->nucl.p;
+  out->plan = ds->tc;
+  out->coef = ds->tc_coef.p;
+  out->stream = ds->stream;
+  out->cutoff = cutoff_of(ctx);
+  return QMCKL_SUCCESS;
+}
+
 qmckl_exit_code dev_invalidate_mo(qmckl_context context) {
   DeviceState* ds = state(context);
   if (ds) { ds->coef_version = ~0ull; ds->tc_coef_version = ~0ull; }

@@ -134,6 +134,8 @@ qmckl_exit_code dev_provide_ao_value(qmckl_context context, double* host_out);
 qmckl_exit_code dev_provide_mo_vgl(qmckl_context context, double* host_out);
 qmckl_exit_code dev_provide_mo_value(qmckl_context context, double* host_out);
 qmckl_exit_code dev_invalidate_mo(qmckl_context context);
+struct PreparedMixed;
+qmckl_exit_code dev_prepared_mixed(qmckl_context context, PreparedMixed* out);
 
 // AO finalization helpers (ao_basis.cpp)
 qmckl_exit_code finalize_basis(qmckl_context context);

@@ -575,4 +575,44 @@ cudaError_t tc_run(const DevTables& T, const TcPlan& plan, int64_t point_num, in
   return cudaSuccess;
 }
 
+cudaError_t tc_run_scratch(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps,
+                           const double* coord, double cutoff, const void* d_coef, void* d_a, int* d_err,
+                           double* out, cudaStream_t s) {
+  if (point_num <= 0) return cudaSuccess;
+  cudaError_t e = cudaMemsetAsync(d_err, 0, sizeof(int), s);
+  if (e != cudaSuccess) return e;
+  const int64_t rows = (int64_t)comps * point_num;
+  const int64_t lda = plan.k_pad;
+  const int64_t pstride = rows * lda;
+  __nv_bfloat16* a = (__nv_bfloat16*)d_a;
+  const int64_t items = point_num * T.nblock;
+  const int grid = (int)std::min<int64_t>((items + kAoWarps - 1) / kAoWarps, (int64_t)sm_count() * 8);
+  if (plan.pieces == 3) {
+    if (comps == 5) ao_split_kernel<3, 5><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, a, lda, pstride);
+    else ao_split_kernel<3, 1><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, a, lda, pstride);
+  } else {
+    if (comps == 5) ao_split_kernel<2, 5><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, a, lda, pstride);
+    else ao_split_kernel<2, 1><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, a, lda, pstride);
+  }
+  count_launch();
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  CUtensorMap ta, tb;
+  if (!make_map(&ta, a, plan.ao_num, rows, lda, plan.pieces, pstride, BM)) return cudaErrorInvalidValue;
+  if (!make_map(&tb, d_coef, plan.ao_num, plan.n_pad, plan.k_pad, plan.pieces, plan.n_pad * plan.k_pad, plan.n_tile))
+    return cudaErrorInvalidValue;
+  const int kblocks = (int)((plan.ao_num + BK - 1) / BK);
+  if (plan.pieces == 3)
+    e = launch_gemm<3, 2>(ta, tb, rows, (int)plan.mo_num, plan.n_tile, plan.n_tiles, kblocks, out, plan.mo_num, d_err, s);
+  else
+    e = launch_gemm<2, 3>(ta, tb, rows, (int)plan.mo_num, plan.n_tile, plan.n_tiles, kblocks, out, plan.mo_num, d_err, s);
+  if (e != cudaSuccess) return e;
+  int h = 0;
+  e = cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e != cudaSuccess) return e;
+  e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return e;
+  return h != 0 ? cudaErrorLaunchTimeout : cudaSuccess;
+}
+
 }  // namespace qb

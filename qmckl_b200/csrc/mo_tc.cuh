@@ -33,4 +33,21 @@ cudaError_t tc_prepare_coef(const TcPlan& plan, const double* coefficient_host, 
 cudaError_t tc_run(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps, const double* coord,
                    double cutoff, const void* d_coef, void* d_a, double* out, cudaStream_t s);
 
+// Same evaluation with caller-provided scratch: the A pieces in d_a and the
+// barrier-timeout word in d_err (cleared here before the launches).  Makes no
+// device allocation.
+cudaError_t tc_run_scratch(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps,
+                           const double* coord, double cutoff, const void* d_coef, void* d_a, int* d_err,
+                           double* out, cudaStream_t s);
+
+// What the fixed-scratch entry point needs from a context whose basis and
+// coefficient pieces are already on the device (device.cu).
+struct PreparedMixed {
+  DevTables T;
+  TcPlan plan;
+  const void* coef = nullptr;
+  cudaStream_t stream = nullptr;
+  double cutoff = 0.0;
+};
+
 }  // namespace qb
