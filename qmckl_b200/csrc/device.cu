@@ -59,6 +59,8 @@ struct DeviceState {
   int tc_pieces = 0;
   DevBuf tc_coef, tc_a;
   int32_t split_pieces = 3;
+  // mixed form: fused AO -> MO kernel instead of AO pieces in device memory + GEMM
+  bool fused = false;
 };
 
 namespace {
@@ -206,6 +208,15 @@ qmckl_exit_code upload_tables(qmckl_context context, DeviceState* ds) {
   const size_t o_pcoef = put(d.coefficient_normalized.data(), sizeof(double) * Pn);
   const size_t o_shnuc = put(shell_nuc.data(), sizeof(int32_t) * S);
   const size_t o_shpr = put(shell_prims.data(), sizeof(int2) * S);
+  std::vector<int32_t> ao_shell(A, 0);
+  std::vector<int2> shell_coef(S);
+  for (int64_t s = 0; s < S; ++s) {
+    shell_coef[s] = make_int2(d.shell_coef_start[s], d.shell_coef_start[s + 1]);
+    const int l = B.shell_ang_mom[s];
+    for (int64_t k = d.ao_index[s]; k < d.ao_index[s] + (l + 1) * (l + 2) / 2 && k < A; ++k) ao_shell[k] = (int32_t)s;
+  }
+  const size_t o_aosh = put(ao_shell.data(), sizeof(int32_t) * A);
+  const size_t o_shco = put(shell_coef.data(), sizeof(int2) * S);
   qmckl_exit_code rc = ensure(context, ds->tables, H.size(), "qmckl_b200_upload_basis");
   if (rc != QMCKL_SUCCESS) return rc;
   QB_CUDA(cudaMemcpyAsync(ds->tables.p, H.data(), H.size(), cudaMemcpyHostToDevice, ds->stream), "qmckl_b200_upload_basis");
@@ -233,6 +244,8 @@ qmckl_exit_code upload_tables(qmckl_context context, DeviceState* ds) {
   T.prim_coef = (const double*)(base + o_pcoef);
   T.shell_nuc = (const int32_t*)(base + o_shnuc);
   T.shell_prims = (const int2*)(base + o_shpr);
+  T.ao_shell = (const int32_t*)(base + o_aosh);
+  T.shell_coef = (const int2*)(base + o_shco);
   ds->basis_version = B.basis_version;
   ds->nucl_version = ~0ull;   // re-point the nuclear coordinates below
   return QMCKL_SUCCESS;
@@ -318,6 +331,12 @@ qmckl_exit_code run_mo_mixed(qmckl_context context, DeviceState* ds, int64_t P, 
     ds->tc = plan;
     ds->tc_coef_version = ctx->mo_basis.coef_version;
     ds->tc_pieces = pieces;
+  }
+  if (ds->fused) {
+    // fused AO -> MO kernel: the AO pieces never leave shared memory
+    QB_CUDA(tc_run_fused(ds->T, ds->tc, P, comps, coord, cutoff_of(ctx), ds->tc_coef.p, out, ds->stream),
+            "qmckl_b200_mo_mixed");
+    return QMCKL_SUCCESS;
   }
   const int64_t rows = (int64_t)comps * P;
   const size_t abytes = tc_a_bytes(ds->tc, rows);
@@ -608,6 +627,14 @@ qmckl_exit_code qmckl_b200_set_split_terms(qmckl_context context, const int32_t 
     qmckl_context_touch(context);
   }
   return QMCKL_SUCCESS;
+}
+
+qmckl_exit_code qmckl_b200_set_mixed_kernel(qmckl_context context, const int32_t fused) {
+  if (qmckl_context_check(context) == QMCKL_NULL_CONTEXT) return QMCKL_INVALID_CONTEXT;
+  qmckl_exit_code rc = dev_attach(context);
+  if (rc != QMCKL_SUCCESS) return rc;
+  state(context)->fused = fused != 0;
+  return qmckl_context_touch(context);
 }
 
 qmckl_exit_code qmckl_b200_set_device(qmckl_context context, const int32_t device) {

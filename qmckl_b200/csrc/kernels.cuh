@@ -38,6 +38,9 @@ struct DevTables {
   const double* prim_coef;        // [prim] normalized coefficient
   const int32_t* shell_nuc;       // [shell]
   const int2* shell_prims;        // [shell] (prim_begin, prim_end)
+  // tables of the fused AO -> MO kernel (global shell numbering)
+  const int32_t* ao_shell;        // [ao] shell of each AO
+  const int2* shell_coef;         // [shell] (begin, end) into coef_prim / coef_val
 };
 
 // Global count of kernels launched by this library.

@@ -33,6 +33,11 @@ cudaError_t tc_prepare_coef(const TcPlan& plan, const double* coefficient_host, 
 cudaError_t tc_run(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps, const double* coord,
                    double cutoff, const void* d_coef, void* d_a, double* out, cudaStream_t s);
 
+// Fused form of tc_run: the AO pieces are produced in shared memory by the
+// GEMM kernel itself and never written to device memory (fused_tc.cu).
+cudaError_t tc_run_fused(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps, const double* coord,
+                         double cutoff, const void* d_coef, double* out, cudaStream_t s);
+
 // Same evaluation with caller-provided scratch: the A pieces in d_a and the
 // barrier-timeout word in d_err (cleared here before the launches).  Makes no
 // device allocation.

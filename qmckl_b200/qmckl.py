@@ -368,6 +368,10 @@ def b200_set_split_terms(ctx, pieces):
     _call("qmckl_b200_set_split_terms", ctx, C.c_int32(pieces))
 
 
+def b200_set_mixed_kernel(ctx, fused):
+    _call("qmckl_b200_set_mixed_kernel", ctx, C.c_int32(1 if fused else 0))
+
+
 def b200_set_stream(ctx, stream_ptr):
     _call("qmckl_b200_set_stream", ctx, C.c_void_p(stream_ptr))
 

@@ -31,8 +31,10 @@ def test_mixed_mo_vgl_chbrclf(chbrclf, pieces, tol):
     pq.context_destroy(ctx)
 
 
-def test_mixed_mo_value_chbrclf(chbrclf):
+@pytest.mark.parametrize("fused", [0, 1])
+def test_mixed_mo_value_chbrclf(chbrclf, fused):
     ctx = make_context(chbrclf, form=pq.FORM_MIXED)
+    pq.b200_set_mixed_kernel(ctx, fused)
     P, M = 136, 224
     mv = pq.get_mo_basis_mo_value(ctx, P * M).reshape(P, M)
     ref, _ = _mo_ref(chbrclf)
@@ -53,13 +55,15 @@ def test_mixed_configs(cid, walkers):
     pq.context_destroy(ctx)
 
 
-def test_mixed_matches_fp64_gpu_on_config1_walkers():
-    """Mixed vs the FP64 GPU form on 32 walkers of the config-1 molecule (10,176 points)."""
+@pytest.mark.parametrize("fused", [0, 1])
+def test_mixed_matches_fp64_gpu_on_config1_walkers(fused):
+    """Mixed (both kernel organisations) vs the FP64 GPU form on 32 walkers of the config-1 molecule."""
     d = gen.config(1, walk_num=32)
     P = d["elec_coord"].shape[0] * d["elec_coord"].shape[1]
     M = d["mo_num"]
     c64 = make_context(d, form=pq.FORM_FP64)
     c32 = make_context(d, form=pq.FORM_MIXED)
+    pq.b200_set_mixed_kernel(c32, fused)
     a = pq.get_mo_basis_mo_vgl(c64, P * 5 * M).reshape(P, 5, M)
     b = pq.get_mo_basis_mo_vgl(c32, P * 5 * M).reshape(P, 5, M)
     assert max(comp_error(b, a)) < MIXED_TOL
