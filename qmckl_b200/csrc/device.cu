@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "internal.h"
+#include "ao_tile.cuh"
 #include "kernels.cuh"
 #include "mo_tc.cuh"
 #include "qmckl_b200.h"
@@ -41,6 +42,7 @@ struct DeviceState {
   uint64_t basis_version = 0;
   DevBuf tables;
   DevTables T{};
+  AoTiles tiles{};
   std::vector<char> host_tables;
   uint64_t nucl_version = ~0ull;
   DevBuf nucl;
@@ -217,6 +219,38 @@ qmckl_exit_code upload_tables(qmckl_context context, DeviceState* ds) {
   }
   const size_t o_aosh = put(ao_shell.data(), sizeof(int32_t) * A);
   const size_t o_shco = put(shell_coef.data(), sizeof(int2) * S);
+  // AO tiles of the tiled kernels (ao_tile.cu)
+  std::vector<int4> tiles;
+  std::vector<int2> tile_nuc;
+  std::vector<int32_t> ao_tcode(A, 0);
+  {
+    bool ordered = true;
+    for (int64_t k = 1; k < A; ++k) ordered = ordered && ao_shell[k] >= ao_shell[k - 1];
+    for (int64_t s = 1; s < S; ++s) ordered = ordered && shell_nuc[s] >= shell_nuc[s - 1];
+    int64_t k = 0;
+    while (ordered && k < A) {
+      int64_t width = 64;
+      for (;;) {
+        const int64_t ke = std::min<int64_t>(k + width, A);
+        const int s0 = ao_shell[k], s1 = ao_shell[ke - 1];
+        const int n0 = shell_nuc[s0], n1 = shell_nuc[s1];
+        if ((s1 - s0 + 1 <= kTileShells && n1 - n0 + 1 <= kTileNuc) || width == 8) {
+          if (s1 - s0 + 1 > kTileShells || n1 - n0 + 1 > kTileNuc) { ordered = false; break; }
+          tiles.push_back(make_int4((int)k, (int)ke, s0, s1 + 1));
+          tile_nuc.push_back(make_int2(n0, n1 + 1));
+          for (int64_t q = k; q < ke; ++q)
+            ao_tcode[q] = (ao_code[q] & 0xFFFF) | ((ao_shell[q] - s0) << 16) | ((shell_nuc[ao_shell[q]] - n0) << 21);
+          k = ke;
+          break;
+        }
+        width /= 2;
+      }
+    }
+    if (!ordered || tiles.size() > 65535) { tiles.clear(); tile_nuc.clear(); }
+  }
+  const size_t o_tile = put(tiles.data(), sizeof(int4) * tiles.size());
+  const size_t o_tnuc = put(tile_nuc.data(), sizeof(int2) * tile_nuc.size());
+  const size_t o_tcode = put(ao_tcode.data(), sizeof(int32_t) * A);
   qmckl_exit_code rc = ensure(context, ds->tables, H.size(), "qmckl_b200_upload_basis");
   if (rc != QMCKL_SUCCESS) return rc;
   QB_CUDA(cudaMemcpyAsync(ds->tables.p, H.data(), H.size(), cudaMemcpyHostToDevice, ds->stream), "qmckl_b200_upload_basis");
@@ -246,6 +280,10 @@ qmckl_exit_code upload_tables(qmckl_context context, DeviceState* ds) {
   T.shell_prims = (const int2*)(base + o_shpr);
   T.ao_shell = (const int32_t*)(base + o_aosh);
   T.shell_coef = (const int2*)(base + o_shco);
+  ds->tiles.ntiles = (int32_t)tiles.size();
+  ds->tiles.tile = (const int4*)(base + o_tile);
+  ds->tiles.tile_nuc = (const int2*)(base + o_tnuc);
+  ds->tiles.ao_tcode = (const int32_t*)(base + o_tcode);
   ds->basis_version = B.basis_version;
   ds->nucl_version = ~0ull;   // re-point the nuclear coordinates below
   return QMCKL_SUCCESS;
@@ -313,7 +351,8 @@ qmckl_exit_code run_ao_vgl(qmckl_context context, DeviceState* ds, int64_t P, co
 
 qmckl_exit_code run_ao_value(qmckl_context context, DeviceState* ds, int64_t P, const double* coord, double* out) {
   Context* ctx = ctx_of(context);
-  QB_CUDA(launch_ao_value_f64(ds->T, P, coord, cutoff_of(ctx), ctx->precision > 23, out, ds->stream), "qmckl_b200_ao_value");
+  QB_CUDA(launch_ao_value_f64(ds->T, P, coord, cutoff_of(ctx), ctx->precision > 23, out, ds->stream),
+          "qmckl_b200_ao_value");
   return QMCKL_SUCCESS;
 }
 
@@ -342,7 +381,8 @@ qmckl_exit_code run_mo_mixed(qmckl_context context, DeviceState* ds, int64_t P, 
   const size_t abytes = tc_a_bytes(ds->tc, rows);
   qmckl_exit_code rc = ensure(context, ds->tc_a, abytes, "qmckl_b200_mo_mixed");
   if (rc != QMCKL_SUCCESS) return rc;
-  QB_CUDA(tc_run(ds->T, ds->tc, P, comps, coord, cutoff_of(ctx), ds->tc_coef.p, ds->tc_a.p, out, ds->stream),
+  QB_CUDA(tc_run(ds->T, ds->tc, P, comps, coord, cutoff_of(ctx), ds->tc_coef.p, ds->tc_a.p, out, ds->stream,
+                 ds->tiles.ntiles > 0 ? &ds->tiles : nullptr),
           "qmckl_b200_mo_mixed");
   return QMCKL_SUCCESS;
 }

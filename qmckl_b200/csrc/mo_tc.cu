@@ -33,6 +33,7 @@
 #include <cstring>
 #include <vector>
 
+#include "ao_tile.cuh"
 #include "mo_tc.cuh"
 #include "tc_ptx.cuh"
 
@@ -444,14 +445,18 @@ cudaError_t tc_prepare_coef(const TcPlan& plan, const double* coefficient_host, 
 }
 
 cudaError_t tc_run(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps, const double* coord,
-                   double cutoff, const void* d_coef, void* d_a, double* out, cudaStream_t s) {
+                   double cutoff, const void* d_coef, void* d_a, double* out, cudaStream_t s,
+                   const AoTiles* tiles) {
   if (point_num <= 0) return cudaSuccess;
   const int64_t rows = (int64_t)comps * point_num;
   const int64_t lda = plan.k_pad;
   const int64_t pstride = rows * lda;
   __nv_bfloat16* a = (__nv_bfloat16*)d_a;
   // 1) AO pieces
-  {
+  if (tiles != nullptr) {
+    cudaError_t e = launch_ao_tile_split(T, *tiles, point_num, coord, cutoff, comps, plan.pieces, a, lda, pstride, s);
+    if (e != cudaSuccess) return e;
+  } else {
     const int64_t items = point_num * T.nblock;
     const int grid = (int)std::min<int64_t>((items + kAoWarps - 1) / kAoWarps, (int64_t)sm_count() * 8);
     if (plan.pieces == 3) {

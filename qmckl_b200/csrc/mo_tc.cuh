@@ -30,8 +30,11 @@ size_t tc_a_bytes(const TcPlan& plan, int64_t rows);
 // coefficient [mo][ao] (host, FP64) -> split bf16 pieces on the device
 cudaError_t tc_prepare_coef(const TcPlan& plan, const double* coefficient_host, void* d_coef, cudaStream_t s);
 // AO (mixed) -> A pieces -> tensor-core GEMM -> out[(point*comps + c)][mo] FP64
+// `tiles` selects the tiled AO kernel (ao_tile.cu) for the pieces when given.
+struct AoTiles;
 cudaError_t tc_run(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps, const double* coord,
-                   double cutoff, const void* d_coef, void* d_a, double* out, cudaStream_t s);
+                   double cutoff, const void* d_coef, void* d_a, double* out, cudaStream_t s,
+                   const AoTiles* tiles = nullptr);
 
 // Fused form of tc_run: the AO pieces are produced in shared memory by the
 // GEMM kernel itself and never written to device memory (fused_tc.cu).
