@@ -37,10 +37,10 @@ qmckl_exit_code qmckl_b200_get_form(const qmckl_context context, int32_t* const 
  * Default 3. */
 qmckl_exit_code qmckl_b200_set_split_terms(qmckl_context context, const int32_t pieces);
 
-/* Kernel organisation of the mixed form: 0 (default) writes the bfloat16 AO
- * pieces to device memory and runs the tensor-core contraction on them;
- * 1 runs the fused kernel that produces the AO pieces in shared memory next
- * to the tensor cores (no AO matrix in device memory). */
+/* Kernel organisation of the mixed form: 1 (default) runs the fused kernel
+ * that produces the bfloat16 AO pieces in shared memory next to the tensor
+ * cores (no AO matrix in device memory); 0 writes the AO pieces to device
+ * memory and runs the tensor-core contraction on them. */
 qmckl_exit_code qmckl_b200_set_mixed_kernel(qmckl_context context, const int32_t fused);
 
 /* The CUDA device and stream (cudaStream_t passed as void*) the context uses.

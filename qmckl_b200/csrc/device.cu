@@ -61,8 +61,14 @@ struct DeviceState {
   int tc_pieces = 0;
   DevBuf tc_coef, tc_a;
   int32_t split_pieces = 3;
-  // mixed form: fused AO -> MO kernel instead of AO pieces in device memory + GEMM
-  bool fused = false;
+  // mixed form: fused AO -> MO kernel (default) instead of AO pieces in device memory + GEMM
+  bool fused = true;
+  // per-K-block records of the fused kernel (rebuilt on basis or nuclear moves)
+  std::vector<int32_t> h_ao_shell, h_ao_code, h_shell_nuc;
+  DevBuf krec;
+  DevBuf order;      // point order of the fused kernel: keys[P], perm[P], cell counts
+  int rec_bytes = 0;
+  uint64_t krec_basis_version = ~0ull, krec_nucl_version = ~0ull;
 };
 
 namespace {
@@ -217,6 +223,9 @@ qmckl_exit_code upload_tables(qmckl_context context, DeviceState* ds) {
     const int l = B.shell_ang_mom[s];
     for (int64_t k = d.ao_index[s]; k < d.ao_index[s] + (l + 1) * (l + 2) / 2 && k < A; ++k) ao_shell[k] = (int32_t)s;
   }
+  ds->h_ao_shell = ao_shell;
+  ds->h_ao_code = ao_code;
+  ds->h_shell_nuc = shell_nuc;
   const size_t o_aosh = put(ao_shell.data(), sizeof(int32_t) * A);
   const size_t o_shco = put(shell_coef.data(), sizeof(int2) * S);
   // AO tiles of the tiled kernels (ao_tile.cu)
@@ -356,6 +365,78 @@ qmckl_exit_code run_ao_value(qmckl_context context, DeviceState* ds, int64_t P, 
   return QMCKL_SUCCESS;
 }
 
+// Records of the fused kernel: one per 64-AO K block, everything its AO
+// producers read (see the layout in fused_tc.cu).  Returns false when the AO
+// numbering does not allow them (then the unfused kernels are used).
+bool build_krec(qmckl_context context, DeviceState* ds) {
+  Context* ctx = ctx_of(context);
+  const AoBasisRec& B = ctx->ao_basis;
+  const AoDerived& d = B.d;
+  const int64_t A = B.ao_num, N = ctx->nucleus.num;
+  const std::vector<int32_t>& aosh = ds->h_ao_shell;
+  if ((int64_t)aosh.size() != A) return false;
+  for (int64_t k = 1; k < A; ++k)
+    if (aosh[k] < aosh[k - 1]) return false;
+  const int64_t nkb = (A + 63) / 64;
+  struct KRecShell { double x, y, z, range; int32_t pb, pe, pad0, pad1; };
+  std::vector<size_t> sizes(nkb);
+  size_t rec = 0;
+  for (int64_t kb = 0; kb < nkb; ++kb) {
+    const int64_t k0 = kb * 64, k1 = std::min<int64_t>(k0 + 64, A);
+    const int s0 = aosh[k0], s1 = aosh[k1 - 1];
+    size_t np = 0;
+    for (int sh = s0; sh <= s1; ++sh) np += d.shell_coef_start[sh + 1] - d.shell_coef_start[sh];
+    sizes[kb] = 16 + 64 * 8 + (size_t)(s1 - s0 + 1) * sizeof(KRecShell) + np * 16;
+    rec = std::max(rec, sizes[kb]);
+  }
+  rec = (rec + 127) / 128 * 128;
+  std::vector<uint8_t> h(rec * nkb, 0);
+  for (int64_t kb = 0; kb < nkb; ++kb) {
+    uint8_t* r = h.data() + kb * rec;
+    const int64_t k0 = kb * 64, k1 = std::min<int64_t>(k0 + 64, A);
+    const int s0 = aosh[k0], s1 = aosh[k1 - 1];
+    int32_t* hdr = (int32_t*)r;
+    int32_t* ao = (int32_t*)(r + 16);
+    KRecShell* sh = (KRecShell*)(r + 16 + 64 * 8);
+    double* prm = (double*)(r + 16 + 64 * 8 + (size_t)(s1 - s0 + 1) * sizeof(KRecShell));
+    hdr[0] = s1 - s0 + 1;
+    for (int64_t t = 0; t < 64; ++t) {
+      const int64_t k = k0 + t;
+      if (k < k1) {
+        const float f = (float)B.ao_factor[k];
+        ao[2 * t] = (ds->h_ao_code[k] & 0xFFFF) | ((aosh[k] - s0) << 16);
+        std::memcpy(&ao[2 * t + 1], &f, 4);
+      } else {
+        ao[2 * t] = -1;
+        ao[2 * t + 1] = 0;
+      }
+    }
+    int np = 0;
+    for (int q = s0; q <= s1; ++q) {
+      const int n = ds->h_shell_nuc[q];
+      KRecShell& e = sh[q - s0];
+      e.x = ctx->nucleus.coord[n];
+      e.y = ctx->nucleus.coord[n + N];
+      e.z = ctx->nucleus.coord[n + 2 * N];
+      e.range = d.nucleus_range[n];
+      e.pb = np;
+      for (int j = d.shell_coef_start[q]; j < d.shell_coef_start[q + 1]; ++j) {
+        prm[2 * np] = d.expo_sorted[d.nuc_prim_start[n] + d.coef_prim[j]];
+        prm[2 * np + 1] = d.coef_val[j];
+        ++np;
+      }
+      e.pe = np;
+    }
+    hdr[1] = np;
+  }
+  if (ensure(context, ds->krec, h.size(), "qmckl_b200_mo_mixed") != QMCKL_SUCCESS) return false;
+  if (cudaMemcpy(ds->krec.p, h.data(), h.size(), cudaMemcpyHostToDevice) != cudaSuccess) return false;
+  ds->rec_bytes = (int)rec;
+  ds->krec_basis_version = ctx->ao_basis.basis_version;
+  ds->krec_nucl_version = ctx->nucleus.coord_version;
+  return true;
+}
+
 qmckl_exit_code run_mo_mixed(qmckl_context context, DeviceState* ds, int64_t P, const double* coord,
                              double* out, int comps) {
   Context* ctx = ctx_of(context);
@@ -372,10 +453,31 @@ qmckl_exit_code run_mo_mixed(qmckl_context context, DeviceState* ds, int64_t P, 
     ds->tc_pieces = pieces;
   }
   if (ds->fused) {
-    // fused AO -> MO kernel: the AO pieces never leave shared memory
-    QB_CUDA(tc_run_fused(ds->T, ds->tc, P, comps, coord, cutoff_of(ctx), ds->tc_coef.p, out, ds->stream),
-            "qmckl_b200_mo_mixed");
-    return QMCKL_SUCCESS;
+    bool ok = ds->krec.p != nullptr && ds->krec_basis_version == ctx->ao_basis.basis_version &&
+              ds->krec_nucl_version == ctx->nucleus.coord_version;
+    if (!ok) ok = build_krec(context, ds);
+    if (ok && tc_fused_smem(ds->tc, comps, ds->rec_bytes) <= 232448) {
+      // spatial order of the points, then the fused AO -> MO kernel (the AO
+      // pieces never leave shared memory)
+      const size_t obytes = sizeof(int) * 2 * (size_t)P + sizeof(unsigned int) * (kSortCells + 1);
+      qmckl_exit_code rc = ensure(context, ds->order, obytes, "qmckl_b200_mo_mixed");
+      if (rc != QMCKL_SUCCESS) return rc;
+      int* keys = (int*)ds->order.p;
+      int* perm = keys + P;
+      unsigned int* counts = (unsigned int*)(perm + P);
+      double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+      const int64_t N = ctx->nucleus.num;
+      for (int64_t n = 0; n < N; ++n)
+        for (int d = 0; d < 3; ++d) {
+          lo[d] = std::min(lo[d], ctx->nucleus.coord[n + d * N] - 4.0);
+          hi[d] = std::max(hi[d], ctx->nucleus.coord[n + d * N] + 4.0);
+        }
+      QB_CUDA(point_order(coord, P, lo, hi, keys, counts, perm, ds->stream), "qmckl_b200_mo_mixed");
+      QB_CUDA(tc_run_fused(ds->T, ds->tc, P, comps, coord, cutoff_of(ctx), ds->tc_coef.p, ds->krec.p, ds->rec_bytes,
+                           perm, out, ds->stream),
+              "qmckl_b200_mo_mixed");
+      return QMCKL_SUCCESS;
+    }
   }
   const int64_t rows = (int64_t)comps * P;
   const size_t abytes = tc_a_bytes(ds->tc, rows);
@@ -441,7 +543,7 @@ void dev_detach(Context* ctx) {
   if (ds->device >= 0) cudaSetDevice(ds->device);
   if (ds->stream) cudaStreamSynchronize(ds->stream);
   for (DevBuf* b : {&ds->tables, &ds->nucl, &ds->coord, &ds->prim_vgl, &ds->shell_vgl, &ds->ao_vgl, &ds->ao_value,
-                    &ds->mo_vgl, &ds->mo_value, &ds->coef_t, &ds->tc_coef, &ds->tc_a})
+                    &ds->mo_vgl, &ds->mo_value, &ds->coef_t, &ds->tc_coef, &ds->tc_a, &ds->krec, &ds->order})
     release(*b);
   if (ds->own_stream && ds->stream) cudaStreamDestroy(ds->stream);
   delete ds;

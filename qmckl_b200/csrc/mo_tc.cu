@@ -60,7 +60,9 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
   constexpr int A_TILE = BM * BK * 2;             // bytes of one A piece tile
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   // 1024-byte aligned base for the swizzled tiles
-  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  // 1024-byte aligned base, kept as pointer arithmetic on the __shared__
+  // array so that accesses compile to shared-memory (not generic) loads
+  uint8_t* smem = smem_raw + ((1024u - (tcx::smem_addr(smem_raw) & 1023u)) & 1023u);
   const int B_TILE = n_tile * BK * 2;
   const int STAGE = PIECES * (A_TILE + B_TILE);
   uint64_t* full = (uint64_t*)(smem + STAGES * STAGE);

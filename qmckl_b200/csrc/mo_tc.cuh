@@ -38,8 +38,18 @@ cudaError_t tc_run(const DevTables& T, const TcPlan& plan, int64_t point_num, in
 
 // Fused form of tc_run: the AO pieces are produced in shared memory by the
 // GEMM kernel itself and never written to device memory (fused_tc.cu).
+// krec: one record of rec_bytes per 64-AO K block (see fused_tc.cu); perm
+// (optional): order in which the points are grouped into tiles.
 cudaError_t tc_run_fused(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps, const double* coord,
-                         double cutoff, const void* d_coef, double* out, cudaStream_t s);
+                         double cutoff, const void* d_coef, const void* krec, int rec_bytes, const int* perm,
+                         double* out, cudaStream_t s);
+// Spatial order of points (32^3 cells over [box_lo, box_hi], Morton order) by
+// a counting sort: perm[P]; keys[P] and counts[kSortCells + 1] are scratch.
+constexpr int kSortCells = 1 << 15;
+cudaError_t point_order(const double* coord, int64_t point_num, const double* box_lo, const double* box_hi,
+                        int* keys, unsigned int* counts, int* perm, cudaStream_t s);
+// dynamic shared memory of the fused kernel (must stay <= 227 KB)
+size_t tc_fused_smem(const TcPlan& plan, int comps, int rec_bytes);
 
 // Same evaluation with caller-provided scratch: the A pieces in d_a and the
 // barrier-timeout word in d_err (cleared here before the launches).  Makes no
