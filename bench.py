@@ -22,7 +22,6 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -60,55 +59,53 @@ def load_traffic():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """SM clock and throttle reasons sampled every ~10 ms (NVML) during the timed region."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event-reason bits
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown", 0x4: "sw_power_cap",
+               0x80: "hw_power_brake_slowdown"}
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
-        self.proc = None
-        self.lines = []
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self.stop_flag = False
+        self.thread = None
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
-        except Exception:
-            self.proc = None
+            import pynvml
+            pynvml.nvmlInit()
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            idx = int(vis.split(",")[self.gpu]) if vis else self.gpu
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(idx)
+            self.nv = pynvml
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception as e:   # no NVML: report it, keep running
+            self.err = str(e)
+            return
+        self.thread = threading.Thread(target=self._run, daemon=True)
+        self.thread.start()
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _run(self):
+        nv = self.nv
+        while not self.stop_flag:
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for b, name in self.REASONS.items():
+                    if bits & b:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.01)
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                smax = float(f[2])
-            except ValueError:
-                continue
-            for name, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(name)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        if self.thread is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["NVML unavailable: " + getattr(self, "err", "")]}
+        self.stop_flag = True
+        self.thread.join(timeout=2)
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples), "source": "NVML, 10 ms polling"}
 
 
 def cpu_baseline(sysd, seconds=15.0, nthreads=0):
@@ -157,17 +154,41 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def profile_case(kind, walkers=64):
+    """One evaluation of the config-1 molecule on `walkers` walkers, for ncu captures."""
+    import torch
+    from qmckl_b200 import gen
+    from qmckl_b200 import qmckl as pq
+    from qmckl_b200.system import make_context
+    d = gen.config(1, walk_num=walkers)
+    P = d["elec_coord"].shape[0] * d["elec_coord"].shape[1]
+    M = d["mo_num"]
+    dc = torch.tensor(np.ascontiguousarray(gen.points(d).T), dtype=torch.float64, device="cuda")
+    out = torch.empty(P * 5 * M, dtype=torch.float64, device="cuda")
+    ctx = make_context(d, points=False, form=pq.FORM_FP64 if kind == "fp64" else pq.FORM_MIXED)
+    if kind != "fp64":
+        pq.b200_set_mixed_kernel(ctx, kind == "fused")
+    pq.b200_mo_vgl_device(ctx, P, dc.data_ptr(), out.data_ptr())
+    pq.b200_synchronize(ctx)
+    pq.context_destroy(ctx)
+    print(f"profile case {kind}: {P} points")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default=os.environ.get("QMCKL_B200_BENCH_FORM", "mixed"), choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", choices=["fused", "split", "fp64"],
+                    help="run one evaluation of a small case (config-1 molecule, 64 walkers) for ncu; no timing")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile:
+        return profile_case(args.profile)
 
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -308,14 +329,23 @@ def main():
                                      "ms_per_launch": ms - ao_ms,
                                      "tflops": 2.0 * 5 * P * A * M / ((ms - ao_ms) * 1e-3) / 1e12}}
     else:
+        # fused kernel: 25 points x 5 components per 128-row MMA tile, MOs
+        # padded to 16, AOs to 64; 6 split-BF16 products per K step
         flops = 2.0 * 5 * P * A * M
-        pieces = 3
-        executed = flops * (6 if pieces == 3 else 3)
+        tiles = -(-P // 25)
+        n_pad = -(-M // 16) * 16 if M <= 160 else M
+        k_pad = -(-A // 64) * 64
+        executed = 2.0 * tiles * 128 * n_pad * k_pad * 6
         achieved = executed / (ms * 1e-3) / 1e12
-        roofline = {"kernel": "split-BF16 tcgen05 MO contraction (whole step)", "bound": "tensor",
-                    "achieved": achieved, "peak": bf16, "unit": "TFLOP/s", "frac": achieved / bf16,
-                    "peak_source": peak_src, "traffic": traffic.get(("mo_tc", "mixed")),
-                    "dense_equivalent_tflops": flops / (ms * 1e-3) / 1e12}
+        t = traffic.get(("fused_mo_kernel", "mixed"))
+        roofline = {"kernel": "fused_mo_kernel<3,5> (AO -> split-BF16 tcgen05 MO VGL; step = 3 ordering kernels + this)",
+                    "bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
+                    "frac": achieved / bf16, "peak_source": peak_src,
+                    "traffic": t * P / 20352.0 if t else None,
+                    "traffic_note": "ncu dram bytes of a 20,352-point launch scaled by points" if t else None,
+                    "executed_tensor_flop_per_launch": executed,
+                    "dense_equivalent_tflops": flops / (ms * 1e-3) / 1e12,
+                    "output_bytes_per_launch": 40.0 * P * M}
 
     value = world * P / (ms * 1e-3)
     line = {
