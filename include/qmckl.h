@@ -169,6 +169,10 @@ qmckl_exit_code qmckl_get_ao_basis_ao_vgl(qmckl_context context, double* const a
 qmckl_exit_code qmckl_get_ao_basis_ao_vgl_inplace(qmckl_context context, double* const ao_vgl, const int64_t size_max);
 qmckl_exit_code qmckl_get_ao_basis_ao_value(qmckl_context context, double* const ao_value, const int64_t size_max);
 qmckl_exit_code qmckl_get_ao_basis_ao_value_inplace(qmckl_context context, double* const ao_value, const int64_t size_max);
+/* ao_hessian[3][point_num][4][ao_num]: [i][p][j][k] = d_i d_j AO_k (j < 3) and
+ * d_i (Laplacian of AO_k) (j = 3), derivatives with respect to the point
+ * coordinates (org/qmckl_ao.org:9400-9404, 9590-9720). */
+qmckl_exit_code qmckl_get_ao_basis_ao_hessian(qmckl_context context, double* const ao_hessian, const int64_t size_max);
 
 /* ---- MO basis: org/qmckl_mo.org:192-1747, 3479 ---- */
 qmckl_exit_code qmckl_set_mo_basis_mo_num(qmckl_context context, const int64_t mo_num);

@@ -65,6 +65,26 @@ qmckl_exit_code qmckl_b200_mo_vgl_device(qmckl_context context, const int64_t po
                                          const double* d_coord, double* d_mo_vgl);
 qmckl_exit_code qmckl_b200_mo_value_device(qmckl_context context, const int64_t point_num,
                                            const double* d_coord, double* d_mo_value);
+/* AO Hessian into device memory, layout of qmckl_get_ao_basis_ao_hessian
+ * ([3][point][4][ao], org/qmckl_ao.org:9400-9404). */
+qmckl_exit_code qmckl_b200_ao_hessian_device(qmckl_context context, const int64_t point_num,
+                                             const double* d_coord, double* d_ao_hessian);
+
+/* Adjoint of MO VGL (no counterpart in the reference, which offers the
+ * orbital forces qmckl_get_forces_mo_value / _mo_g / _mo_l of
+ * org/qmckl_forces.org:5550-6880 as full tensors instead).  For the scalar
+ * L = sum_{p,c,i} d_weight[p][c][i] * mo_vgl[p][c][i] (d_weight in the
+ * mo_vgl layout [point][5][mo]) it writes, each output optional (NULL):
+ *   d_grad_coef  [mo][ao]  dL/d coefficient (the qmckl_set_mo_basis_coefficient layout)
+ *   d_grad_nucl  [nucl][3] dL/d nuclear coordinates
+ *   d_grad_coord [3][point] dL/d point coordinates (the d_coord layout)
+ * Outputs are overwritten.  Nothing of a forward evaluation is reused: the
+ * AOs and their derivatives are recomputed.  The context's form selects FP64
+ * or FP32 exponentials (mixed); the contractions are FP64.  Asynchronous on
+ * the context's stream, like the other device entry points. */
+qmckl_exit_code qmckl_b200_mo_vgl_adjoint_device(qmckl_context context, const int64_t point_num,
+                                                 const double* d_coord, const double* d_weight,
+                                                 double* d_grad_coef, double* d_grad_nucl, double* d_grad_coord);
 
 /* Mixed-form MO VGL that allocates no device memory.  No counterpart in the
  * reference library.

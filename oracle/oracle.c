@@ -611,3 +611,224 @@ int oracle_mo_value(int64_t ao_num, int64_t mo_num, int64_t point_num,
   }
   return 0;
 }
+
+/* ------------------------------------------------------------------ derivatives
+ *
+ * Second and third derivatives used by the nuclear-derivative checks.  The
+ * reference builds them from the doc (Fortran) routines: shell Hessian
+ * qmckl_compute_ao_basis_shell_gaussian_hessian (org/qmckl_ao.org:5480-5580),
+ * polynomial Hessian qmckl_compute_ao_polynomial_hessian_doc (7113-7236), AO
+ * Hessian qmckl_compute_ao_hessian_doc (9590-9720), and the orbital forces
+ * qmckl_compute_forces_mo_value_doc / _mo_g / _mo_l
+ * (org/qmckl_forces.org:5688-5800, 6132-6337, 6648-6772). */
+
+/* shell_hessian[point][3][4][shell]: [d][m] = d_d d_m R for m < 3 and
+ * [d][3] = d_d lap R (org/qmckl_ao.org:5530-5578).  Primitives with a r^2 >
+ * cutoff are skipped one by one (no sort), as the reference does. */
+int oracle_shell_hessian_doc(const oracle_basis* b, int32_t precision, int64_t point_num,
+                             const double* coord, const double* nucl_coord, double* shell_hessian) {
+  const double cutoff = oracle_cutoff(precision);
+  const int64_t N = b->nucl_num, S = b->shell_num;
+  memset(shell_hessian, 0, sizeof(double) * 12 * S * point_num);
+  for (int64_t ip = 0; ip < point_num; ++ip) {
+    double* o = shell_hessian + ip * 12 * S;
+    for (int64_t n = 0; n < N; ++n) {
+      const double xyz[3] = {coord[ip] - nucl_coord[n], coord[ip + point_num] - nucl_coord[n + N],
+                             coord[ip + 2 * point_num] - nucl_coord[n + 2 * N]};
+      const double r2 = xyz[0] * xyz[0] + xyz[1] * xyz[1] + xyz[2] * xyz[2];
+      if (r2 > cutoff * b->nucleus_range[n]) continue;
+      for (int64_t s = b->nucleus_index[n]; s < b->nucleus_index[n] + b->nucleus_shell_num[n]; ++s) {
+        for (int64_t p = b->shell_prim_index[s]; p < b->shell_prim_index[s] + b->shell_prim_num[s]; ++p) {
+          const double ar2 = b->exponent[p] * r2;
+          if (ar2 > cutoff) continue;
+          const double v = b->coef_norm[p] * exp(-ar2);
+          const double two_a = 2.0 * b->exponent[p];
+          for (int i = 0; i < 3; ++i) {
+            for (int j = 0; j < 3; ++j) {
+              double* h = &o[(j * 4 + i) * S + s];
+              if (i == j) *h -= two_a * v;
+              *h += two_a * two_a * xyz[i] * xyz[j] * v;
+            }
+            o[(i * 4 + 3) * S + s] += (5.0 * two_a * two_a * xyz[i] - two_a * two_a * two_a * r2 * xyz[i]) * v;
+          }
+        }
+      }
+    }
+  }
+  return 0;
+}
+
+/* hess[n][m][k] = d_k d_m P_n (m < 3), hess[n][3][k] = d_k lap P_n, with the
+ * 1e-20 shift on the displacement (org/qmckl_ao.org:7113-7236). */
+static void poly_hessian_doc(int lmax, const double X[3], const double R[3], double hess[20][4][3]) {
+  double Y[3], pw[3][8];  /* pw[.][i+2] = Y^i for i >= -2 */
+  for (int i = 0; i < 3; ++i) Y[i] = (X[i] - R[i]) + 1.e-20;
+  memset(hess, 0, sizeof(double) * 20 * 4 * 3);
+  if (lmax < 2) return;
+  for (int d = 0; d < 3; ++d) {
+    pw[d][0] = pw[d][1] = pw[d][2] = 1.0;
+    for (int i = 1; i <= lmax; ++i) pw[d][i + 2] = pw[d][i + 1] * Y[d];
+  }
+#define PW(d, e) pw[d][(e) + 2]
+  int n = 4;
+  double dd = 2.0;
+  for (int d = 2; d <= lmax; ++d) {
+    double da = dd;
+    for (int a = d; a >= 0; --a) {
+      double db = dd - da;
+      for (int bb = d - a; bb >= 0; --bb) {
+        const int c = d - a - bb;
+        const double dc = dd - da - db;
+        double (*h)[3] = hess[n];
+        h[0][0] = da * (da - 1.) * PW(0, a - 2) * PW(1, bb) * PW(2, c);
+        h[1][1] = db * (db - 1.) * PW(0, a) * PW(1, bb - 2) * PW(2, c);
+        h[2][2] = dc * (dc - 1.) * PW(0, a) * PW(1, bb) * PW(2, c - 2);
+        h[1][0] = h[0][1] = da * db * PW(0, a - 1) * PW(1, bb - 1) * PW(2, c);
+        h[2][0] = h[0][2] = da * dc * PW(0, a - 1) * PW(1, bb) * PW(2, c - 1);
+        h[2][1] = h[1][2] = db * dc * PW(0, a) * PW(1, bb - 1) * PW(2, c - 1);
+        h[3][0] = da * db * (db - 1.) * PW(0, a - 1) * PW(1, bb - 2) * PW(2, c) +
+                  da * dc * (dc - 1.) * PW(0, a - 1) * PW(1, bb) * PW(2, c - 2);
+        h[3][1] = db * da * (da - 1.) * PW(0, a - 2) * PW(1, bb - 1) * PW(2, c) +
+                  db * dc * (dc - 1.) * PW(0, a) * PW(1, bb - 1) * PW(2, c - 2);
+        h[3][2] = dc * da * (da - 1.) * PW(0, a - 2) * PW(1, bb) * PW(2, c - 1) +
+                  dc * db * (db - 1.) * PW(0, a) * PW(1, bb - 2) * PW(2, c - 1);
+        if (da > 2) h[3][0] += da * (da - 1.) * (da - 2.) * PW(0, a - 3) * PW(1, bb) * PW(2, c);
+        if (db > 2) h[3][1] += db * (db - 1.) * (db - 2.) * PW(0, a) * PW(1, bb - 3) * PW(2, c);
+        if (dc > 2) h[3][2] += dc * (dc - 1.) * (dc - 2.) * PW(0, a) * PW(1, bb) * PW(2, c - 3);
+        db -= 1.0;
+        ++n;
+      }
+      da -= 1.0;
+    }
+    dd += 1.0;
+  }
+#undef PW
+}
+
+/* ao_hessian[3][point][4][ao]: [i][p][j][k] = d_i d_j chi_k (j < 3) and
+ * [i][p][3][k] = d_i lap chi_k, derivatives with respect to the electron
+ * coordinates (org/qmckl_ao.org:9590-9720). */
+int oracle_ao_hessian_doc(const oracle_basis* b, int32_t precision, int64_t point_num,
+                          const double* coord, const double* nucl_coord, double* ao_hessian) {
+  const double cutoff = oracle_cutoff(precision);
+  const int64_t N = b->nucl_num, S = b->shell_num, A = b->ao_num;
+  double* sv = (double*)malloc(sizeof(double) * 5 * S * point_num);
+  double* sh = (double*)malloc(sizeof(double) * 12 * S * point_num);
+  oracle_shell_vgl_doc(b, precision, point_num, coord, nucl_coord, sv);
+  oracle_shell_hessian_doc(b, precision, point_num, coord, nucl_coord, sh);
+  double poly[5][20], ph[20][4][3];
+  for (int64_t ip = 0; ip < point_num; ++ip) {
+    for (int i = 0; i < 3; ++i) memset(ao_hessian + (i * point_num + ip) * 4 * A, 0, sizeof(double) * 4 * A);
+    const double X[3] = {coord[ip], coord[ip + point_num], coord[ip + 2 * point_num]};
+    const double* s = sv + ip * 5 * S;
+    const double* H = sh + ip * 12 * S;
+    for (int64_t n = 0; n < N; ++n) {
+      const double R[3] = {nucl_coord[n], nucl_coord[n + N], nucl_coord[n + 2 * N]};
+      const double x = X[0] - R[0], y = X[1] - R[1], z = X[2] - R[2];
+      const double r2 = x * x + y * y + z * z;
+      if (r2 > cutoff * b->nucleus_range[n]) continue;
+      poly_hessian_doc(b->nucleus_max_l[n], X, R, ph);
+      poly_vgl_doc(b->nucleus_max_l[n], X, R, poly);
+      for (int64_t shl = b->nucleus_index[n]; shl < b->nucleus_index[n] + b->nucleus_shell_num[n]; ++shl) {
+        const int l = b->shell_ang_mom[shl];
+        int64_t k = b->ao_index[shl];
+        for (int64_t il = lstart(l); il < lstart(l + 1); ++il, ++k) {
+          const double f = b->ao_factor[k];
+          for (int i = 0; i < 3; ++i) {
+            double* o = ao_hessian + (i * point_num + ip) * 4 * A;
+            for (int j = 0; j < 3; ++j)
+              o[j * A + k] = (ph[il][i][j] * s[shl] + poly[0][il] * H[(i * 4 + j) * S + shl] +
+                              poly[j + 1][il] * s[(i + 1) * S + shl] + poly[i + 1][il] * s[(j + 1) * S + shl]) * f;
+            double t = 0.0;
+            for (int m = 0; m < 3; ++m)
+              t += ph[il][i][m] * s[(m + 1) * S + shl] + poly[m + 1][il] * H[(i * 4 + m) * S + shl];
+            o[3 * A + k] = (ph[il][3][i] * s[shl] + poly[0][il] * H[(i * 4 + 3) * S + shl] +
+                            poly[4][il] * s[(i + 1) * S + shl] + poly[i + 1][il] * s[4 * S + shl] + 2.0 * t) * f;
+          }
+        }
+      }
+    }
+  }
+  free(sv); free(sh);
+  return 0;
+}
+
+/* Gradient of L = sum_{p,c,i} W[p][c][i] mo_vgl[p][c][i] (W in the mo_vgl
+ * layout [point][5][mo]).
+ *   grad_nucl[a][n]  through the orbital forces of the reference:
+ *       forces_mo_value[a][p][n][i] = -sum_{k on a} Ct(i,k) ao_vgl[p][1+n][k]
+ *       forces_mo_g[a][n][p][m][i]  = -sum_{k on a} Ct(i,k) ao_hessian[n][p][m][k]
+ *       forces_mo_l[a][n][p][i]     = -sum_{k on a} Ct(i,k) ao_hessian[n][p][3][k]
+ *     (org/qmckl_forces.org:5688-5800, 6132-6337, 6648-6772), then contracted
+ *     with W over (p, i) and the component;
+ *   grad_coef[i][k]  = sum_{p,c} W[p][c][i] ao_vgl[p][c][k]  ([mo][ao], the
+ *     qmckl_set_mo_basis_coefficient layout);
+ *   grad_coord[n][p] = derivative with respect to the point coordinates
+ *     (the same sums over all nuclei, opposite sign).
+ * Any output pointer may be NULL. */
+int oracle_mo_vgl_adjoint(const oracle_basis* b, int32_t precision, int64_t point_num, const double* coord,
+                          const double* nucl_coord, int64_t mo_num, const double* coefficient,
+                          const double* weight, double* grad_coef, double* grad_nucl, double* grad_coord) {
+  const int64_t N = b->nucl_num, A = b->ao_num, M = mo_num, P = point_num;
+  double* av = (double*)malloc(sizeof(double) * 5 * A * P);
+  double* ah = (double*)malloc(sizeof(double) * 12 * A * P);
+  oracle_ao_vgl_doc(b, precision, P, coord, nucl_coord, av);
+  oracle_ao_hessian_doc(b, precision, P, coord, nucl_coord, ah);
+  if (grad_coef) {
+    memset(grad_coef, 0, sizeof(double) * M * A);
+    for (int64_t p = 0; p < P; ++p)
+      for (int c = 0; c < 5; ++c) {
+        const double* w = weight + (p * 5 + c) * M;
+        const double* a = av + (p * 5 + c) * A;
+        for (int64_t i = 0; i < M; ++i) {
+          const double wi = w[i];
+          if (wi == 0.0) continue;
+          double* g = grad_coef + i * A;
+          for (int64_t k = 0; k < A; ++k) g[k] += wi * a[k];
+        }
+      }
+  }
+  if (grad_nucl) memset(grad_nucl, 0, sizeof(double) * 3 * N);
+  if (grad_coord) memset(grad_coord, 0, sizeof(double) * 3 * P);
+  double* fv = (double*)malloc(sizeof(double) * 3 * M);     /* forces_mo_value[a][p][.][.] */
+  double* fg = (double*)malloc(sizeof(double) * 9 * M);     /* forces_mo_g[a][.][p][.][.]  */
+  double* fl = (double*)malloc(sizeof(double) * 3 * M);     /* forces_mo_l[a][.][p][.]     */
+  for (int64_t a = 0; a < N; ++a) {
+    const int64_t s0 = b->nucleus_index[a], s1 = s0 + b->nucleus_shell_num[a];
+    const int64_t k0 = s1 > s0 ? b->ao_index[s0] : 0;
+    const int64_t k1 = s1 > s0 ? b->ao_index[s1 - 1] + (lstart(b->shell_ang_mom[s1 - 1] + 1) -
+                                                         lstart(b->shell_ang_mom[s1 - 1])) : 0;
+    for (int64_t p = 0; p < P; ++p) {
+      memset(fv, 0, sizeof(double) * 3 * M);
+      memset(fg, 0, sizeof(double) * 9 * M);
+      memset(fl, 0, sizeof(double) * 3 * M);
+      for (int64_t k = k0; k < k1; ++k) {
+        const double* ck = coefficient;   /* Ct(i,k) = coefficient[i][k] */
+        for (int n = 0; n < 3; ++n) {
+          const double c1 = av[(p * 5 + 1 + n) * A + k];
+          for (int64_t i = 0; i < M; ++i) fv[n * M + i] -= c1 * ck[i * A + k];
+          const double* h = ah + (n * P + p) * 4 * A;
+          for (int m = 0; m < 3; ++m) {
+            const double hm = h[m * A + k];
+            if (hm != 0.0)
+              for (int64_t i = 0; i < M; ++i) fg[(n * 3 + m) * M + i] -= ck[i * A + k] * hm;
+          }
+          const double hl = h[3 * A + k];
+          for (int64_t i = 0; i < M; ++i) fl[n * M + i] -= ck[i * A + k] * hl;
+        }
+      }
+      for (int n = 0; n < 3; ++n) {
+        double acc = 0.0;
+        for (int64_t i = 0; i < M; ++i) {
+          acc += weight[(p * 5 + 0) * M + i] * fv[n * M + i];
+          for (int m = 0; m < 3; ++m) acc += weight[(p * 5 + 1 + m) * M + i] * fg[(n * 3 + m) * M + i];
+          acc += weight[(p * 5 + 4) * M + i] * fl[n * M + i];
+        }
+        if (grad_nucl) grad_nucl[a * 3 + n] += acc;
+        if (grad_coord) grad_coord[n * P + p] -= acc;
+      }
+    }
+  }
+  free(fv); free(fg); free(fl); free(av); free(ah);
+  return 0;
+}

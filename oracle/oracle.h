@@ -75,6 +75,22 @@ int oracle_mo_value(int64_t ao_num, int64_t mo_num, int64_t point_num,
                     const double* coefficient_t, const double* ao_value,
                     double* mo_value, int32_t nthreads);
 
+/* Derivatives (nuclear-derivative checks).
+ *   shell_hessian[point][3][4][shell], ao_hessian[3][point][4][ao]: second
+ *   derivatives and derivatives of the Laplacian with respect to the point
+ *   coordinates (the reference's qmckl_get_ao_basis_ao_hessian layout). */
+int oracle_shell_hessian_doc(const oracle_basis* b, int32_t precision, int64_t point_num,
+                             const double* coord, const double* nucl_coord, double* shell_hessian);
+int oracle_ao_hessian_doc(const oracle_basis* b, int32_t precision, int64_t point_num,
+                          const double* coord, const double* nucl_coord, double* ao_hessian);
+/* Gradient of L = sum W * mo_vgl (W: [point][5][mo]) with respect to the MO
+ * coefficients ([mo][ao]), the nuclear coordinates ([nucl][3]) and the point
+ * coordinates ([3][point]), through the reference's orbital forces.  Outputs
+ * may be NULL. */
+int oracle_mo_vgl_adjoint(const oracle_basis* b, int32_t precision, int64_t point_num, const double* coord,
+                          const double* nucl_coord, int64_t mo_num, const double* coefficient,
+                          const double* weight, double* grad_coef, double* grad_nucl, double* grad_coord);
+
 #ifdef __cplusplus
 }
 #endif

@@ -40,6 +40,10 @@ def lib():
             getattr(L, f).argtypes = [C.c_void_p, C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]
         for f in ("oracle_primitive_vgl", "oracle_shell_vgl_doc", "oracle_ao_vgl_doc"):
             getattr(L, f).argtypes = [C.c_void_p, C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
+        for f in ("oracle_shell_hessian_doc", "oracle_ao_hessian_doc"):
+            getattr(L, f).argtypes = [C.c_void_p, C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oracle_mo_vgl_adjoint.argtypes = [C.c_void_p, C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64,
+                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         for f in ("oracle_mo_vgl", "oracle_mo_value"):
             getattr(L, f).argtypes = [C.c_int64, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]
         _lib = L
@@ -137,6 +141,38 @@ def mo_value(coefficient, ao_value_arr, nthreads=0):
     out = np.empty((P, M), dtype=np.float64)
     lib().oracle_mo_value(A, M, P, _p(ct), _p(a), _p(out), nthreads)
     return out
+
+
+def shell_hessian(basis, coord, nucl_coord, precision=53):
+    """[P][3][4][shell] (qmckl_get_ao_basis_shell_hessian layout)."""
+    c, n = _coords(coord, nucl_coord)
+    P = c.shape[1]
+    out = np.empty((P, 3, 4, basis.shell_num), dtype=np.float64)
+    lib().oracle_shell_hessian_doc(basis.h, precision, P, _p(c), _p(n), _p(out))
+    return out
+
+
+def ao_hessian(basis, coord, nucl_coord, precision=53):
+    """[3][P][4][ao] (qmckl_get_ao_basis_ao_hessian layout)."""
+    c, n = _coords(coord, nucl_coord)
+    P = c.shape[1]
+    out = np.empty((3, P, 4, basis.ao_num), dtype=np.float64)
+    lib().oracle_ao_hessian_doc(basis.h, precision, P, _p(c), _p(n), _p(out))
+    return out
+
+
+def mo_vgl_adjoint(basis, coord, nucl_coord, coefficient, weight, precision=53):
+    """Gradient of sum(weight * mo_vgl): (grad_coef [mo][ao], grad_nucl [nucl][3], grad_coord [P][3])."""
+    c, n = _coords(coord, nucl_coord)
+    P = c.shape[1]
+    coef = np.ascontiguousarray(coefficient, dtype=np.float64)
+    M = coef.shape[0]
+    w = np.ascontiguousarray(weight, dtype=np.float64).reshape(P, 5, M)
+    gc = np.empty((M, basis.ao_num))
+    gn = np.empty((basis.nucl_num, 3))
+    gr = np.empty((3, P))
+    lib().oracle_mo_vgl_adjoint(basis.h, precision, P, _p(c), _p(n), M, _p(coef), _p(w), _p(gc), _p(gn), _p(gr))
+    return gc, gn, np.ascontiguousarray(gr.T)
 
 
 def cutoff(precision=53):

@@ -1,0 +1,306 @@
+// Derivative kernels of the AO VGL: the AO Hessian getter and the adjoint of
+// MO VGL with respect to the nuclear and point coordinates.
+//
+// Quantities (derivatives with respect to the point coordinates r; an AO
+// centred on nucleus A depends on r - R_A, so d/dR_A = -d/dr):
+//   radial part  R(s) = sum_j c_j exp(-a_j s), s = r^2, and its s-derivatives
+//                R1 = -sum a c e, R2 = sum a^2 c e, R3 = -sum a^3 c e
+//                d_d R = 2 x_d R1,  d_d d_e R = 4 x_d x_e R2 + 2 delta_de R1,
+//                lap R = 4 s R2 + 6 R1,  d_d lap R = x_d (20 R2 + 8 s R3)
+//   monomial     P = x^a y^b z^c with all derivatives up to third order
+//   AO           chi = f P R;  H_de = d_d d_e chi;  T_d = d_d lap chi
+// The reference forms the same quantities from the shell Hessian
+// (qmckl_compute_ao_basis_shell_gaussian_hessian, org/qmckl_ao.org:5480-5580),
+// the polynomial Hessian (qmckl_compute_ao_polynomial_hessian_doc, 7113-7236)
+// and the AO Hessian (qmckl_compute_ao_hessian_doc, 9590-9720); its orbital
+// forces (org/qmckl_forces.org:5688-6772) contract them with the MO
+// coefficients.  Screening follows the forward kernels: nucleus skipped when
+// r^2 > cutoff * range, primitives sorted by exponent with a break at
+// a r^2 > cutoff, AO skipped when its contracted radial value is zero.
+//
+// Work decomposition: one warp per (point, nucleus block), as in the forward
+// AO kernel: lanes stage the block's displacements and radial derivative sets
+// in shared memory, then sweep the block's contiguous AO range.
+//   MODE_HESSIAN  writes ao_hessian[3][point][4][ao] (coalesced rows).
+//   MODE_ADJOINT  reads G[point][5][ao] = (W . C)[point][comp][ao], the loss
+//                 weights pulled back through the MO coefficients, and forms
+//                 q_d = G0 d_d chi + sum_e G_{1+e} H_ed + G4 T_d per AO.  A
+//                 segmented warp reduction over the (contiguous) AOs of each
+//                 nucleus feeds per-CTA shared accumulators of dL/dR (one
+//                 device atomic per nucleus and CTA at the end); the sum over
+//                 all AOs gives dL/dr of the point.
+#include <algorithm>
+
+#include "kernels.cuh"
+
+namespace qb {
+namespace {
+
+constexpr int kWarpsD = 8;
+constexpr double kShiftD = 1.e-20;
+constexpr int MODE_HESSIAN = 0, MODE_ADJOINT = 1;
+
+struct DerivSmem {
+  double rad[kBlockSlots][4];   // R, R1, R2, R3 of the block's shells
+  double nuc[kBlockNuc][4];     // displacement, r^2 (negative when screened out)
+};
+
+// x^a and its first three derivatives (Leibniz, one factor x at a time)
+__device__ __forceinline__ void pow_derivs(double x, int a, double (&q)[4]) {
+  q[0] = 1.0; q[1] = 0.0; q[2] = 0.0; q[3] = 0.0;
+  for (int i = 0; i < a; ++i) {
+    q[3] = q[3] * x + 3.0 * q[2];
+    q[2] = q[2] * x + 2.0 * q[1];
+    q[1] = q[1] * x + q[0];
+    q[0] = q[0] * x;
+  }
+}
+
+template <bool MIXED>
+__device__ __forceinline__ void stage_deriv(const DevTables& T, DerivSmem& sm, const int4 blk, const int2 slots,
+                                            double px, double py, double pz, double cutoff, int lane) {
+  const int nn = blk.y - blk.x;
+  if (lane < nn) {
+    const int n = blk.x + lane;
+    const int N = T.nucl_num;
+    const double x = px - T.nucl_coord[n];
+    const double y = py - T.nucl_coord[n + N];
+    const double z = pz - T.nucl_coord[n + 2 * N];
+    const double r2 = x * x + y * y + z * z;
+    const bool in = !(r2 > cutoff * T.nucleus_range[n]);
+    sm.nuc[lane][0] = x;
+    sm.nuc[lane][1] = y;
+    sm.nuc[lane][2] = z;
+    sm.nuc[lane][3] = in ? r2 : -1.0;
+  }
+  __syncwarp();
+  for (int s = slots.x + lane; s < slots.y; s += 32) {
+    const int nucl = T.slot_nuc[s];
+    const double r2 = sm.nuc[nucl - blk.x][3];
+    double acc[4] = {0., 0., 0., 0.};
+    if (r2 >= 0.0) {
+      const int2 cr = T.slot_coef[s];
+      const int p0 = T.nuc_prim_start[nucl];
+      for (int j = cr.x; j < cr.y; ++j) {
+        const double a = T.expo[p0 + T.coef_prim[j]];
+        const double ar2 = a * r2;
+        if (ar2 > cutoff) break;   // primitives sorted by exponent
+        const double e = (MIXED && ar2 <= 30.0) ? (double)expf(-(float)ar2) : exp(-ar2);
+        const double ce = T.coef_val[j] * e;
+        acc[0] += ce;
+        acc[1] -= a * ce;
+        acc[2] += a * a * ce;
+        acc[3] -= a * a * a * ce;
+      }
+    }
+    const int ls = s - slots.x;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) sm.rad[ls][c] = acc[c];
+  }
+  __syncwarp();
+}
+
+// Hessian H[d][e] and gradient of the Laplacian T[d] of one AO (times its
+// factor f), plus its gradient g[d].
+__device__ __forceinline__ void ao_derivs(int code, double f, const double (&v)[3], double s, const double (&R)[4],
+                                          double (&g)[3], double (&H)[3][3], double (&Tl)[3]) {
+  const int ax = code & 15, by = (code >> 4) & 15, cz = (code >> 8) & 15, l = (code >> 12) & 15;
+  double X[4], Y[4], Z[4];
+  pow_derivs(v[0], ax, X);
+  pow_derivs(v[1], by, Y);
+  pow_derivs(v[2], cz, Z);
+  const double P = X[0] * Y[0] * Z[0] + (l >= 1 ? kShiftD : 0.0);
+  const double Pd[3] = {X[1] * Y[0] * Z[0], X[0] * Y[1] * Z[0], X[0] * Y[0] * Z[1]};
+  double Pdd[3][3];
+  Pdd[0][0] = X[2] * Y[0] * Z[0];
+  Pdd[1][1] = X[0] * Y[2] * Z[0];
+  Pdd[2][2] = X[0] * Y[0] * Z[2];
+  Pdd[0][1] = Pdd[1][0] = X[1] * Y[1] * Z[0];
+  Pdd[0][2] = Pdd[2][0] = X[1] * Y[0] * Z[1];
+  Pdd[1][2] = Pdd[2][1] = X[0] * Y[1] * Z[1];
+  const double lapP = Pdd[0][0] + Pdd[1][1] + Pdd[2][2];
+  const double dlapP[3] = {X[3] * Y[0] * Z[0] + X[1] * Y[2] * Z[0] + X[1] * Y[0] * Z[2],
+                           X[2] * Y[1] * Z[0] + X[0] * Y[3] * Z[0] + X[0] * Y[1] * Z[2],
+                           X[2] * Y[0] * Z[1] + X[0] * Y[2] * Z[1] + X[0] * Y[0] * Z[3]};
+  const double Rd[3] = {2.0 * v[0] * R[1], 2.0 * v[1] * R[1], 2.0 * v[2] * R[1]};
+  double Rdd[3][3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+#pragma unroll
+    for (int e = 0; e < 3; ++e) Rdd[d][e] = 4.0 * v[d] * v[e] * R[2] + (d == e ? 2.0 * R[1] : 0.0);
+  const double lapR = 4.0 * s * R[2] + 6.0 * R[1];
+  const double k3 = 20.0 * R[2] + 8.0 * s * R[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    g[d] = f * (Pd[d] * R[0] + P * Rd[d]);
+#pragma unroll
+    for (int e = 0; e < 3; ++e) H[d][e] = f * (Pdd[d][e] * R[0] + Pd[d] * Rd[e] + Pd[e] * Rd[d] + P * Rdd[d][e]);
+    double t = 0.0;
+#pragma unroll
+    for (int e = 0; e < 3; ++e) t += Pdd[d][e] * Rd[e] + Pd[e] * Rdd[d][e];
+    Tl[d] = f * (dlapP[d] * R[0] + lapP * Rd[d] + 2.0 * t + Pd[d] * lapR + P * v[d] * k3);
+  }
+}
+
+// MODE_HESSIAN: out = ao_hessian[3][point_num][4][ao] (point_num points from
+//   coord [3][cstride], cstride >= point_num).
+// MODE_ADJOINT: G = [point_num][5][ao]; grad_nucl [nucl][3] -= sum q (per-CTA
+//   shared accumulators when use_smem, else device atomics); grad_coord
+//   ([3][gstride], may be null) += sum q.
+template <int MODE, bool MIXED>
+__global__ void __launch_bounds__(kWarpsD * 32)
+deriv_kernel(const DevTables T, const int64_t point_num, const double* __restrict__ coord, const int64_t cstride,
+             const double cutoff, double* __restrict__ out, const double* __restrict__ G,
+             double* __restrict__ grad_nucl, double* __restrict__ grad_coord, const int64_t gstride,
+             const bool use_smem) {
+  __shared__ DerivSmem smem[kWarpsD];
+  extern __shared__ double sacc[];   // [nucl][3] (MODE_ADJOINT with use_smem)
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  DerivSmem& sm = smem[warp];
+  const int64_t A = T.ao_num;
+  if (MODE == MODE_ADJOINT && use_smem) {
+    for (int i = threadIdx.x; i < 3 * T.nucl_num; i += blockDim.x) sacc[i] = 0.0;
+    __syncthreads();
+  }
+  const int64_t items = point_num * (int64_t)T.nblock;
+  const int64_t stride = (int64_t)gridDim.x * kWarpsD;
+  for (int64_t it = (int64_t)blockIdx.x * kWarpsD + warp; it < items; it += stride) {
+    const int64_t p = it / T.nblock;
+    const int b = (int)(it - p * T.nblock);
+    const int4 blk = T.block[b];
+    const int2 slots = T.block_slots[b];
+    stage_deriv<MIXED>(T, sm, blk, slots, coord[p], coord[p + cstride], coord[p + 2 * cstride], cutoff, lane);
+    double pg[3] = {0., 0., 0.};
+    for (int k0 = blk.z; k0 < blk.w; k0 += 32) {
+      const int k = k0 + lane;
+      const bool valid = k < blk.w;
+      int nl = kBlockNuc;   // past-the-end lanes form their own (last) segment
+      double g[3] = {0., 0., 0.}, H[3][3] = {{0., 0., 0.}, {0., 0., 0.}, {0., 0., 0.}}, Tl[3] = {0., 0., 0.};
+      if (valid) {
+        const int code = T.ao_code[k];
+        const int slot = (code >> 16) & 255;
+        nl = (code >> 24) & 31;
+        const double r2 = sm.nuc[nl][3];
+        const double R[4] = {sm.rad[slot][0], sm.rad[slot][1], sm.rad[slot][2], sm.rad[slot][3]};
+        if (r2 >= 0.0 && R[0] != 0.0) {
+          const double v[3] = {sm.nuc[nl][0], sm.nuc[nl][1], sm.nuc[nl][2]};
+          ao_derivs(code, T.ao_factor[k], v, r2, R, g, H, Tl);
+        }
+      }
+      if (MODE == MODE_HESSIAN) {
+        if (valid) {
+#pragma unroll
+          for (int i = 0; i < 3; ++i) {
+            double* o = out + ((int64_t)i * point_num + p) * 4 * A;
+            o[k] = H[i][0];
+            o[A + k] = H[i][1];
+            o[2 * A + k] = H[i][2];
+            o[3 * A + k] = Tl[i];
+          }
+        }
+      } else {
+        double q[3] = {0., 0., 0.};
+        if (valid) {
+          const double* gr = G + p * 5 * A + k;
+          const double G0 = gr[0], G1 = gr[A], G2 = gr[2 * A], G3 = gr[3 * A], G4 = gr[4 * A];
+#pragma unroll
+          for (int d = 0; d < 3; ++d) q[d] = G0 * g[d] + G1 * H[0][d] + G2 * H[1][d] + G3 * H[2][d] + G4 * Tl[d];
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) pg[d] += q[d];
+        // segmented sum over lanes of the same nucleus (AOs of a nucleus are
+        // contiguous, so segments are runs of lanes): the first lane of each
+        // run ends up with the run's sum
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+          const int ko = __shfl_down_sync(0xffffffffu, nl, off);
+          double o[3];
+#pragma unroll
+          for (int d = 0; d < 3; ++d) o[d] = __shfl_down_sync(0xffffffffu, q[d], off);
+          if (lane + off < 32 && ko == nl) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) q[d] += o[d];
+          }
+        }
+        const int kprev = __shfl_up_sync(0xffffffffu, nl, 1);
+        if ((lane == 0 || kprev != nl) && nl < kBlockNuc) {
+          const int n = blk.x + nl;
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            if (use_smem) atomicAdd(&sacc[n * 3 + d], q[d]);
+            else if (grad_nucl != nullptr) atomicAdd(&grad_nucl[n * 3 + d], -q[d]);
+          }
+        }
+      }
+    }
+    if (MODE == MODE_ADJOINT && grad_coord != nullptr) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        double s = pg[d];
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+        pg[d] = s;
+      }
+      if (lane == 0) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) atomicAdd(&grad_coord[p + d * gstride], pg[d]);
+      }
+    }
+    __syncwarp();
+  }
+  if (MODE == MODE_ADJOINT && use_smem && grad_nucl != nullptr) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < 3 * T.nucl_num; i += blockDim.x)
+      if (sacc[i] != 0.0) atomicAdd(&grad_nucl[i], -sacc[i]);
+  }
+}
+
+template <int MODE>
+cudaError_t launch_deriv(const DevTables& T, int64_t point_num, const double* coord, int64_t cstride, double cutoff,
+                         bool mixed, double* out, const double* G, double* grad_nucl, double* grad_coord,
+                         int64_t gstride, cudaStream_t s) {
+  if (point_num <= 0) return cudaSuccess;
+  const int64_t items = point_num * (int64_t)T.nblock;
+  const int grid = (int)std::min<int64_t>((items + kWarpsD - 1) / kWarpsD, 148 * 8);
+  size_t dyn = 0;
+  bool use_smem = false;
+  if (MODE == MODE_ADJOINT) {
+    dyn = sizeof(double) * 3 * (size_t)T.nucl_num;
+    use_smem = dyn <= 64 * 1024;
+    if (!use_smem) dyn = 0;
+  }
+  cudaError_t e = cudaSuccess;
+  if (mixed) {
+    auto k = deriv_kernel<MODE, true>;
+    if (dyn > 48 * 1024) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    if (e != cudaSuccess) return e;
+    k<<<grid, kWarpsD * 32, dyn, s>>>(T, point_num, coord, cstride, cutoff, out, G, grad_nucl, grad_coord, gstride,
+                                      use_smem);
+  } else {
+    auto k = deriv_kernel<MODE, false>;
+    if (dyn > 48 * 1024) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    if (e != cudaSuccess) return e;
+    k<<<grid, kWarpsD * 32, dyn, s>>>(T, point_num, coord, cstride, cutoff, out, G, grad_nucl, grad_coord, gstride,
+                                      use_smem);
+  }
+  count_launch();
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_ao_hessian(const DevTables& T, int64_t point_num, const double* coord, double cutoff, bool mixed,
+                              double* ao_hessian, cudaStream_t s) {
+  return launch_deriv<MODE_HESSIAN>(T, point_num, coord, point_num, cutoff, mixed, ao_hessian, nullptr, nullptr,
+                                    nullptr, 0, s);
+}
+
+cudaError_t launch_mo_adjoint_nuclear(const DevTables& T, int64_t point_num, const double* coord, int64_t cstride,
+                                      double cutoff, bool mixed, const double* G, double* grad_nucl,
+                                      double* grad_coord, int64_t gstride, cudaStream_t s) {
+  return launch_deriv<MODE_ADJOINT>(T, point_num, coord, cstride, cutoff, mixed, nullptr, G, grad_nucl, grad_coord,
+                                    gstride, s);
+}
+
+}  // namespace qb

@@ -481,6 +481,17 @@ qmckl_exit_code qmckl_get_ao_basis_ao_vgl_inplace(qmckl_context context, double*
   return dev_provide_ao_vgl(context, ao_vgl);
 }
 
+qmckl_exit_code qmckl_get_ao_basis_ao_hessian(qmckl_context context, double* const ao_hessian, const int64_t size_max) {
+  // org/qmckl_ao.org:9400-9440
+  if (qmckl_context_check(context) == QMCKL_NULL_CONTEXT) return QMCKL_NULL_CONTEXT;
+  Context* ctx = ctx_of(context);
+  if (!ctx->ao_basis.provided) return qmckl_failwith(context, QMCKL_NOT_PROVIDED, "qmckl_provide_ao_basis_ao_hessian", NULL);
+  const int64_t sze = ctx->ao_basis.ao_num * 4 * 3 * ctx->point.num;
+  if (size_max < sze) return qmckl_failwith(context, QMCKL_INVALID_ARG_3, "qmckl_get_ao_basis_ao_hessian", "input array too small");
+  if (ao_hessian == nullptr) return qmckl_failwith(context, QMCKL_INVALID_ARG_2, "qmckl_get_ao_basis_ao_hessian", "NULL pointer");
+  return dev_provide_ao_hessian(context, ao_hessian);
+}
+
 qmckl_exit_code qmckl_get_ao_basis_ao_value(qmckl_context context, double* const ao_value, const int64_t size_max) {
   if (qmckl_context_check(context) == QMCKL_NULL_CONTEXT)
     return qmckl_failwith(context, QMCKL_INVALID_CONTEXT, "qmckl_get_ao_basis_ao_value", NULL);

@@ -69,6 +69,11 @@ struct DeviceState {
   DevBuf order;      // point order of the fused kernel: keys[P], perm[P], cell counts
   int rec_bytes = 0;
   uint64_t krec_basis_version = ~0ull, krec_nucl_version = ~0ull;
+  // derivatives: AO Hessian and the MO VGL adjoint (FP64 coefficient [mo][ao],
+  // per-chunk coordinates, AO / pulled-back weight buffer, split-K partials)
+  DevBuf ao_hessian;
+  uint64_t coef_rows_version = ~0ull;
+  DevBuf coef_rows, adj_coord, adj_buf, adj_part, adj_nucl;
 };
 
 namespace {
@@ -543,7 +548,8 @@ void dev_detach(Context* ctx) {
   if (ds->device >= 0) cudaSetDevice(ds->device);
   if (ds->stream) cudaStreamSynchronize(ds->stream);
   for (DevBuf* b : {&ds->tables, &ds->nucl, &ds->coord, &ds->prim_vgl, &ds->shell_vgl, &ds->ao_vgl, &ds->ao_value,
-                    &ds->mo_vgl, &ds->mo_value, &ds->coef_t, &ds->tc_coef, &ds->tc_a, &ds->krec, &ds->order})
+                    &ds->mo_vgl, &ds->mo_value, &ds->coef_t, &ds->tc_coef, &ds->tc_a, &ds->krec, &ds->order,
+                    &ds->ao_hessian, &ds->coef_rows, &ds->adj_coord, &ds->adj_buf, &ds->adj_part, &ds->adj_nucl})
     release(*b);
   if (ds->own_stream && ds->stream) cudaStreamDestroy(ds->stream);
   delete ds;
@@ -665,6 +671,30 @@ qmckl_exit_code dev_provide_ao_value(qmckl_context context, double* host_out) {
     ctx->ao_basis.ao_value_date = ctx->date;
   }
   return copy_out(context, ds, host_out, ds->ao_value.p, bytes, "qmckl_get_ao_basis_ao_value");
+}
+
+// qmckl_provide_ao_basis_ao_hessian (org/qmckl_ao.org:9470-9540): recomputed
+// when the points are newer than the array.
+qmckl_exit_code dev_provide_ao_hessian(qmckl_context context, double* host_out) {
+  qmckl_exit_code rc = attach_all(context);
+  if (rc != QMCKL_SUCCESS) return rc;
+  Context* ctx = ctx_of(context);
+  DeviceState* ds = state(context);
+  if (ctx->ao_basis.type != 'G')
+    return qmckl_failwith(context, QMCKL_FAILURE, "qmckl_provide_ao_basis_ao_hessian", "only Gaussian basis sets are implemented");
+  const int64_t P = ctx->point.num, A = ctx->ao_basis.ao_num;
+  const size_t bytes = sizeof(double) * 12 * A * P;
+  if (ctx->point.date > ctx->ao_basis.ao_hessian_date || ds->ao_hessian.cap < bytes) {
+    rc = sync_inputs(context, ds, true);
+    if (rc != QMCKL_SUCCESS) return rc;
+    rc = ensure(context, ds->ao_hessian, bytes, "qmckl_provide_ao_basis_ao_hessian");
+    if (rc != QMCKL_SUCCESS) return rc;
+    QB_CUDA(launch_ao_hessian(ds->T, P, (const double*)ds->coord.p, cutoff_of(ctx), ctx->precision <= 23,
+                              (double*)ds->ao_hessian.p, ds->stream),
+            "qmckl_provide_ao_basis_ao_hessian");
+    ctx->ao_basis.ao_hessian_date = ctx->date;
+  }
+  return copy_out(context, ds, host_out, ds->ao_hessian.p, bytes, "qmckl_get_ao_basis_ao_hessian");
 }
 
 qmckl_exit_code dev_provide_mo_vgl(qmckl_context context, double* host_out) {
@@ -872,6 +902,85 @@ qmckl_exit_code qmckl_b200_mo_vgl_device(qmckl_context context, const int64_t po
 qmckl_exit_code qmckl_b200_mo_value_device(qmckl_context context, const int64_t point_num, const double* d_coord,
                                            double* d_mo_value) {
   return mo_device(context, "qmckl_b200_mo_value_device", point_num, d_coord, d_mo_value, 1);
+}
+
+qmckl_exit_code qmckl_b200_ao_hessian_device(qmckl_context context, const int64_t point_num, const double* d_coord,
+                                             double* d_ao_hessian) {
+  qmckl_exit_code rc =
+      device_entry(context, "qmckl_b200_ao_hessian_device", point_num, d_coord, d_ao_hessian, false);
+  if (rc != QMCKL_SUCCESS) return rc;
+  Context* ctx = ctx_of(context);
+  QB_CUDA(launch_ao_hessian(state(context)->T, point_num, d_coord, cutoff_of(ctx), ctx->precision <= 23, d_ao_hessian,
+                            state(context)->stream),
+          "qmckl_b200_ao_hessian_device");
+  return QMCKL_SUCCESS;
+}
+
+// Adjoint of MO VGL.  With L = sum_{p,c,i} W[p][c][i] mo_vgl[p][c][i]:
+//   grad_coef[i][k]  = sum_{p,c} W[p][c][i] ao_vgl[p][c][k]
+//   grad_nucl[a][d]  = dL/dR_a,  grad_coord[d][p] = dL/dr_p
+// Points are processed in chunks that bound the scratch to about 2 GiB.  Per
+// chunk: the AO matrix is recomputed (nothing of the forward pass is kept),
+// grad_coef accumulates AO^T W (split-K FP64 GEMM, partials summed in a fixed
+// order), the AO buffer is then overwritten with G = W C ([point][5][ao]) and
+// the derivative kernel contracts G with the AO Hessian and Laplacian
+// gradient into grad_nucl / grad_coord.
+qmckl_exit_code qmckl_b200_mo_vgl_adjoint_device(qmckl_context context, const int64_t point_num,
+                                                 const double* d_coord, const double* d_weight, double* d_grad_coef,
+                                                 double* d_grad_nucl, double* d_grad_coord) {
+  const char* fname = "qmckl_b200_mo_vgl_adjoint_device";
+  qmckl_exit_code rc = device_entry(context, fname, point_num, d_coord, (void*)d_weight, true);
+  if (rc != QMCKL_SUCCESS) return rc;
+  Context* ctx = ctx_of(context);
+  DeviceState* ds = state(context);
+  const int64_t P = point_num, A = ctx->ao_basis.ao_num, M = ctx->mo_basis.mo_num, N = ctx->nucleus.num;
+  const bool mixed = use_mixed(ctx) || ctx->precision <= 23;
+  const double cutoff = cutoff_of(ctx);
+  cudaStream_t s = ds->stream;
+  if (d_grad_coef) QB_CUDA(cudaMemsetAsync(d_grad_coef, 0, sizeof(double) * M * A, s), fname);
+  if (d_grad_nucl) QB_CUDA(cudaMemsetAsync(d_grad_nucl, 0, sizeof(double) * 3 * N, s), fname);
+  if (d_grad_coord) QB_CUDA(cudaMemsetAsync(d_grad_coord, 0, sizeof(double) * 3 * P, s), fname);
+  if (P == 0 || (!d_grad_coef && !d_grad_nucl && !d_grad_coord)) return QMCKL_SUCCESS;
+  // FP64 coefficient rows [mo][ao] for G = W C
+  if (ds->coef_rows_version != ctx->mo_basis.coef_version || !ds->coef_rows.p) {
+    rc = ensure(context, ds->coef_rows, sizeof(double) * M * A, fname);
+    if (rc != QMCKL_SUCCESS) return rc;
+    QB_CUDA(cudaMemcpyAsync(ds->coef_rows.p, ctx->mo_basis.coefficient.data(), sizeof(double) * M * A,
+                            cudaMemcpyHostToDevice, s), fname);
+    ds->coef_rows_version = ctx->mo_basis.coef_version;
+  }
+  const int64_t budget = (int64_t)2 << 30;
+  const int64_t chunk = std::min<int64_t>(P, std::max<int64_t>(64, budget / (int64_t)(40 * A)));
+  // split-K count: about two CTAs per SM for the (ao x mo) output tiles
+  const int64_t tiles = ((A + 127) / 128) * ((M + 79) / 80);
+  const int splits = (int)std::max<int64_t>(1, std::min<int64_t>(32, (2 * 148 + tiles - 1) / tiles));
+  rc = ensure(context, ds->adj_coord, sizeof(double) * 3 * chunk, fname);
+  if (rc == QMCKL_SUCCESS) rc = ensure(context, ds->adj_buf, sizeof(double) * 5 * chunk * A, fname);
+  if (rc == QMCKL_SUCCESS && d_grad_coef) rc = ensure(context, ds->adj_part, sizeof(double) * splits * A * M, fname);
+  if (rc == QMCKL_SUCCESS && !d_grad_nucl) rc = ensure(context, ds->adj_nucl, sizeof(double) * 3 * N, fname);
+  if (rc != QMCKL_SUCCESS) return rc;
+  double* gnucl = d_grad_nucl ? d_grad_nucl : (double*)ds->adj_nucl.p;
+  double* buf = (double*)ds->adj_buf.p;
+  double* cc = (double*)ds->adj_coord.p;
+  for (int64_t p0 = 0; p0 < P; p0 += chunk) {
+    const int64_t n = std::min<int64_t>(chunk, P - p0);
+    const double* w = d_weight + p0 * 5 * M;
+    QB_CUDA(cudaMemcpy2DAsync(cc, sizeof(double) * n, d_coord + p0, sizeof(double) * P, sizeof(double) * n, 3,
+                              cudaMemcpyDeviceToDevice, s), fname);
+    if (d_grad_coef) {
+      QB_CUDA(launch_ao_vgl_f64(ds->T, n, cc, cutoff, !mixed, buf, s), fname);
+      QB_CUDA(launch_gemm_f64_tn_split(A, M, 5 * n, buf, A, w, M, (double*)ds->adj_part.p, splits, s), fname);
+      QB_CUDA(launch_add_transposed((const double*)ds->adj_part.p, splits, A, M, d_grad_coef, true, s), fname);
+    }
+    if (d_grad_nucl || d_grad_coord) {
+      QB_CUDA(launch_gemm_f64(5 * n, A, M, w, M, (const double*)ds->coef_rows.p, A, buf, A, s), fname);
+      QB_CUDA(launch_mo_adjoint_nuclear(ds->T, n, cc, n, cutoff, mixed, buf, gnucl,
+                                        d_grad_coord ? d_grad_coord + p0 : nullptr, P, s),
+              fname);
+    }
+  }
+  // the AO scratch of the FP64 form was not touched; cached arrays stay valid
+  return QMCKL_SUCCESS;
 }
 
 }  // extern "C"

@@ -41,19 +41,30 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-template <int NT, int VA, int VB>
+// TA: A is stored transposed (element (m, k) at A[k * lda + m]); its shared
+// tile is then kept k-major ([BK][BM + 4]).  Split K: CTA z of the grid
+// covers k in [z * k_split, (z + 1) * k_split) and writes C + z * c_split.
+template <int NT, int VA, int VB, bool TA>
 __global__ void __launch_bounds__(256)
-dgemm_kernel(int64_t M, int64_t N, int64_t K, const double* __restrict__ A, int64_t lda,
-             const double* __restrict__ B, int64_t ldb, double* __restrict__ C, int64_t ldc) {
+dgemm_kernel(int64_t M, int64_t N, int64_t K, const double* __restrict__ A_, int64_t lda,
+             const double* __restrict__ B_, int64_t ldb, double* __restrict__ C_, int64_t ldc, int64_t k_split,
+             int64_t c_split) {
   constexpr int BN = 16 * NT;
   constexpr int LDB_S = BN + 4;
+  constexpr int LDT = BM + 4;                      // row stride of the k-major A tile (TA)
   extern __shared__ __align__(16) double smem[];
-  double* As = smem;                               // [STAGES][BM][LDA_S]
+  double* As = smem;                               // [STAGES][BM][LDA_S] or [STAGES][BK][LDT]
   double* Bs = smem + STAGES * BM * LDA_S;         // [STAGES][BK][LDB_S]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp & 3, wn = warp >> 2;
   const int g = lane >> 2, t = lane & 3;
   const int64_t n0 = (int64_t)blockIdx.x * BN;
+  const int64_t kz0 = (int64_t)blockIdx.z * k_split;
+  // an empty K range (last splits of a short K) still writes its zero slice
+  K = kz0 >= K ? 0 : ((K - kz0) < k_split ? (K - kz0) : k_split);
+  const double* __restrict__ A = A_ + (TA ? kz0 * lda : kz0);
+  const double* __restrict__ B = B_ + kz0 * ldb;
+  double* __restrict__ C = C_ + (int64_t)blockIdx.z * c_split;
   const int ktiles = (int)((K + BK - 1) / BK);
 
   for (int64_t mt = blockIdx.y; mt * BM < M; mt += gridDim.y) {
@@ -70,16 +81,30 @@ dgemm_kernel(int64_t M, int64_t N, int64_t K, const double* __restrict__ A, int6
       double* bs = Bs + st * BK * LDB_S;
       // A tile: BM x BK
       constexpr int ACH = BM * BK / VA;
+      if constexpr (TA) {
 #pragma unroll
-      for (int i = 0; i < ACH / 256; ++i) {
-        const int c = tid + i * 256;
-        const int row = c / (BK / VA), col = (c % (BK / VA)) * VA;
-        const int64_t gm = m0 + row, gk = k0 + col;
-        int bytes = 0;
-        if (gm < M && gk < K) bytes = (int)((K - gk) < VA ? (K - gk) : VA) * 8;
-        const double* src = bytes ? A + gm * lda + gk : A;
-        if (VA == 2) cp_async16(as + row * LDA_S + col, src, bytes);
-        else cp_async8(as + row * LDA_S + col, src, bytes);
+        for (int i = 0; i < ACH / 256; ++i) {
+          const int c = tid + i * 256;
+          const int kr = c / (BM / VA), mc = (c % (BM / VA)) * VA;
+          const int64_t gm = m0 + mc, gk = k0 + kr;
+          int bytes = 0;
+          if (gm < M && gk < K) bytes = (int)((M - gm) < VA ? (M - gm) : VA) * 8;
+          const double* src = bytes ? A + gk * lda + gm : A;
+          if (VA == 2) cp_async16(as + kr * LDT + mc, src, bytes);
+          else cp_async8(as + kr * LDT + mc, src, bytes);
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < ACH / 256; ++i) {
+          const int c = tid + i * 256;
+          const int row = c / (BK / VA), col = (c % (BK / VA)) * VA;
+          const int64_t gm = m0 + row, gk = k0 + col;
+          int bytes = 0;
+          if (gm < M && gk < K) bytes = (int)((K - gk) < VA ? (K - gk) : VA) * 8;
+          const double* src = bytes ? A + gm * lda + gk : A;
+          if (VA == 2) cp_async16(as + row * LDA_S + col, src, bytes);
+          else cp_async8(as + row * LDA_S + col, src, bytes);
+        }
       }
       // B tile: BK x BN
       constexpr int BCH = BK * BN / VB;
@@ -105,13 +130,14 @@ dgemm_kernel(int64_t M, int64_t N, int64_t K, const double* __restrict__ A, int6
       const int nk = kt + STAGES - 1;
       if (nk < ktiles) load_tile(nk, nk % STAGES);
       cp_commit();
-      const double* as = As + (kt % STAGES) * BM * LDA_S + (wm * 32) * LDA_S;
+      const double* as = As + (kt % STAGES) * BM * LDA_S;
       const double* bs = Bs + (kt % STAGES) * BK * LDB_S + wn * (8 * NT);
 #pragma unroll
       for (int kk = 0; kk < BK; kk += 4) {
         double af[4], bf[NT];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) af[i] = as[(i * 8 + g) * LDA_S + kk + t];
+        for (int i = 0; i < 4; ++i)
+          af[i] = TA ? as[(kk + t) * LDT + wm * 32 + i * 8 + g] : as[(wm * 32 + i * 8 + g) * LDA_S + kk + t];
 #pragma unroll
         for (int j = 0; j < NT; ++j) bf[j] = bs[(kk + t) * LDB_S + j * 8 + g];
 #pragma unroll
@@ -142,41 +168,85 @@ dgemm_kernel(int64_t M, int64_t N, int64_t K, const double* __restrict__ A, int6
   }
 }
 
-template <int NT, int VA, int VB>
+template <int NT, int VA, int VB, bool TA>
 cudaError_t run(int64_t M, int64_t N, int64_t K, const double* A, int64_t lda, const double* B,
-                int64_t ldb, double* C, int64_t ldc, cudaStream_t s) {
+                int64_t ldb, double* C, int64_t ldc, int splits, cudaStream_t s) {
   constexpr int BN = 16 * NT;
   const size_t smem = sizeof(double) * STAGES * (BM * LDA_S + BK * (BN + 4));
-  auto kern = dgemm_kernel<NT, VA, VB>;
+  auto kern = dgemm_kernel<NT, VA, VB, TA>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const int64_t mt = (M + BM - 1) / BM;
-  dim3 grid((unsigned)((N + BN - 1) / BN), (unsigned)std::min<int64_t>(mt, 65535));
-  kern<<<grid, 256, smem, s>>>(M, N, K, A, lda, B, ldb, C, ldc);
+  const int64_t k_split = ((K + splits - 1) / splits + BK - 1) / BK * BK;
+  dim3 grid((unsigned)((N + BN - 1) / BN), (unsigned)std::min<int64_t>(mt, 65535), (unsigned)splits);
+  kern<<<grid, 256, smem, s>>>(M, N, K, A, lda, B, ldb, C, ldc, k_split, M * ldc);
   count_launch();
   return cudaGetLastError();
 }
 
-template <int NT>
+template <int NT, bool TA>
 cudaError_t run_nt(int64_t M, int64_t N, int64_t K, const double* A, int64_t lda, const double* B,
-                   int64_t ldb, double* C, int64_t ldc, cudaStream_t s) {
+                   int64_t ldb, double* C, int64_t ldc, int splits, cudaStream_t s) {
   const bool va = (lda % 2 == 0) && ((uintptr_t)A % 16 == 0);
   const bool vb = (ldb % 2 == 0) && ((uintptr_t)B % 16 == 0);
-  if (va && vb) return run<NT, 2, 2>(M, N, K, A, lda, B, ldb, C, ldc, s);
-  if (va) return run<NT, 2, 1>(M, N, K, A, lda, B, ldb, C, ldc, s);
-  if (vb) return run<NT, 1, 2>(M, N, K, A, lda, B, ldb, C, ldc, s);
-  return run<NT, 1, 1>(M, N, K, A, lda, B, ldb, C, ldc, s);
+  if (va && vb) return run<NT, 2, 2, TA>(M, N, K, A, lda, B, ldb, C, ldc, splits, s);
+  if (va) return run<NT, 2, 1, TA>(M, N, K, A, lda, B, ldb, C, ldc, splits, s);
+  if (vb) return run<NT, 1, 2, TA>(M, N, K, A, lda, B, ldb, C, ldc, splits, s);
+  return run<NT, 1, 1, TA>(M, N, K, A, lda, B, ldb, C, ldc, splits, s);
+}
+
+template <bool TA>
+cudaError_t run_any(int64_t M, int64_t N, int64_t K, const double* A, int64_t lda, const double* B, int64_t ldb,
+                    double* C, int64_t ldc, int splits, cudaStream_t s) {
+  if (M <= 0 || N <= 0) return cudaSuccess;
+  // pick the N tile (64 or 80 columns) that wastes fewer padded columns
+  const int64_t w64 = ((N + 63) / 64) * 64 - N, w80 = ((N + 79) / 80) * 80 - N;
+  if (w80 < w64) return run_nt<5, TA>(M, N, K, A, lda, B, ldb, C, ldc, splits, s);
+  return run_nt<4, TA>(M, N, K, A, lda, B, ldb, C, ldc, splits, s);
+}
+
+// out[n][m] (+)= sum_z part[z][m][n], through 32 x 32 shared tiles
+__global__ void add_transposed_kernel(const double* __restrict__ part, int splits, int64_t M, int64_t N,
+                                      double* __restrict__ out, bool accumulate) {
+  __shared__ double tile[32][33];
+  const int64_t m0 = (int64_t)blockIdx.y * 32, n0 = (int64_t)blockIdx.x * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int64_t m = m0 + r, n = n0 + threadIdx.x;
+    double v = 0.0;
+    if (m < M && n < N)
+      for (int z = 0; z < splits; ++z) v += part[((int64_t)z * M + m) * N + n];
+    tile[r][threadIdx.x] = v;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int64_t n = n0 + r, m = m0 + threadIdx.x;
+    if (m < M && n < N) {
+      double* o = out + n * M + m;
+      *o = accumulate ? *o + tile[threadIdx.x][r] : tile[threadIdx.x][r];
+    }
+  }
 }
 
 }  // namespace
 
 cudaError_t launch_gemm_f64(int64_t M, int64_t N, int64_t K, const double* A, int64_t lda,
                             const double* B, int64_t ldb, double* C, int64_t ldc, cudaStream_t s) {
+  return run_any<false>(M, N, K, A, lda, B, ldb, C, ldc, 1, s);
+}
+
+cudaError_t launch_gemm_f64_tn_split(int64_t M, int64_t N, int64_t K, const double* A, int64_t lda, const double* B,
+                                     int64_t ldb, double* part, int splits, cudaStream_t s) {
+  if (splits < 1) return cudaErrorInvalidValue;
+  return run_any<true>(M, N, K, A, lda, B, ldb, part, N, splits, s);
+}
+
+cudaError_t launch_add_transposed(const double* part, int splits, int64_t M, int64_t N, double* out, bool accumulate,
+                                  cudaStream_t s) {
   if (M <= 0 || N <= 0) return cudaSuccess;
-  // pick the N tile (64 or 80 columns) that wastes fewer padded columns
-  const int64_t w64 = ((N + 63) / 64) * 64 - N, w80 = ((N + 79) / 80) * 80 - N;
-  if (w80 < w64) return run_nt<5>(M, N, K, A, lda, B, ldb, C, ldc, s);
-  return run_nt<4>(M, N, K, A, lda, B, ldb, C, ldc, s);
+  dim3 grid((unsigned)((N + 31) / 32), (unsigned)((M + 31) / 32));
+  add_transposed_kernel<<<grid, dim3(32, 8), 0, s>>>(part, splits, M, N, out, accumulate);
+  count_launch();
+  return cudaGetLastError();
 }
 
 }  // namespace qb

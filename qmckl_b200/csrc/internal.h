@@ -83,7 +83,7 @@ struct AoBasisRec {               // org/qmckl_ao.org:148-206
   bool r_power_set = false;
   AoDerived d;
   uint64_t basis_version = 0;     // bumped by each finalization
-  uint64_t primitive_vgl_date = 0, shell_vgl_date = 0, ao_vgl_date = 0, ao_value_date = 0;
+  uint64_t primitive_vgl_date = 0, shell_vgl_date = 0, ao_vgl_date = 0, ao_value_date = 0, ao_hessian_date = 0;
   int32_t uninitialized = (1 << 14) - 1;
   bool provided = false;
   bool ao_cartesian = true;
@@ -131,6 +131,7 @@ qmckl_exit_code dev_provide_primitive_vgl(qmckl_context context, double* host_ou
 qmckl_exit_code dev_provide_shell_vgl(qmckl_context context, double* host_out);
 qmckl_exit_code dev_provide_ao_vgl(qmckl_context context, double* host_out);
 qmckl_exit_code dev_provide_ao_value(qmckl_context context, double* host_out);
+qmckl_exit_code dev_provide_ao_hessian(qmckl_context context, double* host_out);
 qmckl_exit_code dev_provide_mo_vgl(qmckl_context context, double* host_out);
 qmckl_exit_code dev_provide_mo_value(qmckl_context context, double* host_out);
 qmckl_exit_code dev_invalidate_mo(qmckl_context context);

@@ -68,4 +68,23 @@ cudaError_t launch_ao_vgl_split(const DevTables& T, int64_t point_num, const dou
 cudaError_t launch_gemm_f64(int64_t M, int64_t N, int64_t K, const double* A, int64_t lda,
                             const double* B, int64_t ldb, double* C, int64_t ldc, cudaStream_t s);
 
+// Split-K FP64 GEMM with A transposed: part[z][m][n] = sum over the z-th K
+// range of A[k][m] * B[k][n] (A element (m, k) at A[k * lda + m]), for
+// z < splits; part is [splits][M][N].
+cudaError_t launch_gemm_f64_tn_split(int64_t M, int64_t N, int64_t K, const double* A, int64_t lda, const double* B,
+                                     int64_t ldb, double* part, int splits, cudaStream_t s);
+// out[n][m] = (out[n][m] +) sum_z part[z][m][n]  (fixed summation order)
+cudaError_t launch_add_transposed(const double* part, int splits, int64_t M, int64_t N, double* out, bool accumulate,
+                                  cudaStream_t s);
+
+// Derivative kernels (adjoint.cu).  ao_hessian: [3][point_num][4][ao]
+// (coord [3][point_num]).  Adjoint: G [point_num][5][ao]; grad_nucl
+// [nucl][3] -= and grad_coord [3][gstride] += (may be null); coord
+// [3][cstride].  `mixed` selects FP32 exponentials where a r^2 <= 30.
+cudaError_t launch_ao_hessian(const DevTables& T, int64_t point_num, const double* coord, double cutoff, bool mixed,
+                              double* ao_hessian, cudaStream_t s);
+cudaError_t launch_mo_adjoint_nuclear(const DevTables& T, int64_t point_num, const double* coord, int64_t cstride,
+                                      double cutoff, bool mixed, const double* G, double* grad_nucl,
+                                      double* grad_coord, int64_t gstride, cudaStream_t s);
+
 }  // namespace qb

@@ -306,6 +306,7 @@ get_ao_basis_ao_vgl = _array_getter("qmckl_get_ao_basis_ao_vgl")
 get_ao_basis_ao_vgl_inplace = _array_getter("qmckl_get_ao_basis_ao_vgl_inplace")
 get_ao_basis_ao_value = _array_getter("qmckl_get_ao_basis_ao_value")
 get_ao_basis_ao_value_inplace = _array_getter("qmckl_get_ao_basis_ao_value_inplace")
+get_ao_basis_ao_hessian = _array_getter("qmckl_get_ao_basis_ao_hessian")
 
 # ------------------------------------------------------------- MO basis
 
@@ -391,6 +392,15 @@ b200_ao_vgl_device = _device_entry("qmckl_b200_ao_vgl_device")
 b200_ao_value_device = _device_entry("qmckl_b200_ao_value_device")
 b200_mo_vgl_device = _device_entry("qmckl_b200_mo_vgl_device")
 b200_mo_value_device = _device_entry("qmckl_b200_mo_value_device")
+b200_ao_hessian_device = _device_entry("qmckl_b200_ao_hessian_device")
+
+
+def b200_mo_vgl_adjoint_device(ctx, point_num, d_coord_ptr, d_weight_ptr, d_grad_coef_ptr=0, d_grad_nucl_ptr=0,
+                               d_grad_coord_ptr=0):
+    """Gradient of sum(weight * mo_vgl); pointers of device buffers, 0 for an output not wanted."""
+    _call("qmckl_b200_mo_vgl_adjoint_device", ctx, C.c_int64(point_num), C.c_void_p(d_coord_ptr),
+          C.c_void_p(d_weight_ptr), C.c_void_p(d_grad_coef_ptr or None), C.c_void_p(d_grad_nucl_ptr or None),
+          C.c_void_p(d_grad_coord_ptr or None))
 
 
 def b200_kernel_launch_count():
