@@ -86,6 +86,49 @@ qmckl_exit_code qmckl_b200_mo_vgl_adjoint_device(qmckl_context context, const in
                                                  const double* d_coord, const double* d_weight,
                                                  double* d_grad_coef, double* d_grad_nucl, double* d_grad_coord);
 
+/* Batched MO VGL (mixed form) of many independent systems in one persistent
+ * launch driven by a device work queue (no counterpart in the reference,
+ * which evaluates one context at a time).  A batch snapshots, at creation,
+ * the basis, nuclei, MO coefficients and precision of each context and takes
+ * the number of points of each system; re-create it after changing a
+ * context.  Coordinates and results are packed device buffers: system s
+ * reads [3][point_num[s]] doubles at d_coord + coord_offset[s] and writes
+ * mo_vgl[point_num[s]][5][mo_num_s] at d_mo_vgl + out_offset[s]
+ * (qmckl_b200_batch_layout; totals[0], totals[1] = buffer lengths in
+ * doubles).  qmckl_b200_batch_mo_vgl_device enqueues one persistent launch
+ * (replayed from a CUDA graph while the buffers and tuning stay the same;
+ * qmckl_b200_batch_set_graph(b, 0) launches directly) on the batch's own
+ * stream or the one set by qmckl_b200_batch_set_stream (graph capture needs
+ * a stream other than the legacy default one); qmckl_b200_batch_synchronize
+ * waits and returns QMCKL_FAILURE when a bounded wait of the launch gave up
+ * (*status = its code).  qmckl_b200_batch_mo_vgl_loop_device computes the
+ * same with one launch sequence per system (synchronous).
+ * qmckl_b200_batch_tune times the kernel variants (producer warps 16 or 8,
+ * queue order 0: largest work per tile first, 1: system by system, 2: round
+ * robin) on the given buffers and keeps the fastest (*best_ms: its time);
+ * QMCKL_B200_TUNE_FILE names a file where choices are appended and read back
+ * for batches of the same shape.  qmckl_b200_batch_set_wait_limit bounds the
+ * dependency waits of tile items to `polls` polls (0: 2 s); publish = 0 keeps
+ * the point-order items from releasing their systems (test hook: every wait
+ * then fails and the launch ends with an error status). */
+typedef int64_t qmckl_b200_batch;
+qmckl_exit_code qmckl_b200_batch_create(const qmckl_context* contexts, const int64_t* point_num, const int64_t num,
+                                        qmckl_b200_batch* batch);
+qmckl_exit_code qmckl_b200_batch_destroy(qmckl_b200_batch batch);
+qmckl_exit_code qmckl_b200_batch_layout(qmckl_b200_batch batch, int64_t* coord_offset, int64_t* out_offset,
+                                        int64_t* totals);
+qmckl_exit_code qmckl_b200_batch_set_stream(qmckl_b200_batch batch, void* stream);
+qmckl_exit_code qmckl_b200_batch_set_graph(qmckl_b200_batch batch, const int32_t enable);
+qmckl_exit_code qmckl_b200_batch_mo_vgl_device(qmckl_b200_batch batch, const double* d_coord, double* d_mo_vgl);
+qmckl_exit_code qmckl_b200_batch_mo_vgl_loop_device(qmckl_b200_batch batch, const double* d_coord,
+                                                    double* d_mo_vgl);
+qmckl_exit_code qmckl_b200_batch_synchronize(qmckl_b200_batch batch, int32_t* status);
+qmckl_exit_code qmckl_b200_batch_tune(qmckl_b200_batch batch, const double* d_coord, double* d_mo_vgl,
+                                      const int32_t reps, double* best_ms);
+qmckl_exit_code qmckl_b200_batch_set_tuning(qmckl_b200_batch batch, const int32_t producer_warps, const int32_t order);
+qmckl_exit_code qmckl_b200_batch_get_tuning(qmckl_b200_batch batch, int32_t* producer_warps, int32_t* order);
+qmckl_exit_code qmckl_b200_batch_set_wait_limit(qmckl_b200_batch batch, const int64_t polls, const int32_t publish);
+
 /* Mixed-form MO VGL that allocates no device memory.  No counterpart in the
  * reference library.
  *

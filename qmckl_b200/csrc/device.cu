@@ -25,6 +25,87 @@
 
 namespace qb {
 
+// Records of the fused kernels: one per 64-AO K block, everything its AO
+// producers read (layout in fused_common.cuh), from the finalized basis and
+// the nuclear coordinates of a context.  rec_bytes is the common record size
+// (a multiple of 128).  Returns false when the AOs are not numbered shell by
+// shell in increasing order.
+bool build_krec_records(const Context* ctx, std::vector<uint8_t>& h, int& rec_bytes) {
+  const AoBasisRec& B = ctx->ao_basis;
+  const AoDerived& d = B.d;
+  const int64_t A = B.ao_num, N = ctx->nucleus.num, S = B.shell_num;
+  if (A <= 0 || (int64_t)ctx->nucleus.coord.size() < 3 * N) return false;
+  std::vector<int32_t> aosh(A, -1), code(A, 0), shell_nuc(S, 0);
+  for (int64_t m = 0; m < N; ++m)
+    for (int64_t s = B.nucleus_index[m]; s < B.nucleus_index[m] + B.nucleus_shell_num[m]; ++s) shell_nuc[s] = (int32_t)m;
+  for (int64_t s = 0; s < S; ++s) {
+    const int l = B.shell_ang_mom[s];
+    int64_t k = d.ao_index[s];
+    for (int a = l; a >= 0; --a)
+      for (int b = l - a; b >= 0; --b) {
+        if (k < A) {
+          aosh[k] = (int32_t)s;
+          code[k] = a | (b << 4) | ((l - a - b) << 8) | (l << 12);
+        }
+        ++k;
+      }
+  }
+  for (int64_t k = 0; k < A; ++k)
+    if (aosh[k] < 0 || (k > 0 && aosh[k] < aosh[k - 1])) return false;
+  const int64_t nkb = (A + 63) / 64;
+  struct KRecShell { double x, y, z, range; int32_t pb, pe, pad0, pad1; };
+  size_t rec = 0;
+  for (int64_t kb = 0; kb < nkb; ++kb) {
+    const int64_t k0 = kb * 64, k1 = std::min<int64_t>(k0 + 64, A);
+    const int s0 = aosh[k0], s1 = aosh[k1 - 1];
+    size_t np = 0;
+    for (int sh = s0; sh <= s1; ++sh) np += d.shell_coef_start[sh + 1] - d.shell_coef_start[sh];
+    rec = std::max(rec, 16 + 64 * 8 + (size_t)(s1 - s0 + 1) * sizeof(KRecShell) + np * 16);
+  }
+  rec = (rec + 127) / 128 * 128;
+  h.assign(rec * nkb, 0);
+  for (int64_t kb = 0; kb < nkb; ++kb) {
+    uint8_t* r = h.data() + kb * rec;
+    const int64_t k0 = kb * 64, k1 = std::min<int64_t>(k0 + 64, A);
+    const int s0 = aosh[k0], s1 = aosh[k1 - 1];
+    int32_t* hdr = (int32_t*)r;
+    int32_t* ao = (int32_t*)(r + 16);
+    KRecShell* sh = (KRecShell*)(r + 16 + 64 * 8);
+    double* prm = (double*)(r + 16 + 64 * 8 + (size_t)(s1 - s0 + 1) * sizeof(KRecShell));
+    hdr[0] = s1 - s0 + 1;
+    for (int64_t t = 0; t < 64; ++t) {
+      const int64_t k = k0 + t;
+      if (k < k1) {
+        const float f = (float)B.ao_factor[k];
+        ao[2 * t] = code[k] | ((aosh[k] - s0) << 16);
+        std::memcpy(&ao[2 * t + 1], &f, 4);
+      } else {
+        ao[2 * t] = -1;
+        ao[2 * t + 1] = 0;
+      }
+    }
+    int np = 0;
+    for (int q = s0; q <= s1; ++q) {
+      const int n = shell_nuc[q];
+      KRecShell& e = sh[q - s0];
+      e.x = ctx->nucleus.coord[n];
+      e.y = ctx->nucleus.coord[n + N];
+      e.z = ctx->nucleus.coord[n + 2 * N];
+      e.range = d.nucleus_range[n];
+      e.pb = np;
+      for (int j = d.shell_coef_start[q]; j < d.shell_coef_start[q + 1]; ++j) {
+        prm[2 * np] = d.expo_sorted[d.nuc_prim_start[n] + d.coef_prim[j]];
+        prm[2 * np + 1] = d.coef_val[j];
+        ++np;
+      }
+      e.pe = np;
+    }
+    hdr[1] = np;
+  }
+  rec_bytes = (int)rec;
+  return true;
+}
+
 static std::atomic<int64_t> g_launches{0};
 void count_launch(int n) { g_launches += n; }
 
@@ -64,7 +145,6 @@ struct DeviceState {
   // mixed form: fused AO -> MO kernel (default) instead of AO pieces in device memory + GEMM
   bool fused = true;
   // per-K-block records of the fused kernel (rebuilt on basis or nuclear moves)
-  std::vector<int32_t> h_ao_shell, h_ao_code, h_shell_nuc;
   DevBuf krec;
   DevBuf order;      // point order of the fused kernel: keys[P], perm[P], cell counts
   int rec_bytes = 0;
@@ -228,9 +308,6 @@ qmckl_exit_code upload_tables(qmckl_context context, DeviceState* ds) {
     const int l = B.shell_ang_mom[s];
     for (int64_t k = d.ao_index[s]; k < d.ao_index[s] + (l + 1) * (l + 2) / 2 && k < A; ++k) ao_shell[k] = (int32_t)s;
   }
-  ds->h_ao_shell = ao_shell;
-  ds->h_ao_code = ao_code;
-  ds->h_shell_nuc = shell_nuc;
   const size_t o_aosh = put(ao_shell.data(), sizeof(int32_t) * A);
   const size_t o_shco = put(shell_coef.data(), sizeof(int2) * S);
   // AO tiles of the tiled kernels (ao_tile.cu)
@@ -370,73 +447,17 @@ qmckl_exit_code run_ao_value(qmckl_context context, DeviceState* ds, int64_t P, 
   return QMCKL_SUCCESS;
 }
 
-// Records of the fused kernel: one per 64-AO K block, everything its AO
-// producers read (see the layout in fused_tc.cu).  Returns false when the AO
-// numbering does not allow them (then the unfused kernels are used).
+// Device copy of the K-block records of the fused kernel (built by
+// build_krec_records).  Returns false when the AO numbering does not allow
+// them (then the unfused kernels are used).
 bool build_krec(qmckl_context context, DeviceState* ds) {
   Context* ctx = ctx_of(context);
-  const AoBasisRec& B = ctx->ao_basis;
-  const AoDerived& d = B.d;
-  const int64_t A = B.ao_num, N = ctx->nucleus.num;
-  const std::vector<int32_t>& aosh = ds->h_ao_shell;
-  if ((int64_t)aosh.size() != A) return false;
-  for (int64_t k = 1; k < A; ++k)
-    if (aosh[k] < aosh[k - 1]) return false;
-  const int64_t nkb = (A + 63) / 64;
-  struct KRecShell { double x, y, z, range; int32_t pb, pe, pad0, pad1; };
-  std::vector<size_t> sizes(nkb);
-  size_t rec = 0;
-  for (int64_t kb = 0; kb < nkb; ++kb) {
-    const int64_t k0 = kb * 64, k1 = std::min<int64_t>(k0 + 64, A);
-    const int s0 = aosh[k0], s1 = aosh[k1 - 1];
-    size_t np = 0;
-    for (int sh = s0; sh <= s1; ++sh) np += d.shell_coef_start[sh + 1] - d.shell_coef_start[sh];
-    sizes[kb] = 16 + 64 * 8 + (size_t)(s1 - s0 + 1) * sizeof(KRecShell) + np * 16;
-    rec = std::max(rec, sizes[kb]);
-  }
-  rec = (rec + 127) / 128 * 128;
-  std::vector<uint8_t> h(rec * nkb, 0);
-  for (int64_t kb = 0; kb < nkb; ++kb) {
-    uint8_t* r = h.data() + kb * rec;
-    const int64_t k0 = kb * 64, k1 = std::min<int64_t>(k0 + 64, A);
-    const int s0 = aosh[k0], s1 = aosh[k1 - 1];
-    int32_t* hdr = (int32_t*)r;
-    int32_t* ao = (int32_t*)(r + 16);
-    KRecShell* sh = (KRecShell*)(r + 16 + 64 * 8);
-    double* prm = (double*)(r + 16 + 64 * 8 + (size_t)(s1 - s0 + 1) * sizeof(KRecShell));
-    hdr[0] = s1 - s0 + 1;
-    for (int64_t t = 0; t < 64; ++t) {
-      const int64_t k = k0 + t;
-      if (k < k1) {
-        const float f = (float)B.ao_factor[k];
-        ao[2 * t] = (ds->h_ao_code[k] & 0xFFFF) | ((aosh[k] - s0) << 16);
-        std::memcpy(&ao[2 * t + 1], &f, 4);
-      } else {
-        ao[2 * t] = -1;
-        ao[2 * t + 1] = 0;
-      }
-    }
-    int np = 0;
-    for (int q = s0; q <= s1; ++q) {
-      const int n = ds->h_shell_nuc[q];
-      KRecShell& e = sh[q - s0];
-      e.x = ctx->nucleus.coord[n];
-      e.y = ctx->nucleus.coord[n + N];
-      e.z = ctx->nucleus.coord[n + 2 * N];
-      e.range = d.nucleus_range[n];
-      e.pb = np;
-      for (int j = d.shell_coef_start[q]; j < d.shell_coef_start[q + 1]; ++j) {
-        prm[2 * np] = d.expo_sorted[d.nuc_prim_start[n] + d.coef_prim[j]];
-        prm[2 * np + 1] = d.coef_val[j];
-        ++np;
-      }
-      e.pe = np;
-    }
-    hdr[1] = np;
-  }
+  std::vector<uint8_t> h;
+  int rec = 0;
+  if (!build_krec_records(ctx, h, rec)) return false;
   if (ensure(context, ds->krec, h.size(), "qmckl_b200_mo_mixed") != QMCKL_SUCCESS) return false;
   if (cudaMemcpy(ds->krec.p, h.data(), h.size(), cudaMemcpyHostToDevice) != cudaSuccess) return false;
-  ds->rec_bytes = (int)rec;
+  ds->rec_bytes = rec;
   ds->krec_basis_version = ctx->ao_basis.basis_version;
   ds->krec_nucl_version = ctx->nucleus.coord_version;
   return true;

@@ -1,0 +1,296 @@
+// Device pieces shared by the fused AO -> MO kernels (fused_tc.cu: one
+// system, one tile per CTA; batch_tc.cu: many systems, persistent CTAs fed by
+// a device work queue).
+//
+// A CTA owns a tile of points and an N tile of MOs.  Its 128 accumulator rows
+// are (point, component) pairs: 25 points x 5 components (+3 zero rows) for
+// MO VGL, 128 points for MO value.  Per 64-AO K block, producer warps evaluate
+// the block's AOs at the tile's points and write them as bfloat16 split pieces
+// straight into the 128B-swizzled K-major shared-memory tile the tensor core
+// reads; the coefficient pieces arrive by TMA; one thread issues the
+// split-BF16 tcgen05.mma chain into three FP32 TMEM accumulators (leading
+// product in two K halves, corrections in the third); the epilogue sums them
+// in FP64.
+//
+// AO arithmetic (mixed form): FP64 displacement, r^2, exponent argument and
+// radial Laplacian factor, FP32 exponential when a r^2 <= 30 (FP64 above),
+// FP64 radial accumulation, FP32 monomials and product rule; the screening
+// follows qmckl_compute_ao_vgl_hpc_gaussian (org/qmckl_ao.org:8601-8973).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include "tc_ptx.cuh"
+
+namespace qb {
+namespace fz {
+
+using namespace tcx;
+
+constexpr int BM = 128, BK = 64, UMMA_K = 16;
+constexpr int A_TILE = BM * BK * 2;
+
+// Per-K-block record (built on the host): everything the producers need for
+// the block's 64 AOs, so they never read device memory.
+//   [0]    int32 nsh, nprim, 0, 0
+//   [16]   64 x {int32 code (a|b<<4|c<<8|l<<12|local_shell<<16, -1 past ao_num), float ao_factor}
+//   [528]  nsh x KRecShell
+//   [...]  nprim x {double exponent, double coefficient} (sorted per shell)
+struct KRecShell {
+  double x, y, z, range;
+  int32_t pb, pe, pad0, pad1;
+};
+constexpr int kRecAoOff = 16;
+constexpr int kRecShellOff = 16 + 64 * 8;
+
+// Radial VGL of one shell at one point from a K-block record in shared memory.
+__device__ __forceinline__ void radial_rec(const KRecShell& S, const double2* prm, double px, double py, double pz,
+                                           double cutoff, float (&s)[5], float& fx, float& fy, float& fz,
+                                           bool& live) {
+  const double x = px - S.x;
+  const double y = py - S.y;
+  const double z = pz - S.z;
+  const double r2 = x * x + y * y + z * z;
+  fx = (float)x;
+  fy = (float)y;
+  fz = (float)z;
+  double acc[5] = {0., 0., 0., 0., 0.};
+  live = !(r2 > cutoff * S.range);
+  if (live) {
+    for (int j = S.pb; j < S.pe; ++j) {
+      const double2 pc = prm[j];
+      const double ar2 = pc.x * r2;
+      if (ar2 > cutoff) break;   // sorted by exponent
+      const double e = ar2 > 30.0 ? exp(-ar2) : (double)expf(-(float)ar2);
+      const double f = -2.0 * pc.x * e;
+      acc[0] += pc.y * e;
+      acc[1] += pc.y * (f * x);
+      acc[2] += pc.y * (f * y);
+      acc[3] += pc.y * (f * z);
+      acc[4] += pc.y * (f * (3.0 - 2.0 * ar2));
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 5; ++c) s[c] = (float)acc[c];
+}
+
+// Value, gradient and Laplacian of one AO from its shell's radial VGL (FP32).
+__device__ __forceinline__ void ao_product(int code, float f, const float (&s)[5], float x, float y, float z,
+                                           float (&v)[5]) {
+  const int ax = code & 15, by = (code >> 4) & 15, cz = (code >> 8) & 15, l = (code >> 12) & 15;
+  if (l == 0) {
+#pragma unroll
+    for (int c = 0; c < 5; ++c) v[c] = s[c] * f;
+    return;
+  }
+  float P0, P1, P2, P3, P4;
+  if (l == 1) {
+    P0 = ax ? x : (by ? y : z);
+    P1 = (float)ax; P2 = (float)by; P3 = (float)cz; P4 = 0.f;
+  } else {
+    float pa = 1.f, pb = 1.f, pc = 1.f, pa1 = 1.f, pb1 = 1.f, pc1 = 1.f, pa2 = 1.f, pb2 = 1.f, pc2 = 1.f;
+    if (l <= 3) {   // branch-free powers
+      const float x2 = x * x, y2 = y * y, z2 = z * z;
+      const float xs[4] = {1.f, x, x2, x2 * x}, ys[4] = {1.f, y, y2, y2 * y}, zs[4] = {1.f, z, z2, z2 * z};
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (ax == q) { pa = xs[q]; pa1 = q >= 1 ? xs[q - 1] : 1.f; pa2 = q >= 2 ? xs[q - 2] : 1.f; }
+        if (by == q) { pb = ys[q]; pb1 = q >= 1 ? ys[q - 1] : 1.f; pb2 = q >= 2 ? ys[q - 2] : 1.f; }
+        if (cz == q) { pc = zs[q]; pc1 = q >= 1 ? zs[q - 1] : 1.f; pc2 = q >= 2 ? zs[q - 2] : 1.f; }
+      }
+    } else {
+      for (int i = 0; i < ax; ++i) { pa2 = pa1; pa1 = pa; pa *= x; }
+      for (int i = 0; i < by; ++i) { pb2 = pb1; pb1 = pb; pb *= y; }
+      for (int i = 0; i < cz; ++i) { pc2 = pc1; pc1 = pc; pc *= z; }
+    }
+    float xy = pa * pb, yz = pb * pc, xz = pa * pc;
+    P0 = xy * pc;
+    xy *= (float)cz; xz *= (float)by; yz *= (float)ax;
+    P1 = pa1 * yz; P2 = pb1 * xz; P3 = pc1 * xy;
+    P4 = (float)(ax - 1) * pa2 * yz + (float)(by - 1) * pb2 * xz + (float)(cz - 1) * pc2 * xy;
+  }
+  v[0] = P0 * s[0] * f;
+  v[1] = (P1 * s[0] + P0 * s[1]) * f;
+  v[2] = (P2 * s[0] + P0 * s[2]) * f;
+  v[3] = (P3 * s[0] + P0 * s[3]) * f;
+  v[4] = (P4 * s[0] + P0 * s[4] + 2.f * (P1 * s[1] + P2 * s[2] + P3 * s[3])) * f;
+}
+
+// One producer warp's share of a K block: AOs [CHUNK*j, CHUNK*j + CHUNK) of
+// the block (record `rec`) at the tile's points (pts [3][PTS] in shared
+// memory; lanes are points), written as PIECES bfloat16 pieces into the
+// swizzled A tiles at a_base (shared address; pieces A_TILE bytes apart).
+// p_first: index of the tile's first point among the P points (rows past P
+// are written as zeros).  Pairs of AOs that are zero at every point of the
+// warp skip the split arithmetic.
+template <int PIECES, int COMPS, int CHUNK>
+__device__ __forceinline__ void produce_kblock(const uint8_t* rec, const double* pts, int64_t p_first, int64_t P,
+                                               double cutoff, uint32_t a_base, int j, int lane) {
+  static_assert(CHUNK == 4 || CHUNK == 8, "a producer warp covers a half or a whole 16-byte chunk");
+  constexpr int PTS = BM / COMPS;
+  const int2* rao = (const int2*)(rec + kRecAoOff) + j * CHUNK;
+  const KRecShell* rsh = (const KRecShell*)(rec + kRecShellOff);
+  const double2* rprm = (const double2*)(rec + kRecShellOff + ((const int*)rec)[0] * (int)sizeof(KRecShell));
+  for (int g = 0; g < (PTS + 31) / 32; ++g) {
+    const int i = lane + 32 * g;
+    const int ic = i < PTS ? i : PTS - 1;
+    const bool active = i < PTS && p_first + i < P;
+    const double px = pts[ic], py = pts[PTS + ic], pz = pts[2 * PTS + ic];
+    uint32_t pk[PIECES][COMPS][CHUNK / 2];
+    int prev = -1;
+    float rs[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+    float fx = 0.f, fy = 0.f, fz = 0.f;
+    bool live = false;
+#pragma unroll
+    for (int t = 0; t < CHUNK; t += 2) {
+      float v[2][5];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int2 e = rao[t + h];                 // same address in every lane: broadcast
+        const int code = e.x;
+        const int sh = code < 0 ? -1 : (code >> 16);
+        const float f = __int_as_float(e.y);
+#pragma unroll
+        for (int c = 0; c < 5; ++c) v[h][c] = 0.f;
+        if (sh >= 0) {
+          if (sh != prev) {   // sh is warp-uniform
+            if (active) radial_rec(rsh[sh], rprm, px, py, pz, cutoff, rs, fx, fy, fz, live);
+            prev = sh;
+          }
+          if (active && live && rs[0] != 0.f) ao_product(code & 0xFFFF, f, rs, fx, fy, fz, v[h]);
+        }
+      }
+      bool nz = false;
+#pragma unroll
+      for (int c = 0; c < COMPS; ++c) nz = nz || v[0][c] != 0.f || v[1][c] != 0.f;
+      if (!__any_sync(0xffffffffu, nz)) {   // both AOs zero at every point of the warp
+#pragma unroll
+        for (int c = 0; c < COMPS; ++c)
+#pragma unroll
+          for (int q = 0; q < PIECES; ++q) pk[q][c][t >> 1] = 0u;
+        continue;
+      }
+#pragma unroll
+      for (int c = 0; c < COMPS; ++c) {
+        // round-to-nearest bf16 pieces of the two AOs, packed as bf16x2
+        const __nv_bfloat162 h2 = __floats2bfloat162_rn(v[0][c], v[1][c]);
+        const float2 hf = __bfloat1622float2(h2);
+        const float r0 = v[0][c] - hf.x, r1 = v[1][c] - hf.y;
+        const __nv_bfloat162 m2 = __floats2bfloat162_rn(r0, r1);
+        pk[0][c][t >> 1] = *reinterpret_cast<const uint32_t*>(&h2);
+        pk[1][c][t >> 1] = *reinterpret_cast<const uint32_t*>(&m2);
+        if (PIECES == 3) {
+          const float2 mf = __bfloat1622float2(m2);
+          const __nv_bfloat162 l2 = __floats2bfloat162_rn(r0 - mf.x, r1 - mf.y);
+          pk[PIECES - 1][c][t >> 1] = *reinterpret_cast<const uint32_t*>(&l2);
+        }
+      }
+    }
+    if (i < PTS) {
+#pragma unroll
+      for (int c = 0; c < COMPS; ++c) {
+        const int r = i * COMPS + c;
+        if (CHUNK == 4) {
+          // 16-byte chunk j/2 of the 128-byte row (swizzled), 8-byte half j&1
+          const uint32_t off = (uint32_t)(r * 128 + (((j >> 1) ^ (r & 7)) << 4) + ((j & 1) << 3));
+#pragma unroll
+          for (int q = 0; q < PIECES; ++q) st_shared_v2(a_base + q * A_TILE + off, pk[q][c][0], pk[q][c][1]);
+        } else {
+          const uint32_t off = (uint32_t)(r * 128 + ((j ^ (r & 7)) << 4));
+#pragma unroll
+          for (int q = 0; q < PIECES; ++q)
+            st_shared_v4(a_base + q * A_TILE + off, pk[q][c][0], pk[q][c][1], pk[q][c][CHUNK / 2 - 2],
+                         pk[q][c][CHUNK / 2 - 1]);
+        }
+      }
+    }
+  }
+}
+
+// The split-BF16 MMA chain of one K block (kb of kblocks) from the stage at
+// shared address `base` (A pieces, then B pieces): leading product into
+// accumulator 0 (first K half) or 1 (second half), corrections into 2.
+template <int PIECES>
+__device__ __forceinline__ void mma_kblock(uint32_t base, uint32_t a_bytes, uint32_t b_tile, uint32_t tmem,
+                                           int n_tile, uint32_t idesc, int kb, int kblocks) {
+  constexpr int NPROD = PIECES == 3 ? 6 : 3;
+  constexpr int pa3[6] = {2, 1, 0, 1, 0, 0}, pb3[6] = {0, 1, 2, 0, 1, 0};
+  constexpr int pa2[3] = {1, 0, 0}, pb2[3] = {0, 1, 0};
+  for (int kk = 0; kk < BK / UMMA_K; ++kk) {
+#pragma unroll
+    for (int t = 0; t < NPROD; ++t) {
+      const int ia = PIECES == 3 ? pa3[t] : pa2[t];
+      const int ib = PIECES == 3 ? pb3[t] : pb2[t];
+      const uint32_t a_addr = base + ia * A_TILE + kk * UMMA_K * 2;
+      const uint32_t b_addr = base + a_bytes + ib * b_tile + kk * UMMA_K * 2;
+      const bool lead = (t == NPROD - 1);
+      const bool second = lead && (2 * kb >= kblocks);
+      const uint32_t d = tmem + (uint32_t)((lead ? (second ? 1 : 0) : 2) * n_tile);
+      const bool first_use = lead ? (second ? (kb == (kblocks + 1) / 2 && kk == 0) : (kb == 0 && kk == 0))
+                                  : (kb == 0 && kk == 0 && t == 0);
+      umma_bf16(d, smem_desc(a_addr), smem_desc(b_addr), idesc, first_use ? 0u : 1u);
+    }
+  }
+}
+
+__device__ __forceinline__ uint32_t mma_idesc(int n_tile) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n_tile >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
+
+// Epilogue of one warp (TMEM lanes 32*warp .. +31): FP64 sum of the three
+// accumulators, rows (tile point i, component c) written to
+// out[(pidx[i] * COMPS + c) * n_out + col] for the MO columns [n0, n0 + n_tile).
+// stage: 32 x 16 doubles of shared scratch for this warp.
+template <int COMPS>
+__device__ __forceinline__ void epilogue_warp(uint32_t tmem, int n_tile, int n0, int n_out, bool has_second,
+                                              const int64_t* pidx, double* out, double* stage, int warp,
+                                              int lane) {
+  constexpr int PTS = BM / COMPS;
+  const int row_base = warp * 32;
+  for (int c0 = 0; c0 < n_tile; c0 += 16) {
+    uint32_t r0[16], r1[16], r2[16];
+    const uint32_t ta = tmem + ((uint32_t)row_base << 16) + (uint32_t)c0;
+    tmem_ld16(ta, r0);
+    tmem_ld16(ta + (uint32_t)n_tile, r1);
+    tmem_ld16(ta + (uint32_t)(2 * n_tile), r2);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      double v = (double)__uint_as_float(r0[j]) + (double)__uint_as_float(r2[j]);
+      if (has_second) v += (double)__uint_as_float(r1[j]);
+      stage[lane * 16 + ((j + lane) & 15)] = v;
+    }
+    __syncwarp();
+    for (int q = 0; q < 16; ++q) {
+      const int rr = 2 * q + (lane >> 4);
+      const int cc = lane & 15;
+      const int r = row_base + rr;
+      const int col = n0 + c0 + cc;
+      if (r < PTS * COMPS && col < n_out) {
+        const int64_t pq = pidx[r / COMPS];
+        if (pq >= 0) out[(pq * COMPS + r % COMPS) * n_out + col] = stage[rr * 16 + ((cc + rr) & 15)];
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// Zero the rows PTS*COMPS .. 127 of every A tile (they stay zero).
+template <int PIECES, int COMPS, int STAGES>
+__device__ __forceinline__ void zero_pad_rows(uint8_t* smem, int stage_bytes, int tid, int nthreads) {
+  constexpr int PTS = BM / COMPS;
+  constexpr int PAD = BM - PTS * COMPS;
+  if constexpr (PAD > 0) {
+    for (int t = tid; t < STAGES * PIECES * PAD * 8; t += nthreads) {
+      const int chunk = t & 7;
+      const int rr = (t >> 3) % PAD;
+      const int tile = (t >> 3) / PAD;   // stage * PIECES + piece
+      const int r = PTS * COMPS + rr;
+      uint8_t* base = smem + (tile / PIECES) * stage_bytes + (tile % PIECES) * A_TILE;
+      st_shared_v4(smem_addr(base + r * 128 + ((chunk ^ (r & 7)) << 4)), 0u, 0u, 0u, 0u);
+    }
+  }
+}
+
+}  // namespace fz
+}  // namespace qb

@@ -137,6 +137,8 @@ qmckl_exit_code dev_provide_mo_value(qmckl_context context, double* host_out);
 qmckl_exit_code dev_invalidate_mo(qmckl_context context);
 struct PreparedMixed;
 qmckl_exit_code dev_prepared_mixed(qmckl_context context, PreparedMixed* out);
+// K-block records of the fused kernels for the basis and nuclei of a context (device.cu)
+bool build_krec_records(const Context* ctx, std::vector<uint8_t>& records, int& rec_bytes);
 
 // AO finalization helpers (ao_basis.cpp)
 qmckl_exit_code finalize_basis(qmckl_context context);

@@ -7,6 +7,7 @@
 // products of order <= 2).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstddef>
 #include <cstdint>
@@ -43,6 +44,13 @@ cudaError_t tc_run(const DevTables& T, const TcPlan& plan, int64_t point_num, in
 cudaError_t tc_run_fused(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps, const double* coord,
                          double cutoff, const void* d_coef, const void* krec, int rec_bytes, const int* perm,
                          double* out, cudaStream_t s);
+// TMA map of a plan's coefficient pieces (box: 64 AOs x n_tile MOs x 1 piece,
+// 128B swizzle) and a launch of the fused kernel that does not wait for it
+// (err: device error word, left for the caller to check).
+cudaError_t tc_encode_coef_map(const TcPlan& plan, const void* d_coef, CUtensorMap* map);
+cudaError_t tc_launch_fused(const TcPlan& plan, int64_t point_num, int comps, const double* coord, double cutoff,
+                            const CUtensorMap& map, const void* krec, int rec_bytes, const int* perm, double* out,
+                            int* err, cudaStream_t s);
 // Spatial order of points (32^3 cells over [box_lo, box_hi], Morton order) by
 // a counting sort: perm[P]; keys[P] and counts[kSortCells + 1] are scratch.
 constexpr int kSortCells = 1 << 15;

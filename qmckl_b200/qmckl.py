@@ -409,3 +409,86 @@ def b200_kernel_launch_count():
 
 def b200_inject_alloc_failure(n):
     lib().qmckl_b200_inject_alloc_failure(C.c_int64(n))
+
+
+# ------------------------------------------------------ batched systems
+
+
+def _bcall(name, *args, ctx=None):
+    f = getattr(lib(), name)
+    f.restype = C.c_int32
+    _check(f(*args), ctx)
+
+
+def b200_batch_create(contexts, point_num):
+    """One batch over `contexts` with point_num[s] points for system s; returns the handle."""
+    ctxs = np.ascontiguousarray(contexts, dtype=np.int64)
+    pn = np.ascontiguousarray(point_num, dtype=np.int64)
+    if ctxs.size != pn.size:
+        raise ValueError("one point count per context")
+    h = C.c_int64(0)
+    _bcall("qmckl_b200_batch_create", ctxs.ctypes.data_as(C.c_void_p), pn.ctypes.data_as(C.c_void_p),
+           C.c_int64(ctxs.size), C.byref(h), ctx=int(ctxs[0]) if ctxs.size else None)
+    return h.value
+
+
+def b200_batch_destroy(batch):
+    _bcall("qmckl_b200_batch_destroy", C.c_int64(batch))
+
+
+def b200_batch_layout(batch, num):
+    """(coord_offset[num], out_offset[num], (coord_total, out_total)) in doubles."""
+    co = np.zeros(num, dtype=np.int64)
+    oo = np.zeros(num, dtype=np.int64)
+    tot = np.zeros(2, dtype=np.int64)
+    _bcall("qmckl_b200_batch_layout", C.c_int64(batch), co.ctypes.data_as(C.c_void_p),
+           oo.ctypes.data_as(C.c_void_p), tot.ctypes.data_as(C.c_void_p))
+    return co, oo, (int(tot[0]), int(tot[1]))
+
+
+def b200_batch_set_stream(batch, stream_ptr):
+    _bcall("qmckl_b200_batch_set_stream", C.c_int64(batch), C.c_void_p(stream_ptr))
+
+
+def b200_batch_set_graph(batch, enable):
+    _bcall("qmckl_b200_batch_set_graph", C.c_int64(batch), C.c_int32(1 if enable else 0))
+
+
+def b200_batch_mo_vgl_device(batch, d_coord_ptr, d_out_ptr):
+    _bcall("qmckl_b200_batch_mo_vgl_device", C.c_int64(batch), C.c_void_p(d_coord_ptr), C.c_void_p(d_out_ptr))
+
+
+def b200_batch_mo_vgl_loop_device(batch, d_coord_ptr, d_out_ptr):
+    _bcall("qmckl_b200_batch_mo_vgl_loop_device", C.c_int64(batch), C.c_void_p(d_coord_ptr), C.c_void_p(d_out_ptr))
+
+
+def b200_batch_synchronize(batch, raise_on_error=True):
+    """Wait for the batch; returns the launch's error word (0 = success)."""
+    st = C.c_int32(0)
+    f = lib().qmckl_b200_batch_synchronize
+    f.restype = C.c_int32
+    rc = f(C.c_int64(batch), C.byref(st))
+    if rc != 0 and raise_on_error:
+        _check(rc)
+    return st.value
+
+
+def b200_batch_tune(batch, d_coord_ptr, d_out_ptr, reps=3):
+    best = C.c_double(0.0)
+    _bcall("qmckl_b200_batch_tune", C.c_int64(batch), C.c_void_p(d_coord_ptr), C.c_void_p(d_out_ptr),
+           C.c_int32(reps), C.byref(best))
+    return best.value
+
+
+def b200_batch_set_tuning(batch, producer_warps, order):
+    _bcall("qmckl_b200_batch_set_tuning", C.c_int64(batch), C.c_int32(producer_warps), C.c_int32(order))
+
+
+def b200_batch_get_tuning(batch):
+    pw, od = C.c_int32(0), C.c_int32(0)
+    _bcall("qmckl_b200_batch_get_tuning", C.c_int64(batch), C.byref(pw), C.byref(od))
+    return pw.value, od.value
+
+
+def b200_batch_set_wait_limit(batch, polls, publish=True):
+    _bcall("qmckl_b200_batch_set_wait_limit", C.c_int64(batch), C.c_int64(polls), C.c_int32(1 if publish else 0))
