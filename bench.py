@@ -174,6 +174,159 @@ def profile_case(kind, walkers=64):
     print(f"profile case {kind}: {P} points")
 
 
+def _events_time(stream, fn, steps, flush=None, after=None):
+    """Median device time (ms) of fn() over `steps` calls, CUDA events on `stream`."""
+    import torch
+    ts = []
+    for _ in range(steps):
+        if flush is not None:
+            flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        if after is not None:
+            after()
+        ts.append(e0.elapsed_time(e1))
+    return statistics.median(ts), ts
+
+
+def case_batched(args):
+    """Config 2: 256 independent molecules, one persistent launch (CUDA graph) vs a per-system launch loop."""
+    import torch
+    from qmckl_b200 import gen
+    from qmckl_b200 import qmckl as pq
+    from qmckl_b200.system import make_context
+    t0 = time.time()
+    systems = gen.batch_config()
+    ctxs = [make_context(s, points=False, form=pq.FORM_MIXED) for s in systems]
+    P = [gen.points(s).shape[0] for s in systems]
+    b = pq.b200_batch_create(ctxs, P)
+    setup_s = time.time() - t0
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    pq.b200_batch_set_stream(b, stream.cuda_stream)
+    co, oo, (ct, ot) = pq.b200_batch_layout(b, len(ctxs))
+    coord = np.zeros(ct)
+    for s, sysd in enumerate(systems):
+        coord[co[s]:co[s] + 3 * P[s]] = gen.points(sysd).T.reshape(-1)
+    d_coord = torch.tensor(coord, dtype=torch.float64, device="cuda")
+    d_out = torch.empty(ot, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    best = pq.b200_batch_tune(b, d_coord.data_ptr(), d_out.data_ptr(), 2)
+    tuning = pq.b200_batch_get_tuning(b)
+    pq.b200_batch_set_graph(b, True)
+
+    def persistent():
+        pq.b200_batch_mo_vgl_device(b, d_coord.data_ptr(), d_out.data_ptr())
+
+    def check():
+        assert pq.b200_batch_synchronize(b) == 0
+
+    def loop():
+        pq.b200_batch_mo_vgl_loop_device(b, d_coord.data_ptr(), d_out.data_ptr())
+
+    for _ in range(max(3, args.warmup)):
+        persistent()
+        check()
+    n = max(3, min(args.steps, 10))
+    t_p, _ = _events_time(stream, persistent, n, flush, check)
+    for _ in range(2):
+        loop()
+    t_l, _ = _events_time(stream, loop, n, flush)
+    flops = sum(10.0 * p * s["ao_num"] * s["mo_num"] for p, s in zip(P, systems))
+    line = {"case": "batched systems: 256 molecules, 5-80 nuclei, cc-pVDZ/TZ shapes, 16-256 walkers",
+            "systems": len(systems), "points": int(sum(P)), "form": "mixed",
+            "persistent_ms": t_p, "loop_ms": t_l, "loop_over_persistent": t_l / t_p,
+            "points_per_s": sum(P) / (t_p * 1e-3), "dense_equivalent_tflops": flops / (t_p * 1e-3) / 1e12,
+            "tuning": {"producer_warps": tuning[0], "queue_order": tuning[1], "tuned_ms": best},
+            "graph": True, "setup_s": setup_s, "steps": n,
+            "timing": "CUDA events on the batch stream, median, 256 MB L2 flush before each step"}
+    print(json.dumps(line))
+    pq.b200_batch_destroy(b)
+    for c in ctxs:
+        pq.context_destroy(c)
+
+
+def case_adjoint(args):
+    """Config 3: forward MO VGL + adjoint (coefficient, nuclear, point gradients), config-1 molecule, 128 walkers."""
+    import torch
+    from qmckl_b200 import gen
+    from qmckl_b200 import qmckl as pq
+    from qmckl_b200.system import make_context
+    d = gen.config(3)
+    pts = gen.points(d)
+    P, A, M, N = pts.shape[0], d["ao_num"], d["mo_num"], d["nucl_num"]
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    dc = torch.tensor(np.ascontiguousarray(pts.T), dtype=torch.float64, device="cuda")
+    w = torch.randn((P, 5, M), dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(3))
+    out = torch.empty((P, 5, M), dtype=torch.float64, device="cuda")
+    gc = torch.empty((M, A), dtype=torch.float64, device="cuda")
+    gn = torch.empty((N, 3), dtype=torch.float64, device="cuda")
+    gr = torch.empty((3, P), dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    res = {}
+    for name, form in (("fp64", pq.FORM_FP64), ("mixed", pq.FORM_MIXED)):
+        ctx = make_context(d, points=False, form=form)
+        pq.b200_set_stream(ctx, stream.cuda_stream)
+        fwd = lambda: pq.b200_mo_vgl_device(ctx, P, dc.data_ptr(), out.data_ptr())
+        bwd = lambda: pq.b200_mo_vgl_adjoint_device(ctx, P, dc.data_ptr(), w.data_ptr(), gc.data_ptr(),
+                                                    gn.data_ptr(), gr.data_ptr())
+        for _ in range(3):
+            fwd()
+            bwd()
+        torch.cuda.synchronize()
+        tf, _ = _events_time(stream, fwd, max(3, min(args.steps, 20)), flush)
+        tb, _ = _events_time(stream, bwd, max(3, min(args.steps, 20)), flush)
+        res[name] = {"forward_ms": tf, "backward_ms": tb, "points_per_s_fwd_bwd": P / ((tf + tb) * 1e-3)}
+        pq.context_destroy(ctx)
+    print(json.dumps({"case": "adjoint: config-1 molecule, 128 walkers, L = sum W * mo_vgl", "points": P,
+                      "ao_num": A, "mo_num": M, "results": res,
+                      "timing": "CUDA events, median, 256 MB L2 flush before each call"}))
+
+
+def case_large(args):
+    """Config 4: 200 nuclei, 5000 AOs, 350 MOs, 700 electrons x 256 walkers: fused mixed vs unfused FP64."""
+    import torch
+    from qmckl_b200 import gen
+    from qmckl_b200 import qmckl as pq
+    from qmckl_b200.system import make_context
+    d = gen.config(4)
+    pts = gen.points(d)
+    P, A, M = pts.shape[0], d["ao_num"], d["mo_num"]
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    dc = torch.tensor(np.ascontiguousarray(pts.T), dtype=torch.float64, device="cuda")
+    out = torch.empty((P, 5, M), dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    res = {}
+    ref = None
+    for name, form in (("fp64_unfused", pq.FORM_FP64), ("mixed_fused", pq.FORM_MIXED)):
+        ctx = make_context(d, points=False, form=form)
+        pq.b200_set_stream(ctx, stream.cuda_stream)
+        fn = lambda: pq.b200_mo_vgl_device(ctx, P, dc.data_ptr(), out.data_ptr())
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        t, _ = _events_time(stream, fn, max(3, min(args.steps, 10)), flush)
+        res[name] = {"ms": t, "points_per_s": P / (t * 1e-3)}
+        if ref is None:
+            ref = out.clone()
+        else:
+            diff = (out - ref).abs()
+            res[name]["max_abs_over_max_ref"] = {
+                n: float(diff[:, c, :].max() / ref[:, c, :].abs().max())
+                for c, n in enumerate(["value", "grad_x", "grad_y", "grad_z", "laplacian"])}
+        pq.context_destroy(ctx)
+    res["speedup"] = res["fp64_unfused"]["ms"] / res["mixed_fused"]["ms"]
+    print(json.dumps({"case": "large: 200 nuclei, 5000 AOs, 350 MOs, 700 electrons x 256 walkers", "points": P,
+                      "ao_num": A, "mo_num": M, "results": res,
+                      "timing": "CUDA events, median, 256 MB L2 flush before each call"}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -184,7 +337,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", choices=["fused", "split", "fp64"],
                     help="run one evaluation of a small case (config-1 molecule, 64 walkers) for ncu; no timing")
+    ap.add_argument("--case", choices=["batched", "adjoint", "large"],
+                    help="measure another workload instead of the headline one (one JSON line)")
     args = ap.parse_args()
+    if args.case:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        return {"batched": case_batched, "adjoint": case_adjoint, "large": case_large}[args.case](args)
     if args.impl == "reference":
         return run_reference(args)
     if args.profile:
