@@ -335,6 +335,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default=os.environ.get("QMCKL_B200_BENCH_FORM", "mixed"), choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--pieces", type=int, default=3, choices=[2, 3],
+                    help="operand split of the mixed form: 3 bfloat16 pieces (default) or 2 float16 pieces")
     ap.add_argument("--profile", choices=["fused", "split", "fp64"],
                     help="run one evaluation of a small case (config-1 molecule, 64 walkers) for ncu; no timing")
     ap.add_argument("--case", choices=["batched", "adjoint", "large"],
@@ -369,6 +371,8 @@ def main():
     P, A, M = W * E, sysd["ao_num"], sysd["mo_num"]
     form = pq.FORM_MIXED if args.form == "mixed" else pq.FORM_FP64
     ctx = make_context(sysd, points=False, form=form)
+    if form == pq.FORM_MIXED:
+        pq.b200_set_split_terms(ctx, args.pieces)
     stream = torch.cuda.Stream()          # evaluation stream shared by torch and the library
     torch.cuda.set_stream(stream)
     pq.b200_set_stream(ctx, stream.cuda_stream)
@@ -494,10 +498,13 @@ def main():
         tiles = -(-P // 25)
         n_pad = -(-M // 16) * 16 if M <= 160 else M
         k_pad = -(-A // 64) * 64
-        executed = 2.0 * tiles * 128 * n_pad * k_pad * 6
+        nprod = 6 if args.pieces == 3 else 3
+        executed = 2.0 * tiles * 128 * n_pad * k_pad * nprod
         achieved = executed / (ms * 1e-3) / 1e12
         t = traffic.get(("fused_mo_kernel", "mixed"))
-        roofline = {"kernel": "fused_mo_kernel<3,5> (AO -> split-BF16 tcgen05 MO VGL; step = 3 ordering kernels + this)",
+        kname = ("fused_mo_kernel<3,5> (AO -> split-BF16 tcgen05 MO VGL" if args.pieces == 3 else
+                 "fused_mo_kernel<2,5> (AO -> split-FP16 tcgen05 MO VGL")
+        roofline = {"kernel": kname + "; step = 3 ordering kernels + this)",
                     "bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
                     "frac": achieved / bf16, "peak_source": peak_src,
                     "traffic": t * P / 20352.0 if t else None,
@@ -510,7 +517,7 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "electron-points/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if form == pq.FORM_FP64 else "f32/bf16x3",
+        "vs_baseline": None, "dtype": "f64" if form == pq.FORM_FP64 else ("f32/bf16x3" if args.pieces == 3 else "f32/f16x2"),
         "data": "synthetic (seeded generator qmckl_b200/gen.py, no dataset)",
         "config": {"workload": WORKLOAD, "points": P, "ao_num": A, "mo_num": M,
                    "form": args.form, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",

@@ -15,6 +15,7 @@
 #include <cuda_bf16.h>
 
 #include "ao_tile.cuh"
+#include "split.cuh"
 
 namespace qb {
 namespace {
@@ -112,7 +113,7 @@ template <int MODE, int COMPS>
 __global__ void __launch_bounds__(kThreads)
 ao_tile_kernel(const DevTables T, const AoTiles Tl, const int64_t P, const double* __restrict__ coord,
                const double cutoff, const bool dp_exp, void* __restrict__ out, const int64_t ld,
-               const int64_t piece_stride) {
+               const int64_t piece_stride, const double* __restrict__ scales) {
   using R = typename RadT<typename std::conditional<MODE == 0, double, float>::type>::T;
   __shared__ double s_pts[3][TP];
   __shared__ double s_nuc[kTileNuc][4];          // x, y, z, cutoff * range
@@ -254,25 +255,17 @@ ao_tile_kernel(const DevTables T, const AoTiles Tl, const int64_t P, const doubl
     {
       constexpr int PIECES = MODE == 0 ? 2 : MODE;
       uint16_t* a = (uint16_t*)out;
+      float inv[5];
+      load_inv_scales<COMPS>(scales, inv);
 #pragma unroll
       for (int c = 0; c < COMPS; ++c) {
         uint32_t pk[PIECES][4];
 #pragma unroll
-        for (int t = 0; t < 8; ++t) {
-          const float v = (float)vals[t][c];
-          const __nv_bfloat16 h = __float2bfloat16_rn(v);
-          float r = v - __bfloat162float(h);
-          const __nv_bfloat16 m = __float2bfloat16_rn(r);
-          uint32_t bits[3] = {(uint32_t)__bfloat16_as_ushort(h), (uint32_t)__bfloat16_as_ushort(m), 0u};
-          if (PIECES == 3) {
-            r = r - __bfloat162float(m);
-            bits[2] = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(r));
-          }
+        for (int t = 0; t < 8; t += 2) {
+          uint32_t q3[3];
+          split_pair<PIECES>((float)vals[t][c], (float)vals[t + 1][c], inv[c], q3);
 #pragma unroll
-          for (int q = 0; q < PIECES; ++q) {
-            if (t & 1) pk[q][t >> 1] |= bits[q] << 16;
-            else pk[q][t >> 1] = bits[q];
-          }
+          for (int q = 0; q < PIECES; ++q) pk[q][t >> 1] = q3[q];
         }
         const int64_t off = (p * COMPS + c) * ld + k0;   // k0 multiple of 8, ld multiple of 64
 #pragma unroll
@@ -286,12 +279,12 @@ ao_tile_kernel(const DevTables T, const AoTiles Tl, const int64_t P, const doubl
 
 template <int MODE, int COMPS>
 cudaError_t launch(const DevTables& T, const AoTiles& Tl, int64_t P, const double* coord, double cutoff, bool dp_exp,
-                   void* out, int64_t ld, int64_t piece_stride, cudaStream_t s) {
+                   void* out, int64_t ld, int64_t piece_stride, const double* scales, cudaStream_t s) {
   if (P <= 0) return cudaSuccess;
   const int64_t ptiles = (P + TP - 1) / TP;
   if (ptiles > 0x7fffffff || Tl.ntiles > 65535) return cudaErrorInvalidValue;
   dim3 grid((unsigned)ptiles, (unsigned)Tl.ntiles);
-  ao_tile_kernel<MODE, COMPS><<<grid, kThreads, 0, s>>>(T, Tl, P, coord, cutoff, dp_exp, out, ld, piece_stride);
+  ao_tile_kernel<MODE, COMPS><<<grid, kThreads, 0, s>>>(T, Tl, P, coord, cutoff, dp_exp, out, ld, piece_stride, scales);
   count_launch();
   return cudaGetLastError();
 }
@@ -301,17 +294,16 @@ cudaError_t launch(const DevTables& T, const AoTiles& Tl, int64_t P, const doubl
 cudaError_t launch_ao_tile_f64(const DevTables& T, const AoTiles& Tl, int64_t P, const double* coord, double cutoff,
                                bool dp_exp, int comps, double* out, cudaStream_t s) {
   const int64_t ld = T.ao_num;
-  return comps == 5 ? launch<0, 5>(T, Tl, P, coord, cutoff, dp_exp, out, ld, 0, s)
-                    : launch<0, 1>(T, Tl, P, coord, cutoff, dp_exp, out, ld, 0, s);
+  return comps == 5 ? launch<0, 5>(T, Tl, P, coord, cutoff, dp_exp, out, ld, 0, nullptr, s)
+                    : launch<0, 1>(T, Tl, P, coord, cutoff, dp_exp, out, ld, 0, nullptr, s);
 }
 
 cudaError_t launch_ao_tile_split(const DevTables& T, const AoTiles& Tl, int64_t P, const double* coord, double cutoff,
-                                 int comps, int pieces, void* a, int64_t lda, int64_t piece_stride, cudaStream_t s) {
-  if (pieces == 3)
-    return comps == 5 ? launch<3, 5>(T, Tl, P, coord, cutoff, false, a, lda, piece_stride, s)
-                      : launch<3, 1>(T, Tl, P, coord, cutoff, false, a, lda, piece_stride, s);
-  return comps == 5 ? launch<2, 5>(T, Tl, P, coord, cutoff, false, a, lda, piece_stride, s)
-                    : launch<2, 1>(T, Tl, P, coord, cutoff, false, a, lda, piece_stride, s);
+                                 int comps, int pieces, const double* scales, void* a, int64_t lda,
+                                 int64_t piece_stride, cudaStream_t s) {
+  if (pieces != 3) return cudaErrorInvalidValue;   // 3 bfloat16 pieces (unfused organisation)
+  return comps == 5 ? launch<3, 5>(T, Tl, P, coord, cutoff, false, a, lda, piece_stride, scales, s)
+                    : launch<3, 1>(T, Tl, P, coord, cutoff, false, a, lda, piece_stride, scales, s);
 }
 
 }  // namespace qb

@@ -25,7 +25,10 @@ struct AoTiles {
 
 cudaError_t launch_ao_tile_f64(const DevTables& T, const AoTiles& Tl, int64_t P, const double* coord, double cutoff,
                                bool dp_exp, int comps, double* out, cudaStream_t s);
+// AO pieces (split.cuh) of rows (point, component); scales: the scale block
+// of the coefficient pieces (its AO-component scales are used).
 cudaError_t launch_ao_tile_split(const DevTables& T, const AoTiles& Tl, int64_t P, const double* coord, double cutoff,
-                                 int comps, int pieces, void* a, int64_t lda, int64_t piece_stride, cudaStream_t s);
+                                 int comps, int pieces, const double* scales, void* a, int64_t lda,
+                                 int64_t piece_stride, cudaStream_t s);
 
 }  // namespace qb

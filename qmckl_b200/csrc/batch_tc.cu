@@ -47,7 +47,7 @@ namespace {
 using namespace fz;
 
 constexpr int kStages = 2;
-constexpr int kPieces = 3;
+constexpr int kPieces = 3;   // bfloat16 x 3 operands (split.cuh), as the single-system default
 constexpr int kCellsAxis = 16;
 constexpr int kCells = kCellsAxis * kCellsAxis * kCellsAxis;
 constexpr int kPts = BM / 5;   // 25 points per tile (MO VGL)
@@ -58,6 +58,8 @@ struct alignas(64) BatchDesc {
   int64_t perm_off;    // offset of its point order in the permutation buffer
   int64_t P;
   const uint8_t* krec;
+  const double* scales;   // scale block of the system's coefficient pieces
+  RowBound rb;            // row bounds of the float16 operands
   double cutoff;
   double lo[3];
   double inv_cell;
@@ -72,6 +74,7 @@ struct BatchCtl {                 // shared-memory control block of a CTA
   int ok;
   double pts[3 * kPts];
   int64_t pidx[kPts];
+  int rexp[3 * kPts];
 };
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
@@ -239,8 +242,13 @@ batch_mo_kernel(const BatchDesc* __restrict__ desc, const CUtensorMap* __restric
       const int64_t q = (p0 + i < P) ? (int64_t)__ldcg(pm + p0 + i) : -1;
       C.pts[t] = q >= 0 ? crd[q + d * P] : 0.0;
       if (d == 0) C.pidx[i] = q;
+      C.rexp[t] = PIECES == 2 ? kExpMin : 0;
     }
     __syncthreads();
+    if (PIECES == 2) {
+      row_exponents<kPts>(D.rb, C.pts, C.pidx, C.rexp, tid, NTHREADS);
+      __syncthreads();
+    }
     const int kblocks = D.kblocks, n_tile = D.n_tile, rec_bytes = D.rec_bytes;
     const int n0 = ntile * n_tile;
     const int B_TILE = n_tile * BK * 2;
@@ -252,8 +260,8 @@ batch_mo_kernel(const BatchDesc* __restrict__ desc, const CUtensorMap* __restric
         bool ok = mbar_wait(&C.empty[s], phase ^ 1u, err, 21);
         ok = ok && mbar_wait(&C.rec_full[s], phase, err, 25);
         if (!__all_sync(0xffffffffu, ok)) break;
-        produce_kblock<PIECES, COMPS, CHUNK>(recs + s * rec_max, C.pts, p0, P, D.cutoff, smem_addr(smem + s * STAGE),
-                                             warp, lane);
+        produce_kblock<PIECES, COMPS, CHUNK>(recs + s * rec_max, C.pts, p0, P, D.cutoff, C.rexp,
+                                             smem_addr(smem + s * STAGE), warp, lane);
         fence_async_smem();
         mbar_arrive(&C.full[s]);
       }
@@ -274,7 +282,7 @@ batch_mo_kernel(const BatchDesc* __restrict__ desc, const CUtensorMap* __restric
       }
     } else {
       if (lane == 0) {
-        const uint32_t idesc = mma_idesc(n_tile);
+        const uint32_t idesc = mma_idesc<PIECES>(n_tile);
         for (int kb = 0; kb < kblocks; ++kb) {
           const uint32_t g = kbase + (uint32_t)kb;
           const int s = (int)(g & 1u);
@@ -288,15 +296,17 @@ batch_mo_kernel(const BatchDesc* __restrict__ desc, const CUtensorMap* __restric
         umma_commit(&C.acc_full);
       }
     }
-    if (warp < 4) {
-      // epilogue (its staging scratch overlaps the zero rows of the first A
-      // tile; those rows only feed accumulator rows that are never stored)
+    if (warp < PRODW) {
+      // epilogue: every producer warp, TMEM lane quadrant warp % 4 (its
+      // staging scratch overlaps the zero rows of the first A tile; those
+      // rows only feed accumulator rows that are never stored)
       bool ok = mbar_wait(&C.acc_full, ntiles & 1u, err, 24);
       ok = __all_sync(0xffffffffu, ok && *(volatile int*)err == 0);
       tc_fence_after();
       if (ok)
-        epilogue_warp<COMPS>(tmem, n_tile, n0, D.n_out, kblocks >= 2, C.pidx, out + D.out_off,
-                             (double*)smem + warp * 32 * 16, warp, lane);
+        epilogue_warp<PIECES, COMPS>(tmem, n_tile, n0, D.n_out, kblocks >= 2, C.pidx, C.rexp, D.scales,
+                                     out + D.out_off, (double*)smem + warp * 32 * 16, warp, lane, warp >> 2,
+                                     PRODW / 4);
     }
     kbase += (uint32_t)kblocks;
     ++ntiles;
@@ -329,6 +339,7 @@ struct BatchSys {
   double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
   int64_t coord_off = 0, out_off = 0, perm_off = 0;
   CUtensorMap map;
+  RowBound rb{};
 };
 
 struct DBuf {
@@ -355,7 +366,7 @@ struct Batch {
   std::vector<BatchSys> sys;
   int64_t coord_total = 0, out_total = 0, perm_total = 0;
   int n_tile_max = 0, rec_max = 0;
-  DBuf coef, krec, desc, tmaps, items, ctl, perm, keys, counts, loop_err;
+  DBuf coef, krec, desc, tmaps, items, ctl, perm, keys, counts, loop_err, nucl, env;
   int n_items = 0;
   // tuning
   int prod_warps = 16;
@@ -562,8 +573,11 @@ qmckl_exit_code qmckl_b200_batch_create(const qmckl_context* contexts, const int
     return fail(c0, fname, msg);
   };
   B->sys.resize((size_t)num);
-  size_t coef_total = 0, krec_total = 0;
+  size_t coef_total = 0, krec_total = 0, nucl_total = 0, env_total = 0;
   std::vector<std::vector<uint8_t>> recs((size_t)num);
+  std::vector<std::vector<float>> envs((size_t)num);
+  std::vector<float> env_r0((size_t)num), env_il((size_t)num);
+  std::vector<size_t> nucl_off((size_t)num), env_off((size_t)num);
   uint64_t sig = 1469598103934665603ull;
   sig = fnv(sig, num);
   for (int64_t s = 0; s < num; ++s) {
@@ -575,6 +589,11 @@ qmckl_exit_code qmckl_b200_batch_create(const qmckl_context* contexts, const int
     S.plan = tc_plan(S.A, S.M, kPieces);
     S.cutoff = std::log((double)(((uint64_t)1) << (ctx->precision - 1)));
     if (!build_krec_records(ctx, recs[s], S.rec_bytes)) return bail("AOs are not numbered shell by shell");
+    build_envelopes(ctx, envs[s], env_r0[s], env_il[s]);
+    nucl_off[s] = nucl_total;
+    nucl_total += 3 * (size_t)ctx->nucleus.num;
+    env_off[s] = env_total;
+    env_total += envs[s].size();
     const int64_t N = ctx->nucleus.num;
     for (int d = 0; d < 3; ++d) {
       S.lo[d] = 1e300;
@@ -605,6 +624,8 @@ qmckl_exit_code qmckl_b200_batch_create(const qmckl_context* contexts, const int
       dalloc(B->tmaps, sizeof(CUtensorMap) * num) != cudaSuccess ||
       dalloc(B->ctl, sizeof(int) * (2 + num)) != cudaSuccess ||
       dalloc(B->perm, sizeof(int) * std::max<int64_t>(B->perm_total, 1)) != cudaSuccess ||
+      dalloc(B->nucl, sizeof(double) * std::max<size_t>(nucl_total, 1)) != cudaSuccess ||
+      dalloc(B->env, sizeof(float) * std::max<size_t>(env_total, 1)) != cudaSuccess ||
       cudaMallocHost(&B->h_err, sizeof(int)) != cudaSuccess) {
     cudaGetLastError();
     return bail("device allocation failed");
@@ -619,6 +640,13 @@ qmckl_exit_code qmckl_b200_batch_create(const qmckl_context* contexts, const int
     void* dcoef = (char*)B->coef.p + S.coef_off;
     if (tc_prepare_coef(S.plan, ctx->mo_basis.coefficient.data(), dcoef, B->stream) != cudaSuccess)
       return bail("coefficient upload failed");
+    double* dn = (double*)B->nucl.p + nucl_off[s];
+    float* de = (float*)B->env.p + env_off[s];
+    if (cudaMemcpyAsync(dn, ctx->nucleus.coord.data(), sizeof(double) * 3 * ctx->nucleus.num, cudaMemcpyHostToDevice,
+                        B->stream) != cudaSuccess ||
+        (!envs[s].empty() && cudaMemcpyAsync(de, envs[s].data(), sizeof(float) * envs[s].size(),
+                                             cudaMemcpyHostToDevice, B->stream) != cudaSuccess))
+      return bail("nuclear data upload failed");
     if (tc_encode_coef_map(S.plan, dcoef, &S.map) != cudaSuccess) return bail("tensor map encoding failed");
     hm[s] = S.map;
     if (!recs[s].empty() &&
@@ -632,6 +660,9 @@ qmckl_exit_code qmckl_b200_batch_create(const qmckl_context* contexts, const int
     D.perm_off = S.perm_off;
     D.P = S.P;
     D.krec = (const uint8_t*)B->krec.p + S.krec_off;
+    D.scales = tc_scales(S.plan, dcoef);
+    D.rb = RowBound{dn, de, (int)ctx->nucleus.num, env_r0[s], env_il[s]};
+    S.rb = D.rb;
     D.cutoff = S.cutoff;
     double ext = 0.0;
     for (int d = 0; d < 3; ++d) {
@@ -663,7 +694,7 @@ qmckl_exit_code qmckl_b200_batch_destroy(qmckl_b200_batch batch) {
   if (B->stream) cudaStreamSynchronize(B->stream);
   drop_graph(B);
   for (DBuf* b : {&B->coef, &B->krec, &B->desc, &B->tmaps, &B->items, &B->ctl, &B->perm, &B->keys, &B->counts,
-                  &B->loop_err})
+                  &B->loop_err, &B->nucl, &B->env})
     if (b->p) cudaFree(b->p);
   if (B->h_err) cudaFreeHost(B->h_err);
   if (B->own_stream && B->stream) cudaStreamDestroy(B->stream);
@@ -781,7 +812,8 @@ qmckl_exit_code qmckl_b200_batch_mo_vgl_loop_device(qmckl_b200_batch batch, cons
     e = point_order(c, S.P, S.lo, S.hi, (int*)B->keys.p, (unsigned*)B->counts.p, pm, B->stream);
     if (e == cudaSuccess)
       e = tc_launch_fused(S.plan, S.P, 5, c, S.cutoff, S.map, (const char*)B->krec.p + S.krec_off, S.rec_bytes, pm,
-                          d_mo_vgl + S.out_off, (int*)B->loop_err.p, B->stream);
+                          (const char*)B->coef.p + S.coef_off, S.rb, d_mo_vgl + S.out_off, (int*)B->loop_err.p,
+                          B->stream);
   }
   if (e == cudaSuccess) e = cudaMemcpyAsync(B->h_err, B->loop_err.p, sizeof(int), cudaMemcpyDeviceToHost, B->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(B->stream);

@@ -106,6 +106,53 @@ bool build_krec_records(const Context* ctx, std::vector<uint8_t>& h, int& rec_by
   return true;
 }
 
+// Row-bound envelopes of the 2-piece float16 operands (fused_common.cuh
+// RowBound) for the basis of a context: env[nucl][3][kEnvCells], and the
+// radial cells (r0, 1 / log2 of the cell ratio) shared by all nuclei.
+void build_envelopes(const Context* ctx, std::vector<float>& env, float& r0, float& inv_log2q) {
+  using fz::kEnvCells;
+  const AoBasisRec& B = ctx->ao_basis;
+  const AoDerived& d = B.d;
+  const int64_t N = ctx->nucleus.num, A = B.ao_num;
+  const double cutoff = std::log((double)(((uint64_t)1) << (ctx->precision - 1)));
+  double r_far = 1e-2;
+  std::vector<double> r_max((size_t)N);
+  for (int64_t n = 0; n < N; ++n) {
+    r_max[n] = std::sqrt(std::max(0.0, cutoff * d.nucleus_range[n]));
+    r_far = std::max(r_far, r_max[n]);
+  }
+  r0 = 1.0e-3f;
+  inv_log2q = (float)((kEnvCells - 2) / std::log2(r_far / r0));
+  env.assign((size_t)N * 3 * kEnvCells, 0.f);
+  std::vector<double> ex, cf;
+  std::vector<ShellBound> sb;
+  for (int64_t n = 0; n < N; ++n) {
+    ex.clear();
+    cf.clear();
+    sb.clear();
+    std::vector<std::pair<size_t, size_t>> span;
+    for (int64_t s = B.nucleus_index[n]; s < B.nucleus_index[n] + B.nucleus_shell_num[n]; ++s) {
+      const size_t b0 = ex.size();
+      for (int j = d.shell_coef_start[s]; j < d.shell_coef_start[s + 1]; ++j) {
+        ex.push_back(d.expo_sorted[d.nuc_prim_start[n] + d.coef_prim[j]]);
+        cf.push_back(d.coef_val[j]);
+      }
+      span.push_back({b0, ex.size()});
+      const int l = B.shell_ang_mom[s];
+      double f = 0.0;
+      for (int64_t k = d.ao_index[s]; k < d.ao_index[s] + (l + 1) * (l + 2) / 2 && k < A; ++k)
+        f = std::max(f, std::fabs(B.ao_factor[k]));
+      sb.push_back(ShellBound{l, f, nullptr, nullptr, 0});
+    }
+    for (size_t q = 0; q < sb.size(); ++q) {
+      sb[q].expo = ex.data() + span[q].first;
+      sb[q].coef = cf.data() + span[q].first;
+      sb[q].nprim = (int)(span[q].second - span[q].first);
+    }
+    tc_envelope(sb.data(), (int)sb.size(), r_max[n], r0, inv_log2q, env.data() + (size_t)n * 3 * kEnvCells);
+  }
+}
+
 static std::atomic<int64_t> g_launches{0};
 void count_launch(int n) { g_launches += n; }
 
@@ -137,11 +184,18 @@ struct DeviceState {
   uint64_t coef_version = ~0ull;
   DevBuf coef_t;
   // mixed form: split-bf16 coefficient pieces and the A-matrix scratch
-  TcPlan tc;
+  TcPlan tc;                       // fused kernel (split_pieces)
   uint64_t tc_coef_version = ~0ull;
   int tc_pieces = 0;
   DevBuf tc_coef, tc_a;
-  int32_t split_pieces = 3;
+  TcPlan tc3;                      // unfused kernels and the fixed-scratch entry: 3 bfloat16 pieces
+  uint64_t tc3_coef_version = ~0ull;
+  DevBuf tc3_coef;
+  // row-bound envelopes of the float16 operands (per basis)
+  DevBuf env;
+  uint64_t env_basis_version = ~0ull;
+  float env_r0 = 0.f, env_inv_log2q = 0.f;
+  int32_t split_pieces = 3;   // bfloat16 x 3; 2 = float16 x 2 with row / MO scales (split.cuh)
   // mixed form: fused AO -> MO kernel (default) instead of AO pieces in device memory + GEMM
   bool fused = true;
   // per-K-block records of the fused kernel (rebuilt on basis or nuclear moves)
@@ -463,12 +517,12 @@ bool build_krec(qmckl_context context, DeviceState* ds) {
   return true;
 }
 
-qmckl_exit_code run_mo_mixed(qmckl_context context, DeviceState* ds, int64_t P, const double* coord,
-                             double* out, int comps) {
+// Coefficient pieces of the fused plan (split_pieces) and of the unfused
+// plan (3 bfloat16 pieces), and the row-bound envelopes, on the device.
+qmckl_exit_code prepare_mixed(qmckl_context context, DeviceState* ds) {
   Context* ctx = ctx_of(context);
   const int64_t A = ctx->ao_basis.ao_num, M = ctx->mo_basis.mo_num;
   const int pieces = ds->split_pieces;
-  // coefficient pieces
   if (ds->tc_coef_version != ctx->mo_basis.coef_version || ds->tc_pieces != pieces || !ds->tc_coef.p) {
     TcPlan plan = tc_plan(A, M, pieces);
     qmckl_exit_code rc = ensure(context, ds->tc_coef, plan.coef_bytes, "qmckl_b200_mo_mixed");
@@ -478,6 +532,34 @@ qmckl_exit_code run_mo_mixed(qmckl_context context, DeviceState* ds, int64_t P, 
     ds->tc_coef_version = ctx->mo_basis.coef_version;
     ds->tc_pieces = pieces;
   }
+  if (ds->tc3_coef_version != ctx->mo_basis.coef_version || !ds->tc3_coef.p) {
+    TcPlan plan = tc_plan(A, M, 3);
+    qmckl_exit_code rc = ensure(context, ds->tc3_coef, plan.coef_bytes, "qmckl_b200_mo_mixed");
+    if (rc != QMCKL_SUCCESS) return rc;
+    QB_CUDA(tc_prepare_coef(plan, ctx->mo_basis.coefficient.data(), ds->tc3_coef.p, ds->stream), "qmckl_b200_mo_mixed");
+    ds->tc3 = plan;
+    ds->tc3_coef_version = ctx->mo_basis.coef_version;
+  }
+  if (ds->env_basis_version != ctx->ao_basis.basis_version || !ds->env.p) {
+    std::vector<float> env;
+    float r0 = 0.f, il = 0.f;
+    build_envelopes(ctx, env, r0, il);
+    qmckl_exit_code rc = ensure(context, ds->env, sizeof(float) * std::max<size_t>(env.size(), 1), "qmckl_b200_mo_mixed");
+    if (rc != QMCKL_SUCCESS) return rc;
+    if (!env.empty())
+      QB_CUDA(cudaMemcpy(ds->env.p, env.data(), sizeof(float) * env.size(), cudaMemcpyHostToDevice), "qmckl_b200_mo_mixed");
+    ds->env_r0 = r0;
+    ds->env_inv_log2q = il;
+    ds->env_basis_version = ctx->ao_basis.basis_version;
+  }
+  return QMCKL_SUCCESS;
+}
+
+qmckl_exit_code run_mo_mixed(qmckl_context context, DeviceState* ds, int64_t P, const double* coord,
+                             double* out, int comps) {
+  Context* ctx = ctx_of(context);
+  qmckl_exit_code rc0 = prepare_mixed(context, ds);
+  if (rc0 != QMCKL_SUCCESS) return rc0;
   if (ds->fused) {
     bool ok = ds->krec.p != nullptr && ds->krec_basis_version == ctx->ao_basis.basis_version &&
               ds->krec_nucl_version == ctx->nucleus.coord_version;
@@ -499,17 +581,18 @@ qmckl_exit_code run_mo_mixed(qmckl_context context, DeviceState* ds, int64_t P, 
           hi[d] = std::max(hi[d], ctx->nucleus.coord[n + d * N] + 4.0);
         }
       QB_CUDA(point_order(coord, P, lo, hi, keys, counts, perm, ds->stream), "qmckl_b200_mo_mixed");
+      fz::RowBound rb{(const double*)ds->nucl.p, (const float*)ds->env.p, (int)N, ds->env_r0, ds->env_inv_log2q};
       QB_CUDA(tc_run_fused(ds->T, ds->tc, P, comps, coord, cutoff_of(ctx), ds->tc_coef.p, ds->krec.p, ds->rec_bytes,
-                           perm, out, ds->stream),
+                           perm, rb, out, ds->stream),
               "qmckl_b200_mo_mixed");
       return QMCKL_SUCCESS;
     }
   }
   const int64_t rows = (int64_t)comps * P;
-  const size_t abytes = tc_a_bytes(ds->tc, rows);
+  const size_t abytes = tc_a_bytes(ds->tc3, rows);
   qmckl_exit_code rc = ensure(context, ds->tc_a, abytes, "qmckl_b200_mo_mixed");
   if (rc != QMCKL_SUCCESS) return rc;
-  QB_CUDA(tc_run(ds->T, ds->tc, P, comps, coord, cutoff_of(ctx), ds->tc_coef.p, ds->tc_a.p, out, ds->stream,
+  QB_CUDA(tc_run(ds->T, ds->tc3, P, comps, coord, cutoff_of(ctx), ds->tc3_coef.p, ds->tc_a.p, out, ds->stream,
                  ds->tiles.ntiles > 0 ? &ds->tiles : nullptr),
           "qmckl_b200_mo_mixed");
   return QMCKL_SUCCESS;
@@ -570,7 +653,8 @@ void dev_detach(Context* ctx) {
   if (ds->stream) cudaStreamSynchronize(ds->stream);
   for (DevBuf* b : {&ds->tables, &ds->nucl, &ds->coord, &ds->prim_vgl, &ds->shell_vgl, &ds->ao_vgl, &ds->ao_value,
                     &ds->mo_vgl, &ds->mo_value, &ds->coef_t, &ds->tc_coef, &ds->tc_a, &ds->krec, &ds->order,
-                    &ds->ao_hessian, &ds->coef_rows, &ds->adj_coord, &ds->adj_buf, &ds->adj_part, &ds->adj_nucl})
+                    &ds->ao_hessian, &ds->coef_rows, &ds->adj_coord, &ds->adj_buf, &ds->adj_part, &ds->adj_nucl,
+                    &ds->tc3_coef, &ds->env})
     release(*b);
   if (ds->own_stream && ds->stream) cudaStreamDestroy(ds->stream);
   delete ds;
@@ -586,8 +670,8 @@ qmckl_exit_code dev_prepared_mixed(qmckl_context context, PreparedMixed* out) {
   DeviceState* ds = ctx->extra;
   const char* fname = "qmckl_b200_mo_vgl_device_noalloc";
   if (ds == nullptr || ds->tables.p == nullptr || ds->basis_version != ctx->ao_basis.basis_version ||
-      ds->tc_coef.p == nullptr || ds->tc_coef_version != ctx->mo_basis.coef_version ||
-      ds->tc_pieces != ds->split_pieces || (ds->stream == nullptr && !ds->stream_given))
+      ds->tc3_coef.p == nullptr || ds->tc3_coef_version != ctx->mo_basis.coef_version ||
+      (ds->stream == nullptr && !ds->stream_given))
     return qmckl_failwith(context, QMCKL_NOT_PROVIDED, fname,
                           "basis or MO coefficients not on the device yet: run one regular mixed-form "
                           "evaluation of this context first");
@@ -601,8 +685,8 @@ qmckl_exit_code dev_prepared_mixed(qmckl_context context, PreparedMixed* out) {
   }
   out->T = ds->T;
   out->T.nucl_coord = (const double*)ds->nucl.p;
-  out->plan = ds->tc;
-  out->coef = ds->tc_coef.p;
+  out->plan = ds->tc3;
+  out->coef = ds->tc3_coef.p;
   out->stream = ds->stream;
   out->cutoff = cutoff_of(ctx);
   return QMCKL_SUCCESS;
@@ -610,7 +694,7 @@ qmckl_exit_code dev_prepared_mixed(qmckl_context context, PreparedMixed* out) {
 
 qmckl_exit_code dev_invalidate_mo(qmckl_context context) {
   DeviceState* ds = state(context);
-  if (ds) { ds->coef_version = ~0ull; ds->tc_coef_version = ~0ull; }
+  if (ds) { ds->coef_version = ~0ull; ds->tc_coef_version = ~0ull; ds->tc3_coef_version = ~0ull; }
   return QMCKL_SUCCESS;
 }
 

@@ -5,12 +5,12 @@
 // A CTA owns a tile of points and an N tile of MOs.  Its 128 accumulator rows
 // are (point, component) pairs: 25 points x 5 components (+3 zero rows) for
 // MO VGL, 128 points for MO value.  Per 64-AO K block, producer warps evaluate
-// the block's AOs at the tile's points and write them as bfloat16 split pieces
+// the block's AOs at the tile's points and write them as 16-bit split pieces
 // straight into the 128B-swizzled K-major shared-memory tile the tensor core
 // reads; the coefficient pieces arrive by TMA; one thread issues the
-// split-BF16 tcgen05.mma chain into three FP32 TMEM accumulators (leading
-// product in two K halves, corrections in the third); the epilogue sums them
-// in FP64.
+// split tcgen05.mma chain into three FP32 TMEM accumulators (leading product
+// in two K halves, corrections in the third); the epilogue sums them in FP64
+// and undoes the power-of-two scales.
 //
 // AO arithmetic (mixed form): FP64 displacement, r^2, exponent argument and
 // radial Laplacian factor, FP32 exponential when a r^2 <= 30 (FP64 above),
@@ -21,6 +21,7 @@
 #include <cuda.h>
 #include <cuda_bf16.h>
 
+#include "split.cuh"
 #include "tc_ptx.cuh"
 
 namespace qb {
@@ -55,7 +56,10 @@ __device__ __forceinline__ void radial_rec(const KRecShell& S, const double2* pr
   fx = (float)x;
   fy = (float)y;
   fz = (float)z;
-  double acc[5] = {0., 0., 0., 0., 0.};
+  // With S_n = sum_j c_j a_j^n e_j:  value S0, gradient -2 S1 (x, y, z),
+  // Laplacian sum_j c_j (-2 a_j e_j)(3 - 2 a_j r^2) = 4 r^2 S2 - 6 S1, all in
+  // FP64 (the Laplacian's cancellation happens before the FP32 rounding).
+  double S0 = 0.0, S1 = 0.0, S2 = 0.0;
   live = !(r2 > cutoff * S.range);
   if (live) {
     for (int j = S.pb; j < S.pe; ++j) {
@@ -63,16 +67,76 @@ __device__ __forceinline__ void radial_rec(const KRecShell& S, const double2* pr
       const double ar2 = pc.x * r2;
       if (ar2 > cutoff) break;   // sorted by exponent
       const double e = ar2 > 30.0 ? exp(-ar2) : (double)expf(-(float)ar2);
-      const double f = -2.0 * pc.x * e;
-      acc[0] += pc.y * e;
-      acc[1] += pc.y * (f * x);
-      acc[2] += pc.y * (f * y);
-      acc[3] += pc.y * (f * z);
-      acc[4] += pc.y * (f * (3.0 - 2.0 * ar2));
+      const double ce = pc.y * e;
+      const double ace = pc.x * ce;
+      S0 += ce;
+      S1 += ace;
+      S2 = fma(pc.x, ace, S2);
     }
   }
+  const double g = -2.0 * S1;
+  s[0] = (float)S0;
+  s[1] = (float)(g * x);
+  s[2] = (float)(g * y);
+  s[3] = (float)(g * z);
+  s[4] = (float)(fma(4.0 * r2, S2, -6.0 * S1));
+}
+
+// Per-row power-of-two scales of the 2-piece float16 operands (split.cuh).
+// Each accumulator row (point i, component c) is scaled by 2^-e so that its
+// AO values stay below 2^10 in magnitude; e comes from an upper bound of the
+// row's AOs: max over the nuclei of a per-nucleus envelope of |AO|, |grad AO|
+// or |lap AO| at the point's distance (RowBound.env, a suffix maximum over
+// geometric radial cells: cell 0 = [0, r0), cell g >= 1 starts at
+// r0 * 2^((g-1)/inv_log2q); built on the host).  Scales are exact, the
+// epilogue multiplies the row by 2^e again.
+constexpr int kEnvCells = 64;
+constexpr int kExpMin = -60, kExpMax = 60;
+struct RowBound {
+  const double* nucl;   // [3][nucl_num]
+  const float* env;     // [nucl_num][3][kEnvCells]: value, gradient, Laplacian envelopes
+  int nucl_num;
+  float r0, inv_log2q;
+};
+
+// 2^e for |e| <= 60, built from the exponent bits
+__device__ __forceinline__ float pow2f(int e) { return __int_as_float((127 + e) << 23); }
+__device__ __forceinline__ double pow2d(int e) { return __longlong_as_double((long long)(1023 + e) << 52); }
+
+// envelope group of a component: value 0, gradient 1, Laplacian 2
+template <int COMPS>
+__device__ __forceinline__ int comp_group(int c) {
+  return COMPS == 1 ? 0 : (c == 0 ? 0 : (c == 4 ? 2 : 1));
+}
+
+// rexp[3][PTS] (shared, preset to kExpMin) <- the scale exponents of the
+// tile's rows; all threads of the CTA take part (then a barrier).
+template <int PTS>
+__device__ __forceinline__ void row_exponents(const RowBound& RB, const double* pts, const int64_t* pidx, int* rexp,
+                                              int tid, int nthreads) {
+  const int N = RB.nucl_num;
+  for (int u = tid; u < PTS * N; u += nthreads) {
+    const int i = u % PTS, n = u / PTS;
+    if (pidx[i] < 0) continue;
+    const double dx = pts[i] - RB.nucl[n], dy = pts[PTS + i] - RB.nucl[n + N], dz = pts[2 * PTS + i] - RB.nucl[n + 2 * N];
+    const float r = sqrtf((float)(dx * dx + dy * dy + dz * dz));
+    int g = 0;
+    if (r >= RB.r0) {
+      // lower cell on a rounding tie: a larger (still valid) bound
+      const float x = log2f(r / RB.r0) * RB.inv_log2q - 1.0e-3f;
+      g = x < 0.f ? 1 : min(kEnvCells - 1, 1 + (int)x);
+    }
+    const float* e = RB.env + (size_t)n * 3 * kEnvCells + g;
 #pragma unroll
-  for (int c = 0; c < 5; ++c) s[c] = (float)acc[c];
+    for (int q = 0; q < 3; ++q) {
+      const float b = e[q * kEnvCells];
+      if (b > 0.f) {
+        int ex;
+        frexpf(b * (1.0f / 1024.0f), &ex);
+        atomicMax(&rexp[q * PTS + i], min(ex, kExpMax));
+      }
+    }
+  }
 }
 
 // Value, gradient and Laplacian of one AO from its shell's radial VGL (FP32).
@@ -119,14 +183,15 @@ __device__ __forceinline__ void ao_product(int code, float f, const float (&s)[5
 
 // One producer warp's share of a K block: AOs [CHUNK*j, CHUNK*j + CHUNK) of
 // the block (record `rec`) at the tile's points (pts [3][PTS] in shared
-// memory; lanes are points), written as PIECES bfloat16 pieces into the
+// memory; lanes are points), scaled by 2^-rexp[group][point] (2 pieces) and
+// written as PIECES 16-bit pieces (split.cuh) into the
 // swizzled A tiles at a_base (shared address; pieces A_TILE bytes apart).
 // p_first: index of the tile's first point among the P points (rows past P
 // are written as zeros).  Pairs of AOs that are zero at every point of the
 // warp skip the split arithmetic.
 template <int PIECES, int COMPS, int CHUNK>
 __device__ __forceinline__ void produce_kblock(const uint8_t* rec, const double* pts, int64_t p_first, int64_t P,
-                                               double cutoff, uint32_t a_base, int j, int lane) {
+                                               double cutoff, const int* rexp, uint32_t a_base, int j, int lane) {
   static_assert(CHUNK == 4 || CHUNK == 8, "a producer warp covers a half or a whole 16-byte chunk");
   constexpr int PTS = BM / COMPS;
   const int2* rao = (const int2*)(rec + kRecAoOff) + j * CHUNK;
@@ -137,6 +202,9 @@ __device__ __forceinline__ void produce_kblock(const uint8_t* rec, const double*
     const int ic = i < PTS ? i : PTS - 1;
     const bool active = i < PTS && p_first + i < P;
     const double px = pts[ic], py = pts[PTS + ic], pz = pts[2 * PTS + ic];
+    float inv[COMPS];
+#pragma unroll
+    for (int c = 0; c < COMPS; ++c) inv[c] = PIECES == 2 ? pow2f(-rexp[comp_group<COMPS>(c) * PTS + ic]) : 1.0f;
     uint32_t pk[PIECES][COMPS][CHUNK / 2];
     int prev = -1;
     float rs[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
@@ -173,18 +241,11 @@ __device__ __forceinline__ void produce_kblock(const uint8_t* rec, const double*
       }
 #pragma unroll
       for (int c = 0; c < COMPS; ++c) {
-        // round-to-nearest bf16 pieces of the two AOs, packed as bf16x2
-        const __nv_bfloat162 h2 = __floats2bfloat162_rn(v[0][c], v[1][c]);
-        const float2 hf = __bfloat1622float2(h2);
-        const float r0 = v[0][c] - hf.x, r1 = v[1][c] - hf.y;
-        const __nv_bfloat162 m2 = __floats2bfloat162_rn(r0, r1);
-        pk[0][c][t >> 1] = *reinterpret_cast<const uint32_t*>(&h2);
-        pk[1][c][t >> 1] = *reinterpret_cast<const uint32_t*>(&m2);
-        if (PIECES == 3) {
-          const float2 mf = __bfloat1622float2(m2);
-          const __nv_bfloat162 l2 = __floats2bfloat162_rn(r0 - mf.x, r1 - mf.y);
-          pk[PIECES - 1][c][t >> 1] = *reinterpret_cast<const uint32_t*>(&l2);
-        }
+        // pieces of the two AOs, packed two per 32-bit word (split.cuh)
+        uint32_t q3[3];
+        split_pair<PIECES>(v[0][c], v[1][c], inv[c], q3);
+#pragma unroll
+        for (int q = 0; q < PIECES; ++q) pk[q][c][t >> 1] = q3[q];
       }
     }
     if (i < PTS) {
@@ -234,21 +295,28 @@ __device__ __forceinline__ void mma_kblock(uint32_t base, uint32_t a_bytes, uint
   }
 }
 
+// Instruction descriptor of tcgen05.mma kind::f16: FP32 accumulator, A and B
+// both bfloat16 (3 pieces) or both float16 (2 pieces), K-major, M = 128.
+template <int PIECES>
 __device__ __forceinline__ uint32_t mma_idesc(int n_tile) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n_tile >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+  const uint32_t fmt = PIECES == 3 ? 1u : 0u;
+  return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(n_tile >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
 }
 
-// Epilogue of one warp (TMEM lanes 32*warp .. +31): FP64 sum of the three
-// accumulators, rows (tile point i, component c) written to
-// out[(pidx[i] * COMPS + c) * n_out + col] for the MO columns [n0, n0 + n_tile).
+// Epilogue of one warp (TMEM lanes 32*(warp%4) .. +31, 16-column chunks
+// chunk0, chunk0 + chunk_step, ...): FP64 sum of the three
+// accumulators times the row scale 2^rexp and the MO scale (split.cuh), rows
+// (tile point i, component c) written to out[(pidx[i] * COMPS + c) * n_out +
+// col] for the MO columns [n0, n0 + n_tile).
 // stage: 32 x 16 doubles of shared scratch for this warp.
-template <int COMPS>
+template <int PIECES, int COMPS>
 __device__ __forceinline__ void epilogue_warp(uint32_t tmem, int n_tile, int n0, int n_out, bool has_second,
-                                              const int64_t* pidx, double* out, double* stage, int warp,
-                                              int lane) {
+                                              const int64_t* pidx, const int* rexp, const double* scales,
+                                              double* out, double* stage, int warp, int lane, int chunk0 = 0,
+                                              int chunk_step = 1) {
   constexpr int PTS = BM / COMPS;
-  const int row_base = warp * 32;
-  for (int c0 = 0; c0 < n_tile; c0 += 16) {
+  const int row_base = (warp & 3) * 32;   // a warp reads the TMEM lanes of its quadrant
+  for (int c0 = 16 * chunk0; c0 < n_tile; c0 += 16 * chunk_step) {
     uint32_t r0[16], r1[16], r2[16];
     const uint32_t ta = tmem + ((uint32_t)row_base << 16) + (uint32_t)c0;
     tmem_ld16(ta, r0);
@@ -261,14 +329,20 @@ __device__ __forceinline__ void epilogue_warp(uint32_t tmem, int n_tile, int n0,
       stage[lane * 16 + ((j + lane) & 15)] = v;
     }
     __syncwarp();
+    const int cc = lane & 15;
+    const int col = n0 + c0 + cc;
+    const double cs = (PIECES == 2 && col < n_out) ? scales[kScaleCols + col] : 1.0;
     for (int q = 0; q < 16; ++q) {
       const int rr = 2 * q + (lane >> 4);
-      const int cc = lane & 15;
       const int r = row_base + rr;
-      const int col = n0 + c0 + cc;
       if (r < PTS * COMPS && col < n_out) {
         const int64_t pq = pidx[r / COMPS];
-        if (pq >= 0) out[(pq * COMPS + r % COMPS) * n_out + col] = stage[rr * 16 + ((cc + rr) & 15)];
+        if (pq >= 0) {
+          const int c = r % COMPS, i = r / COMPS;
+          double v = stage[rr * 16 + ((cc + rr) & 15)];
+          if (PIECES == 2) v *= cs * pow2d(rexp[comp_group<COMPS>(c) * PTS + i]);
+          out[(pq * COMPS + c) * n_out + col] = v;
+        }
       }
     }
     __syncwarp();

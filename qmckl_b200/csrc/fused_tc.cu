@@ -5,7 +5,7 @@
 // Warp roles: warps 0..15 produce the AO pieces of each 64-AO K block (4 AOs
 // per warp, lanes = points); warp 16 bulk-copies the block's record and
 // TMA-loads the coefficient pieces; warp 17 owns TMEM and issues the MMAs;
-// warps 0..3 then run the epilogue.  Every mbarrier wait is bounded (2 s of
+// the 16 producer warps then run the epilogue (4 per TMEM lane quadrant).  Every mbarrier wait is bounded (2 s of
 // %globaltimer); a timeout sets the error word and the CTA still releases its
 // TMEM.
 #include <cuda.h>
@@ -37,7 +37,8 @@ __global__ void __launch_bounds__(kThreadsF, 1)
 fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, const int64_t P,
                 const double* __restrict__ coord, const double cutoff, const int n_out, const int n_tile,
                 const int kblocks, const uint8_t* __restrict__ krec, const int rec_bytes,
-                const int* __restrict__ perm, double* __restrict__ out, int* __restrict__ err) {
+                const int* __restrict__ perm, const double* __restrict__ scales, const RowBound rb,
+                double* __restrict__ out, int* __restrict__ err) {
   constexpr int PTS = BM / COMPS;            // 25 points (VGL) or 128 (value)
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   // 1024-byte aligned base, kept as pointer arithmetic on the __shared__
@@ -54,6 +55,7 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
   uint32_t* tmem_slot = (uint32_t*)(acc_full + 1);
   double* pts = (double*)(acc_full + 2);      // [3][PTS]
   int64_t* pidx = (int64_t*)(pts + 3 * PTS);  // [PTS] original index of each tile point
+  int* rexp = (int*)(pidx + PTS);             // [3][PTS] row scale exponents (2 pieces)
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int64_t p0 = (int64_t)blockIdx.x * PTS;
@@ -75,6 +77,11 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
     const int64_t q = (p0 + i < P) ? (perm ? (int64_t)perm[p0 + i] : p0 + i) : -1;
     pts[t] = q >= 0 ? coord[q + d * P] : 0.0;
     if (d == 0) pidx[i] = q;
+    rexp[t] = PIECES == 2 ? kExpMin : 0;
+  }
+  if (PIECES == 2) {
+    __syncthreads();
+    row_exponents<PTS>(rb, pts, pidx, rexp, tid, kThreadsF);
   }
   // rows PTS*COMPS .. 127 of the A tiles stay zero for the whole kernel
   zero_pad_rows<PIECES, COMPS, STAGES>(smem, STAGE, tid, kThreadsF);
@@ -101,7 +108,7 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
       ok = ok && mbar_wait(&rec_full[s], phase, err, 15);
       if (!__all_sync(0xffffffffu, ok)) break;
       const uint32_t a_base = smem_addr(smem + s * STAGE);
-      produce_kblock<PIECES, COMPS, kChunk>(recs + s * rec_bytes, pts, p0, P, cutoff, a_base, j, lane);
+      produce_kblock<PIECES, COMPS, kChunk>(recs + s * rec_bytes, pts, p0, P, cutoff, rexp, a_base, j, lane);
       fence_async_smem();
       mbar_arrive(&full[s]);
     }
@@ -122,7 +129,7 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
   } else {
     // ---------------- MMA issuer
     if (lane == 0) {
-      const uint32_t idesc = mma_idesc(n_tile);
+      const uint32_t idesc = mma_idesc<PIECES>(n_tile);
       for (int kb = 0; kb < kblocks; ++kb) {
         const int s = kb & 1;
         const uint32_t phase = (uint32_t)(kb >> 1) & 1u;
@@ -136,14 +143,15 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
     }
   }
 
-  if (warp < 4) {
-    // ---------------- epilogue: TMEM lanes 32*warp .. 32*warp+31
+  if (warp < kProdWarps) {
+    // ---------------- epilogue: every producer warp, TMEM lane quadrant warp % 4,
+    // a quarter of the 16-column chunks (staging in the idle stage memory)
     bool ok = mbar_wait(acc_full, 0, err, 14);
     ok = __all_sync(0xffffffffu, ok && *(volatile int*)err == 0);
     tc_fence_after();
     if (ok)
-      epilogue_warp<COMPS>(tmem, n_tile, n0, n_out, kblocks >= 2, pidx, out, (double*)smem + warp * 32 * 16, warp,
-                           lane);
+      epilogue_warp<PIECES, COMPS>(tmem, n_tile, n0, n_out, kblocks >= 2, pidx, rexp, scales, out,
+                                   (double*)smem + warp * 32 * 16, warp, lane, warp >> 2, kProdWarps / 4);
   }
   tc_fence_before();
   __syncthreads();
@@ -182,20 +190,22 @@ template <int PIECES, int COMPS>
 size_t fused_smem(int n_tile, int rec_bytes) {
   constexpr int PTS = BM / COMPS;
   const size_t stage = (size_t)PIECES * (A_TILE + (size_t)n_tile * BK * 2);
-  return 1024 + STAGES * stage + (size_t)STAGES * rec_bytes + (3 * STAGES + 2) * 8 + 4 * PTS * 8 + 16;
+  return 1024 + STAGES * stage + (size_t)STAGES * rec_bytes + (3 * STAGES + 2) * 8 + 4 * PTS * 8 + 3 * PTS * 4 + 16;
 }
 
 template <int PIECES, int COMPS>
 cudaError_t launch_fused(const DevTables& T, const CUtensorMap& tb, int64_t P, const double* coord, double cutoff,
                          int n_out, int n_tile, int n_tiles, int kblocks, const uint8_t* krec, int rec_bytes,
-                         const int* perm, double* out, int* err, cudaStream_t s) {
+                         const int* perm, const double* scales, const RowBound& rb, double* out, int* err,
+                         cudaStream_t s) {
   constexpr int PTS = BM / COMPS;
   const size_t smem = fused_smem<PIECES, COMPS>(n_tile, rec_bytes);
   auto kern = fused_mo_kernel<PIECES, COMPS>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid((unsigned)((P + PTS - 1) / PTS), (unsigned)n_tiles);
-  kern<<<grid, kThreadsF, smem, s>>>(T, tb, P, coord, cutoff, n_out, n_tile, kblocks, krec, rec_bytes, perm, out, err);
+  kern<<<grid, kThreadsF, smem, s>>>(T, tb, P, coord, cutoff, n_out, n_tile, kblocks, krec, rec_bytes, perm, scales,
+                                     rb, out, err);
   count_launch();
   return cudaGetLastError();
 }
@@ -221,28 +231,29 @@ cudaError_t tc_encode_coef_map(const TcPlan& plan, const void* d_coef, CUtensorM
 }
 
 cudaError_t tc_launch_fused(const TcPlan& plan, int64_t point_num, int comps, const double* coord, double cutoff,
-                            const CUtensorMap& tb, const void* krec, int rec_bytes, const int* perm, double* out,
-                            int* err, cudaStream_t s) {
+                            const CUtensorMap& tb, const void* krec, int rec_bytes, const int* perm, const void* d_coef,
+                            const RowBound& rb, double* out, int* err, cudaStream_t s) {
   if (point_num <= 0) return cudaSuccess;
   if (rec_bytes <= 0 || rec_bytes % 128 != 0) return cudaErrorInvalidValue;
   const DevTables T{};   // the fused kernel reads the records only
   const int kblocks = (int)((plan.ao_num + BK - 1) / BK);
   const uint8_t* kr = (const uint8_t*)krec;
   const int M = (int)plan.mo_num;
+  const double* sc = tc_scales(plan, d_coef);
   if (plan.pieces == 3)
     return comps == 5 ? launch_fused<3, 5>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
-                                           rec_bytes, perm, out, err, s)
+                                           rec_bytes, perm, sc, rb, out, err, s)
                       : launch_fused<3, 1>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
-                                           rec_bytes, perm, out, err, s);
+                                           rec_bytes, perm, sc, rb, out, err, s);
   return comps == 5 ? launch_fused<2, 5>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
-                                         rec_bytes, perm, out, err, s)
+                                         rec_bytes, perm, sc, rb, out, err, s)
                     : launch_fused<2, 1>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
-                                         rec_bytes, perm, out, err, s);
+                                         rec_bytes, perm, sc, rb, out, err, s);
 }
 
 cudaError_t tc_run_fused(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps, const double* coord,
                          double cutoff, const void* d_coef, const void* krec, int rec_bytes, const int* perm,
-                         double* out, cudaStream_t s) {
+                         const RowBound& rb, double* out, cudaStream_t s) {
   (void)T;
   if (point_num <= 0) return cudaSuccess;
   CUtensorMap tb;
@@ -250,7 +261,7 @@ cudaError_t tc_run_fused(const DevTables& T, const TcPlan& plan, int64_t point_n
   if (e != cudaSuccess) return e;
   int* err = fused_err_word();
   if (!err) return cudaErrorMemoryAllocation;
-  e = tc_launch_fused(plan, point_num, comps, coord, cutoff, tb, krec, rec_bytes, perm, out, err, s);
+  e = tc_launch_fused(plan, point_num, comps, coord, cutoff, tb, krec, rec_bytes, perm, d_coef, rb, out, err, s);
   if (e != cudaSuccess) return e;
   int h = 0;
   e = cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s);

@@ -139,6 +139,8 @@ struct PreparedMixed;
 qmckl_exit_code dev_prepared_mixed(qmckl_context context, PreparedMixed* out);
 // K-block records of the fused kernels for the basis and nuclei of a context (device.cu)
 bool build_krec_records(const Context* ctx, std::vector<uint8_t>& records, int& rec_bytes);
+// Row-bound envelopes of the mixed form's 2-piece float16 operands (device.cu)
+void build_envelopes(const Context* ctx, std::vector<float>& env, float& r0, float& inv_log2q);
 
 // AO finalization helpers (ao_basis.cpp)
 qmckl_exit_code finalize_basis(qmckl_context context);

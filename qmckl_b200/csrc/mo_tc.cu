@@ -4,11 +4,12 @@
 // (comps*point_num) x ao_num matrix (qmckl_compute_mo_basis_mo_vgl_hpc,
 // org/qmckl_mo.org:2015-2163, in dense form) and C = coefficient[mo][ao].
 //
-// Both operands are split into bfloat16 pieces, X = X1 + X2 (+ X3), the
-// pieces of A produced by the mixed AO kernel and those of C once per
-// coefficient update.  Products X_i*Y_j with i + j < pieces are accumulated
-// in FP32 in tensor memory: 3 products for 2 pieces (error ~2^-16 relative),
-// 6 products for 3 pieces (~2^-24, below the FP32 rounding of the AOs).
+// Both operands are split into 16-bit pieces (split.cuh: 3 bfloat16 pieces,
+// or 2 float16 pieces of power-of-two scaled values), the pieces of A
+// produced by the mixed AO kernel and those of C once per coefficient
+// update.  Products X_i*Y_j with i + j < pieces are accumulated in FP32 in
+// tensor memory: 6 products for 3 bfloat16 pieces, 3 for 2 float16 pieces
+// (both ~2^-22..2^-24 relative, below the FP32 rounding of the AOs).
 // The rounding of the FP32 accumulation grows with the number of
 // accumulation steps, so the leading product A1*C1 is accumulated in two
 // accumulators (first and second half of K) and the correction products,
@@ -35,6 +36,7 @@
 
 #include "ao_tile.cuh"
 #include "mo_tc.cuh"
+#include "split.cuh"
 #include "tc_ptx.cuh"
 
 namespace qb {
@@ -54,8 +56,9 @@ constexpr int kThreads = 32 * (kEpiWarps + 2);
 template <int PIECES, int STAGES>
 __global__ void __launch_bounds__(kThreads, 1)
 tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-               const int64_t M, const int n_out, const int n_tile, const int kblocks,
-               double* __restrict__ out, const int64_t ldo, int* __restrict__ err) {
+               const int64_t M, const int n_out, const int n_tile, const int kblocks, const int comps,
+               const double* __restrict__ scales, double* __restrict__ out, const int64_t ldo,
+               int* __restrict__ err) {
   constexpr int NPROD = PIECES == 3 ? 6 : 3;
   constexpr int A_TILE = BM * BK * 2;             // bytes of one A piece tile
   extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -115,7 +118,8 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
   } else if (warp == kEpiWarps + 1) {
     // ---------------- MMA issuer
     if (lane == 0) {
-      const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n_tile >> 3) << 17) |
+      const uint32_t fmt = PIECES == 3 ? 1u : 0u;   // bfloat16 or float16 operands
+      const uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(n_tile >> 3) << 17) |
                              ((uint32_t)(BM >> 4) << 24);
       // products (i, j) with i + j < PIECES, smallest terms first
       constexpr int pa3[6] = {2, 1, 0, 1, 0, 0}, pb3[6] = {0, 1, 2, 0, 1, 0};
@@ -174,7 +178,9 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
           const int cc = lane & 15;
           const int64_t row = m0 + row_base + rr;
           const int col = n0 + c0 + cc;
-          if (row < M && col < n_out) out[row * ldo + col] = stage[rr * 16 + ((cc + rr) & 15)];
+          if (row < M && col < n_out)
+            out[row * ldo + col] =
+                stage[rr * 16 + ((cc + rr) & 15)] * (scales[(int)(row % comps)] * scales[kScaleCols + col]);
         }
         __syncwarp();
       }
@@ -190,20 +196,6 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
 
 // ------------------------------------------------------------ A pieces
 
-// bf16 round-to-nearest split of an FP32 value into `pieces` terms.
-template <int PIECES>
-__device__ __forceinline__ void split_bf16(float v, __nv_bfloat16 (&o)[3]) {
-  const __nv_bfloat16 h = __float2bfloat16_rn(v);
-  o[0] = h;
-  float r = v - __bfloat162float(h);
-  const __nv_bfloat16 m = __float2bfloat16_rn(r);
-  o[1] = m;
-  if (PIECES == 3) {
-    r = r - __bfloat162float(m);
-    o[2] = __float2bfloat16_rn(r);
-  }
-}
-
 constexpr int kAoWarps = 8;
 
 struct MixSmem {
@@ -214,12 +206,16 @@ struct MixSmem {
 // Mixed-form AO VGL: radial part with FP64 displacement, r^2, exponent
 // argument, radial Laplacian factor and FP64 accumulation (FP32 exponential
 // when a r^2 <= 30, FP64 above); monomials and the product rule in FP32; the
-// five components of each AO written as bf16 pieces of rows p*comps + c.
+// five components of each AO written as 16-bit pieces (split.cuh) of rows
+// p*comps + c.
 template <int PIECES, int COMPS>
 __global__ void __launch_bounds__(kAoWarps * 32)
 ao_split_kernel(const DevTables T, const int64_t point_num, const double* __restrict__ coord, const double cutoff,
-                __nv_bfloat16* __restrict__ a, const int64_t lda, const int64_t piece_stride) {
+                const double* __restrict__ scales, uint16_t* __restrict__ a, const int64_t lda,
+                const int64_t piece_stride) {
   __shared__ MixSmem smem[kAoWarps];
+  float inv[5];
+  load_inv_scales<COMPS>(scales, inv);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   MixSmem& sm = smem[warp];
   const int64_t items = point_num * (int64_t)T.nblock;
@@ -314,8 +310,8 @@ ao_split_kernel(const DevTables T, const int64_t point_num, const double* __rest
       }
 #pragma unroll
       for (int c = 0; c < COMPS; ++c) {
-        __nv_bfloat16 pcs[3];
-        split_bf16<PIECES>(v[c], pcs);
+        uint16_t pcs[3];
+        split_one<PIECES>(v[c], inv[c], pcs);
         const int64_t off = (p * COMPS + c) * lda + k;
 #pragma unroll
         for (int q = 0; q < PIECES; ++q) a[q * piece_stride + off] = pcs[q];
@@ -377,14 +373,15 @@ int* err_word() {
 
 template <int PIECES, int STAGES>
 cudaError_t launch_gemm(const CUtensorMap& ta, const CUtensorMap& tb, int64_t M, int n_out, int n_tile, int n_tiles,
-                        int kblocks, double* out, int64_t ldo, int* err, cudaStream_t s) {
+                        int kblocks, int comps, const double* scales, double* out, int64_t ldo, int* err,
+                        cudaStream_t s) {
   const size_t stage = (size_t)PIECES * (BM * BK * 2 + (size_t)n_tile * BK * 2);
   const size_t smem = 1024 + STAGES * stage + (2 * STAGES + 1) * 8 + 16;
   auto kern = tc_gemm_kernel<PIECES, STAGES>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid((unsigned)((M + BM - 1) / BM), (unsigned)n_tiles);
-  kern<<<grid, kThreads, smem, s>>>(ta, tb, M, n_out, n_tile, kblocks, out, ldo, err);
+  kern<<<grid, kThreads, smem, s>>>(ta, tb, M, n_out, n_tile, kblocks, comps, scales, out, ldo, err);
   count_launch();
   return cudaGetLastError();
 }
@@ -409,7 +406,8 @@ TcPlan tc_plan(int64_t ao_num, int64_t mo_num, int pieces) {
     p.n_tile = (int)((q + 15) / 16 * 16);
   }
   p.n_pad = (int64_t)p.n_tile * p.n_tiles;
-  p.coef_bytes = (size_t)pieces * p.n_pad * p.k_pad * 2;
+  p.scale_off = ((size_t)pieces * p.n_pad * p.k_pad * 2 + 255) / 256 * 256;
+  p.coef_bytes = p.scale_off + sizeof(double) * (kScaleCols + (size_t)p.n_pad);
   return p;
 }
 
@@ -417,57 +415,121 @@ size_t tc_a_bytes(const TcPlan& plan, int64_t rows) { return (size_t)plan.pieces
 
 cudaError_t tc_prepare_coef(const TcPlan& plan, const double* coefficient_host, void* d_coef, cudaStream_t s) {
   const int64_t A = plan.ao_num, M = plan.mo_num, KP = plan.k_pad, NP = plan.n_pad;
-  std::vector<uint16_t> h((size_t)plan.pieces * NP * KP, 0);
-  auto to_bf16 = [](double x) -> uint16_t {   // round to nearest even of the FP32 rounding
-    float f = (float)x;
-    uint32_t u;
-    std::memcpy(&u, &f, 4);
-    if ((u & 0x7f800000u) == 0x7f800000u) return (uint16_t)(u >> 16);
-    u += 0x7fffu + ((u >> 16) & 1u);
-    return (uint16_t)(u >> 16);
-  };
-  auto from_bf16 = [](uint16_t b) -> double {
-    uint32_t u = (uint32_t)b << 16;
-    float f;
-    std::memcpy(&f, &u, 4);
-    return (double)f;
-  };
-  for (int64_t i = 0; i < M; ++i)
-    for (int64_t k = 0; k < A; ++k) {
-      double r = coefficient_host[i * A + k];
-      for (int p = 0; p < plan.pieces; ++p) {
-        const uint16_t b = to_bf16(r);
-        h[((size_t)p * NP + i) * KP + k] = b;
-        r -= from_bf16(b);
+  std::vector<uint8_t> h(plan.coef_bytes, 0);
+  uint16_t* pc = (uint16_t*)h.data();
+  double* sc = (double*)(h.data() + plan.scale_off);
+  for (int i = 0; i < kScaleCols + NP; ++i) sc[i] = 1.0;
+  if (plan.pieces == 3) {
+    auto to_bf16 = [](double x) -> uint16_t {   // round to nearest even of the FP32 rounding
+      float f = (float)x;
+      uint32_t u;
+      std::memcpy(&u, &f, 4);
+      if ((u & 0x7f800000u) == 0x7f800000u) return (uint16_t)(u >> 16);
+      u += 0x7fffu + ((u >> 16) & 1u);
+      return (uint16_t)(u >> 16);
+    };
+    auto from_bf16 = [](uint16_t b) -> double {
+      uint32_t u = (uint32_t)b << 16;
+      float f;
+      std::memcpy(&f, &u, 4);
+      return (double)f;
+    };
+    for (int64_t i = 0; i < M; ++i)
+      for (int64_t k = 0; k < A; ++k) {
+        double r = coefficient_host[i * A + k];
+        for (int p = 0; p < 3; ++p) {
+          const uint16_t b = to_bf16(r);
+          pc[((size_t)p * NP + i) * KP + k] = b;
+          r -= from_bf16(b);
+        }
+      }
+  } else {
+    for (int64_t i = 0; i < M; ++i) {
+      double mx = 0.0;
+      for (int64_t k = 0; k < A; ++k) mx = std::max(mx, std::fabs(coefficient_host[i * A + k]));
+      // per-MO power of two bringing the largest coefficient to 2^10
+      const double tau = mx > 0.0 ? std::ldexp(1.0, (int)std::ceil(std::log2(mx / 1024.0))) : 1.0;
+      sc[kScaleCols + i] = tau;
+      for (int64_t k = 0; k < A; ++k) {
+        const double x = coefficient_host[i * A + k] / tau;
+        const __half x1 = __float2half_rn((float)x);
+        const __half x2 = __float2half_rn((float)(x - (double)__half2float(x1)));
+        pc[((size_t)0 * NP + i) * KP + k] = __half_as_ushort(x1);
+        pc[((size_t)1 * NP + i) * KP + k] = __half_as_ushort(x2);
       }
     }
-  cudaError_t e = cudaMemcpyAsync(d_coef, h.data(), h.size() * 2, cudaMemcpyHostToDevice, s);
+  }
+  cudaError_t e = cudaMemcpyAsync(d_coef, h.data(), h.size(), cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return e;
   return cudaStreamSynchronize(s);   // the host staging buffer goes out of scope
+}
+
+void tc_envelope(const ShellBound* shells, int nshell, double r_max, float r0, float inv_log2q, float* env) {
+  using fz::kEnvCells;
+  // Upper bounds, with |x^a y^b z^c| <= r^l, |grad P| <= l r^(l-1),
+  // |lap P| <= l(l-1) r^(l-2) and, for R(r) = sum c exp(-a r^2) with
+  // S_n = sum c a^n exp(-a r^2): |grad R| = 2 r |S1|, lap R = 4 r^2 S2 - 6 S1.
+  // Sampled 16 times per radial cell; the envelope of a cell is the maximum
+  // over it and every later cell (suffix maximum), doubled for the sampling.
+  constexpr int kSub = 16;
+  double cell[3][kEnvCells];
+  for (int q = 0; q < 3; ++q)
+    for (int g = 0; g < kEnvCells; ++g) cell[q][g] = 0.0;
+  auto start = [&](int g) { return g == 0 ? 0.0 : (double)r0 * std::exp2((double)(g - 1) / inv_log2q); };
+  for (int g = 0; g < kEnvCells; ++g) {
+    const double a0 = start(g);
+    const double a1 = g + 1 < kEnvCells ? start(g + 1) : std::max(a0, r_max);
+    for (int t = 0; t <= kSub; ++t) {
+      const double r = a0 + (a1 - a0) * t / kSub;
+      if (r > r_max) break;
+      for (int s = 0; s < nshell; ++s) {
+        const ShellBound& S = shells[s];
+        double S0 = 0.0, S1 = 0.0, S2 = 0.0;
+        for (int j = 0; j < S.nprim; ++j) {
+          const double e = S.coef[j] * std::exp(-S.expo[j] * r * r);
+          S0 += e;
+          S1 += S.expo[j] * e;
+          S2 += S.expo[j] * S.expo[j] * e;
+        }
+        const int l = S.l;
+        const double rl = std::pow(r, l), rl1 = l >= 1 ? l * std::pow(r, l - 1) : 0.0,
+                     rl2 = l >= 2 ? l * (l - 1) * std::pow(r, l - 2) : 0.0;
+        const double gR = 2.0 * r * std::fabs(S1), lR = std::fabs(4.0 * r * r * S2 - 6.0 * S1);
+        cell[0][g] = std::max(cell[0][g], S.factor * rl * std::fabs(S0));
+        cell[1][g] = std::max(cell[1][g], S.factor * (rl1 * std::fabs(S0) + rl * gR));
+        cell[2][g] = std::max(cell[2][g], S.factor * (rl2 * std::fabs(S0) + 2.0 * rl1 * gR + rl * lR));
+      }
+    }
+  }
+  for (int q = 0; q < 3; ++q) {
+    double m = 0.0;
+    for (int g = kEnvCells - 1; g >= 0; --g) {
+      m = std::max(m, cell[q][g]);
+      env[q * kEnvCells + g] = (float)(2.0 * m);
+    }
+  }
 }
 
 cudaError_t tc_run(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps, const double* coord,
                    double cutoff, const void* d_coef, void* d_a, double* out, cudaStream_t s,
                    const AoTiles* tiles) {
   if (point_num <= 0) return cudaSuccess;
+  if (plan.pieces != 3) return cudaErrorInvalidValue;   // the unfused kernels take 3 bfloat16 pieces
   const int64_t rows = (int64_t)comps * point_num;
   const int64_t lda = plan.k_pad;
   const int64_t pstride = rows * lda;
-  __nv_bfloat16* a = (__nv_bfloat16*)d_a;
+  uint16_t* a = (uint16_t*)d_a;
+  const double* sc = tc_scales(plan, d_coef);
   // 1) AO pieces
   if (tiles != nullptr) {
-    cudaError_t e = launch_ao_tile_split(T, *tiles, point_num, coord, cutoff, comps, plan.pieces, a, lda, pstride, s);
+    cudaError_t e =
+        launch_ao_tile_split(T, *tiles, point_num, coord, cutoff, comps, plan.pieces, sc, a, lda, pstride, s);
     if (e != cudaSuccess) return e;
   } else {
     const int64_t items = point_num * T.nblock;
     const int grid = (int)std::min<int64_t>((items + kAoWarps - 1) / kAoWarps, (int64_t)sm_count() * 8);
-    if (plan.pieces == 3) {
-      if (comps == 5) ao_split_kernel<3, 5><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, a, lda, pstride);
-      else ao_split_kernel<3, 1><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, a, lda, pstride);
-    } else {
-      if (comps == 5) ao_split_kernel<2, 5><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, a, lda, pstride);
-      else ao_split_kernel<2, 1><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, a, lda, pstride);
-    }
+    if (comps == 5) ao_split_kernel<3, 5><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, sc, a, lda, pstride);
+    else ao_split_kernel<3, 1><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, sc, a, lda, pstride);
     count_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -481,10 +543,8 @@ cudaError_t tc_run(const DevTables& T, const TcPlan& plan, int64_t point_num, in
   if (!err) return cudaErrorMemoryAllocation;
   const int kblocks = (int)((plan.ao_num + BK - 1) / BK);
   cudaError_t e;
-  if (plan.pieces == 3)
-    e = launch_gemm<3, 2>(ta, tb, rows, (int)plan.mo_num, plan.n_tile, plan.n_tiles, kblocks, out, plan.mo_num, err, s);
-  else
-    e = launch_gemm<2, 3>(ta, tb, rows, (int)plan.mo_num, plan.n_tile, plan.n_tiles, kblocks, out, plan.mo_num, err, s);
+  e = launch_gemm<3, 2>(ta, tb, rows, (int)plan.mo_num, plan.n_tile, plan.n_tiles, kblocks, comps, sc, out,
+                        plan.mo_num, err, s);
   if (e != cudaSuccess) return e;
   // surface a timed-out barrier wait as an error (the word is cleared for the next call)
   int h = 0;
@@ -503,21 +563,18 @@ cudaError_t tc_run_scratch(const DevTables& T, const TcPlan& plan, int64_t point
                            const double* coord, double cutoff, const void* d_coef, void* d_a, int* d_err,
                            double* out, cudaStream_t s) {
   if (point_num <= 0) return cudaSuccess;
+  if (plan.pieces != 3) return cudaErrorInvalidValue;   // the unfused kernels take 3 bfloat16 pieces
   cudaError_t e = cudaMemsetAsync(d_err, 0, sizeof(int), s);
   if (e != cudaSuccess) return e;
   const int64_t rows = (int64_t)comps * point_num;
   const int64_t lda = plan.k_pad;
   const int64_t pstride = rows * lda;
-  __nv_bfloat16* a = (__nv_bfloat16*)d_a;
+  uint16_t* a = (uint16_t*)d_a;
+  const double* sc = tc_scales(plan, d_coef);
   const int64_t items = point_num * T.nblock;
   const int grid = (int)std::min<int64_t>((items + kAoWarps - 1) / kAoWarps, (int64_t)sm_count() * 8);
-  if (plan.pieces == 3) {
-    if (comps == 5) ao_split_kernel<3, 5><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, a, lda, pstride);
-    else ao_split_kernel<3, 1><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, a, lda, pstride);
-  } else {
-    if (comps == 5) ao_split_kernel<2, 5><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, a, lda, pstride);
-    else ao_split_kernel<2, 1><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, a, lda, pstride);
-  }
+  if (comps == 5) ao_split_kernel<3, 5><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, sc, a, lda, pstride);
+  else ao_split_kernel<3, 1><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, sc, a, lda, pstride);
   count_launch();
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
@@ -526,10 +583,8 @@ cudaError_t tc_run_scratch(const DevTables& T, const TcPlan& plan, int64_t point
   if (!make_map(&tb, d_coef, plan.ao_num, plan.n_pad, plan.k_pad, plan.pieces, plan.n_pad * plan.k_pad, plan.n_tile))
     return cudaErrorInvalidValue;
   const int kblocks = (int)((plan.ao_num + BK - 1) / BK);
-  if (plan.pieces == 3)
-    e = launch_gemm<3, 2>(ta, tb, rows, (int)plan.mo_num, plan.n_tile, plan.n_tiles, kblocks, out, plan.mo_num, d_err, s);
-  else
-    e = launch_gemm<2, 3>(ta, tb, rows, (int)plan.mo_num, plan.n_tile, plan.n_tiles, kblocks, out, plan.mo_num, d_err, s);
+  e = launch_gemm<3, 2>(ta, tb, rows, (int)plan.mo_num, plan.n_tile, plan.n_tiles, kblocks, comps, sc, out,
+                        plan.mo_num, d_err, s);
   if (e != cudaSuccess) return e;
   int h = 0;
   e = cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, s);

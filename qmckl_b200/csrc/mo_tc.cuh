@@ -12,6 +12,7 @@
 #include <cstddef>
 #include <cstdint>
 
+#include "fused_common.cuh"
 #include "kernels.cuh"
 
 namespace qb {
@@ -23,13 +24,32 @@ struct TcPlan {
   int64_t n_pad = 0;     // MO count padded to a multiple of 16 (one tile <= 256)
   int n_tiles = 0;       // number of N tiles of n_tile columns
   int n_tile = 0;
-  size_t coef_bytes = 0; // pieces * n_pad * k_pad bfloat16
+  size_t scale_off = 0;  // byte offset of the scale block (split.cuh) after the pieces
+  size_t coef_bytes = 0; // pieces * n_pad * k_pad 16-bit values + the scale block
 };
+
+// Device pointer to the scale block of a plan's coefficient buffer.
+inline const double* tc_scales(const TcPlan& plan, const void* d_coef) {
+  return (const double*)((const char*)d_coef + plan.scale_off);
+}
 
 TcPlan tc_plan(int64_t ao_num, int64_t mo_num, int pieces);
 size_t tc_a_bytes(const TcPlan& plan, int64_t rows);
-// coefficient [mo][ao] (host, FP64) -> split bf16 pieces on the device
+// coefficient [mo][ao] (host, FP64) -> split pieces and the scale block on
+// the device (per-MO scales for 2 pieces).
 cudaError_t tc_prepare_coef(const TcPlan& plan, const double* coefficient_host, void* d_coef, cudaStream_t s);
+// Envelopes of the row bounds (fused_common.cuh RowBound) for one nucleus:
+// env[3][kEnvCells] <- suffix maxima over the radial cells of upper bounds
+// of |AO|, |grad AO| and |lap AO| over the nucleus's shells (shells: l, AO
+// factor bound, primitive exponents / coefficients; AOs vanish beyond r_max).
+struct ShellBound {
+  int l;
+  double factor;
+  const double* expo;
+  const double* coef;
+  int nprim;
+};
+void tc_envelope(const ShellBound* shells, int nshell, double r_max, float r0, float inv_log2q, float* env);
 // AO (mixed) -> A pieces -> tensor-core GEMM -> out[(point*comps + c)][mo] FP64
 // `tiles` selects the tiled AO kernel (ao_tile.cu) for the pieces when given.
 struct AoTiles;
@@ -41,16 +61,17 @@ cudaError_t tc_run(const DevTables& T, const TcPlan& plan, int64_t point_num, in
 // GEMM kernel itself and never written to device memory (fused_tc.cu).
 // krec: one record of rec_bytes per 64-AO K block (see fused_tc.cu); perm
 // (optional): order in which the points are grouped into tiles.
+// rb: the per-row scale bounds of 2-piece float16 operands (fused_common.cuh).
 cudaError_t tc_run_fused(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps, const double* coord,
                          double cutoff, const void* d_coef, const void* krec, int rec_bytes, const int* perm,
-                         double* out, cudaStream_t s);
+                         const fz::RowBound& rb, double* out, cudaStream_t s);
 // TMA map of a plan's coefficient pieces (box: 64 AOs x n_tile MOs x 1 piece,
 // 128B swizzle) and a launch of the fused kernel that does not wait for it
 // (err: device error word, left for the caller to check).
 cudaError_t tc_encode_coef_map(const TcPlan& plan, const void* d_coef, CUtensorMap* map);
 cudaError_t tc_launch_fused(const TcPlan& plan, int64_t point_num, int comps, const double* coord, double cutoff,
-                            const CUtensorMap& map, const void* krec, int rec_bytes, const int* perm, double* out,
-                            int* err, cudaStream_t s);
+                            const CUtensorMap& map, const void* krec, int rec_bytes, const int* perm, const void* d_coef,
+                            const fz::RowBound& rb, double* out, int* err, cudaStream_t s);
 // Spatial order of points (32^3 cells over [box_lo, box_hi], Morton order) by
 // a counting sort: perm[P]; keys[P] and counts[kSortCells + 1] are scratch.
 constexpr int kSortCells = 1 << 15;
