@@ -335,6 +335,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default=os.environ.get("QMCKL_B200_BENCH_FORM", "mixed"), choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--unfused", action="store_true",
+                    help="mixed form with the AO pieces written to HBM and a separate tensor-core GEMM")
     ap.add_argument("--pieces", type=int, default=3, choices=[2, 3],
                     help="operand split of the mixed form: 3 bfloat16 pieces (default) or 2 float16 pieces")
     ap.add_argument("--profile", choices=["fused", "split", "fp64"],
@@ -364,6 +366,7 @@ def main():
 
     from qmckl_b200 import gen
     from qmckl_b200 import qmckl as pq
+    from qmckl_b200 import replicas
     from qmckl_b200.system import make_context
 
     sysd = gen.config(1)
@@ -373,6 +376,8 @@ def main():
     ctx = make_context(sysd, points=False, form=form)
     if form == pq.FORM_MIXED:
         pq.b200_set_split_terms(ctx, args.pieces)
+        if args.unfused:
+            pq.b200_set_mixed_kernel(ctx, False)
     stream = torch.cuda.Stream()          # evaluation stream shared by torch and the library
     torch.cuda.set_stream(stream)
     pq.b200_set_stream(ctx, stream.cuda_stream)
@@ -437,11 +442,7 @@ def main():
             e1.synchronize()
             ao_times.append(e0.elapsed_time(e1))
     clocks = sampler.stop()
-    ms = statistics.mean(times)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = replicas.max_over_ranks(statistics.mean(times), device="cuda")
 
     # end to end through the public host API (pinned host buffers)
     h_coord = torch.from_numpy(np.ascontiguousarray(sysd["elec_coord"].reshape(-1))).pin_memory()
@@ -471,12 +472,8 @@ def main():
         e1.record(stream)
         e1.synchronize()
         e2e_times.append(e0.elapsed_time(e1))
-    e2e_ms = statistics.mean(e2e_times)
     pq.context_destroy(ctx_e)
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = replicas.max_over_ranks(statistics.mean(e2e_times), device="cuda")
 
     hbm, bf16, bf16_sus, peak_src = load_peaks()
     traffic = load_traffic()
@@ -500,11 +497,16 @@ def main():
         k_pad = -(-A // 64) * 64
         nprod = 6 if args.pieces == 3 else 3
         executed = 2.0 * tiles * 128 * n_pad * k_pad * nprod
-        achieved = executed / (ms * 1e-3) / 1e12
         t = traffic.get(("fused_mo_kernel", "mixed"))
         kname = ("fused_mo_kernel<3,5> (AO -> split-BF16 tcgen05 MO VGL" if args.pieces == 3 else
-                 "fused_mo_kernel<2,5> (AO -> split-FP16 tcgen05 MO VGL")
-        roofline = {"kernel": kname + "; step = 3 ordering kernels + this)",
+                 "fused_mo_kernel<2,5> (AO -> split-FP16 tcgen05 MO VGL") + "; step = 3 ordering kernels + this)"
+        if args.unfused:
+            # AO pieces to HBM, then 128-row tiles of the 5P x A pieces matrix x 6 products
+            executed = 2.0 * (-(-5 * P // 128) * 128) * n_pad * k_pad * 6
+            kname = "ao_tile_kernel<3,5> + tc_gemm_kernel<3,2> (unfused mixed form; whole step)"
+            t = None
+        achieved = executed / (ms * 1e-3) / 1e12
+        roofline = {"kernel": kname,
                     "bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
                     "frac": achieved / bf16, "peak_source": peak_src,
                     "traffic": t * P / 20352.0 if t else None,

@@ -42,8 +42,8 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
 }
 
 // TA: A is stored transposed (element (m, k) at A[k * lda + m]); its shared
-// tile is then kept k-major ([BK][BM + 4]).  Split K: CTA z of the grid
-// covers k in [z * k_split, (z + 1) * k_split) and writes C + z * c_split.
+// tile is then kept k-major ([BK][BM + 4]).  Split K (TA only): CTA z of the
+// grid covers k in [z * k_split, (z + 1) * k_split) and writes C + z * c_split.
 template <int NT, int VA, int VB, bool TA>
 __global__ void __launch_bounds__(256)
 dgemm_kernel(int64_t M, int64_t N, int64_t K, const double* __restrict__ A_, int64_t lda,
@@ -59,12 +59,17 @@ dgemm_kernel(int64_t M, int64_t N, int64_t K, const double* __restrict__ A_, int
   const int wm = warp & 3, wn = warp >> 2;
   const int g = lane >> 2, t = lane & 3;
   const int64_t n0 = (int64_t)blockIdx.x * BN;
-  const int64_t kz0 = (int64_t)blockIdx.z * k_split;
-  // an empty K range (last splits of a short K) still writes its zero slice
-  K = kz0 >= K ? 0 : ((K - kz0) < k_split ? (K - kz0) : k_split);
-  const double* __restrict__ A = A_ + (TA ? kz0 * lda : kz0);
-  const double* __restrict__ B = B_ + kz0 * ldb;
-  double* __restrict__ C = C_ + (int64_t)blockIdx.z * c_split;
+  const double* __restrict__ A = A_;
+  const double* __restrict__ B = B_;
+  double* __restrict__ C = C_;
+  if constexpr (TA) {   // split K (used with the transposed form only)
+    const int64_t kz0 = (int64_t)blockIdx.z * k_split;
+    // an empty K range (last splits of a short K) still writes its zero slice
+    K = kz0 >= K ? 0 : ((K - kz0) < k_split ? (K - kz0) : k_split);
+    A = A_ + kz0 * lda;
+    B = B_ + kz0 * ldb;
+    C = C_ + (int64_t)blockIdx.z * c_split;
+  }
   const int ktiles = (int)((K + BK - 1) / BK);
 
   for (int64_t mt = blockIdx.y; mt * BM < M; mt += gridDim.y) {
@@ -199,6 +204,7 @@ template <bool TA>
 cudaError_t run_any(int64_t M, int64_t N, int64_t K, const double* A, int64_t lda, const double* B, int64_t ldb,
                     double* C, int64_t ldc, int splits, cudaStream_t s) {
   if (M <= 0 || N <= 0) return cudaSuccess;
+  if (!TA && splits != 1) return cudaErrorInvalidValue;
   // pick the N tile (64 or 80 columns) that wastes fewer padded columns
   const int64_t w64 = ((N + 63) / 64) * 64 - N, w80 = ((N + 79) / 80) * 80 - N;
   if (w80 < w64) return run_nt<5, TA>(M, N, K, A, lda, B, ldb, C, ldc, splits, s);

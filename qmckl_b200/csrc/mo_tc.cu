@@ -178,9 +178,12 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
           const int cc = lane & 15;
           const int64_t row = m0 + row_base + rr;
           const int col = n0 + c0 + cc;
-          if (row < M && col < n_out)
-            out[row * ldo + col] =
-                stage[rr * 16 + ((cc + rr) & 15)] * (scales[(int)(row % comps)] * scales[kScaleCols + col]);
+          if (row < M && col < n_out) {
+            double v = stage[rr * 16 + ((cc + rr) & 15)];
+            // float16 operands carry power-of-two component and MO scales
+            if constexpr (PIECES == 2) v *= scales[(int)(row % comps)] * scales[kScaleCols + col];
+            out[row * ldo + col] = v;
+          }
         }
         __syncwarp();
       }
