@@ -32,9 +32,12 @@ extern "C" {
 qmckl_exit_code qmckl_b200_set_form(qmckl_context context, const int32_t form);
 qmckl_exit_code qmckl_b200_get_form(const qmckl_context context, int32_t* const form);
 
-/* Number of bfloat16 pieces in the mixed MO contraction: 2 (3 products,
- * hi*hi + hi*lo + lo*hi) or 3 (6 products, all pairs of total order <= 2).
- * Default 3. */
+/* Operand split of the fused mixed MO contraction: 3 (default) = three
+ * bfloat16 pieces, six products (all pairs of total order <= 2); 2 = two
+ * float16 pieces of values scaled by powers of two (per accumulator row from
+ * a bound of the row's AOs, per MO from its largest coefficient), three
+ * products.  The unfused organisation (qmckl_b200_set_mixed_kernel(ctx, 0))
+ * and qmckl_b200_mo_vgl_device_noalloc always use three bfloat16 pieces. */
 qmckl_exit_code qmckl_b200_set_split_terms(qmckl_context context, const int32_t pieces);
 
 /* Kernel organisation of the mixed form: 1 (default) runs the fused kernel
@@ -143,7 +146,7 @@ qmckl_exit_code qmckl_b200_batch_set_wait_limit(qmckl_b200_batch batch, const in
  * one fixed 32 MiB array inside the library, held by every GPU that loads the
  * library until the process exits.  The caller passes the coordinates and the
  * output buffer (device memory).
- *   - Limit: point_num * 5 rows of the AO matrix in 3 (or 2) bfloat16 pieces
+ *   - Limit: point_num * 5 rows of the AO matrix in 3 bfloat16 pieces
  *     of ao_num rounded up to 64 columns must fit in the 32 MiB; larger
  *     point_num is rejected with QMCKL_INVALID_ARG_2 and a message giving the
  *     largest point count for the basis (546 points for 2000 AOs, 3 pieces).

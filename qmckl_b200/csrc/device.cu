@@ -154,6 +154,8 @@ void build_envelopes(const Context* ctx, std::vector<float>& env, float& r0, flo
 }
 
 static std::atomic<int64_t> g_launches{0};
+constexpr int kSlices = 8;                 // slices of a host-getter evaluation (copy overlap)
+constexpr int64_t kSliceMinPoints = 2048;  // slicing only above 8 x this many points
 void count_launch(int n) { g_launches += n; }
 
 struct DevBuf {
@@ -193,6 +195,9 @@ struct DeviceState {
   DevBuf tc3_coef;
   // row-bound envelopes of the float16 operands (per basis)
   DevBuf env;
+  // host getters: slices of the evaluation copied out on a second stream
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t slice_ev[8] = {};
   uint64_t env_basis_version = ~0ull;
   float env_r0 = 0.f, env_inv_log2q = 0.f;
   int32_t split_pieces = 3;   // bfloat16 x 3; 2 = float16 x 2 with row / MO scales (split.cuh)
@@ -555,9 +560,14 @@ qmckl_exit_code prepare_mixed(qmckl_context context, DeviceState* ds) {
   return QMCKL_SUCCESS;
 }
 
+// Mixed-form MO VGL / value of P points into `out` (device).  With host_out
+// (the host getters), the fused path evaluates the points in slices and
+// copies each slice to the host on a second stream while the next slice is
+// computed; *copied then reports that host_out holds the result.
 qmckl_exit_code run_mo_mixed(qmckl_context context, DeviceState* ds, int64_t P, const double* coord,
-                             double* out, int comps) {
+                             double* out, int comps, double* host_out = nullptr, bool* copied = nullptr) {
   Context* ctx = ctx_of(context);
+  if (copied) *copied = false;
   qmckl_exit_code rc0 = prepare_mixed(context, ds);
   if (rc0 != QMCKL_SUCCESS) return rc0;
   if (ds->fused) {
@@ -580,11 +590,35 @@ qmckl_exit_code run_mo_mixed(qmckl_context context, DeviceState* ds, int64_t P, 
           lo[d] = std::min(lo[d], ctx->nucleus.coord[n + d * N] - 4.0);
           hi[d] = std::max(hi[d], ctx->nucleus.coord[n + d * N] + 4.0);
         }
-      QB_CUDA(point_order(coord, P, lo, hi, keys, counts, perm, ds->stream), "qmckl_b200_mo_mixed");
       fz::RowBound rb{(const double*)ds->nucl.p, (const float*)ds->env.p, (int)N, ds->env_r0, ds->env_inv_log2q};
-      QB_CUDA(tc_run_fused(ds->T, ds->tc, P, comps, coord, cutoff_of(ctx), ds->tc_coef.p, ds->krec.p, ds->rec_bytes,
-                           perm, rb, out, ds->stream),
-              "qmckl_b200_mo_mixed");
+      const int64_t M = ctx->mo_basis.mo_num;
+      const bool slices = host_out != nullptr && P >= 8 * kSliceMinPoints;
+      if (slices && ds->copy_stream == nullptr) {
+        QB_CUDA(cudaStreamCreateWithFlags(&ds->copy_stream, cudaStreamNonBlocking), "qmckl_b200_mo_mixed");
+        for (cudaEvent_t& ev : ds->slice_ev) QB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "qmckl_b200_mo_mixed");
+      }
+      const int64_t step = slices ? ((P + kSlices - 1) / kSlices + 24) / 25 * 25 : P;
+      int slice = 0;
+      for (int64_t a = 0; a < P; a += step, ++slice) {
+        const int64_t n = std::min(step, P - a);
+        double* o = out + a * comps * M;
+        QB_CUDA(point_order(coord + a, n, lo, hi, keys, counts, perm, ds->stream, P), "qmckl_b200_mo_mixed");
+        QB_CUDA(tc_run_fused(ds->T, ds->tc, n, comps, coord + a, cutoff_of(ctx), ds->tc_coef.p, ds->krec.p,
+                             ds->rec_bytes, perm, rb, o, ds->stream, P),
+                "qmckl_b200_mo_mixed");
+        if (slices) {
+          cudaEvent_t ev = ds->slice_ev[slice % kSlices];
+          QB_CUDA(cudaEventRecord(ev, ds->stream), "qmckl_b200_mo_mixed");
+          QB_CUDA(cudaStreamWaitEvent(ds->copy_stream, ev, 0), "qmckl_b200_mo_mixed");
+          QB_CUDA(cudaMemcpyAsync(host_out + a * comps * M, o, sizeof(double) * n * comps * M, cudaMemcpyDeviceToHost,
+                                  ds->copy_stream),
+                  "qmckl_get_mo_basis_mo_vgl");
+        }
+      }
+      if (slices) {
+        QB_CUDA(cudaStreamSynchronize(ds->copy_stream), "qmckl_get_mo_basis_mo_vgl");
+        if (copied) *copied = true;
+      }
       return QMCKL_SUCCESS;
     }
   }
@@ -656,6 +690,12 @@ void dev_detach(Context* ctx) {
                     &ds->ao_hessian, &ds->coef_rows, &ds->adj_coord, &ds->adj_buf, &ds->adj_part, &ds->adj_nucl,
                     &ds->tc3_coef, &ds->env})
     release(*b);
+  if (ds->copy_stream) {
+    cudaStreamSynchronize(ds->copy_stream);
+    cudaStreamDestroy(ds->copy_stream);
+    for (cudaEvent_t ev : ds->slice_ev)
+      if (ev) cudaEventDestroy(ev);
+  }
   if (ds->own_stream && ds->stream) cudaStreamDestroy(ds->stream);
   delete ds;
   ctx->extra = nullptr;
@@ -813,13 +853,14 @@ qmckl_exit_code dev_provide_mo_vgl(qmckl_context context, double* host_out) {
     return qmckl_failwith(context, QMCKL_NOT_PROVIDED, "qmckl_ao_basis", NULL);
   const int64_t P = ctx->point.num, A = ctx->ao_basis.ao_num, M = ctx->mo_basis.mo_num;
   const size_t bytes = sizeof(double) * 5 * M * P;
+  bool copied = false;   // set when the evaluation already copied the slices to host_out
   if (ctx->point.date > ctx->mo_basis.mo_vgl_date || ds->mo_vgl.cap < bytes) {
     rc = sync_inputs(context, ds, true);
     if (rc != QMCKL_SUCCESS) return rc;
     rc = ensure(context, ds->mo_vgl, bytes, "qmckl_provide_mo_basis_mo_vgl");
     if (rc != QMCKL_SUCCESS) return rc;
     if (use_mixed(ctx)) {
-      rc = run_mo_mixed(context, ds, P, (const double*)ds->coord.p, (double*)ds->mo_vgl.p, 5);
+      rc = run_mo_mixed(context, ds, P, (const double*)ds->coord.p, (double*)ds->mo_vgl.p, 5, host_out, &copied);
     } else {
       // FP64 form: the AO array is materialised (and cached) as in the reference
       rc = sync_coef(context, ds);
@@ -838,7 +879,7 @@ qmckl_exit_code dev_provide_mo_vgl(qmckl_context context, double* host_out) {
     if (rc != QMCKL_SUCCESS) return rc;
     ctx->mo_basis.mo_vgl_date = ctx->date;
   }
-  return copy_out(context, ds, host_out, ds->mo_vgl.p, bytes, "qmckl_get_mo_basis_mo_vgl");
+  return copy_out(context, ds, copied ? nullptr : host_out, ds->mo_vgl.p, bytes, "qmckl_get_mo_basis_mo_vgl");
 }
 
 qmckl_exit_code dev_provide_mo_value(qmckl_context context, double* host_out) {

@@ -38,7 +38,7 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
                 const double* __restrict__ coord, const double cutoff, const int n_out, const int n_tile,
                 const int kblocks, const uint8_t* __restrict__ krec, const int rec_bytes,
                 const int* __restrict__ perm, const double* __restrict__ scales, const RowBound rb,
-                double* __restrict__ out, int* __restrict__ err) {
+                double* __restrict__ out, int* __restrict__ err, const int64_t cstride) {
   constexpr int PTS = BM / COMPS;            // 25 points (VGL) or 128 (value)
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   // 1024-byte aligned base, kept as pointer arithmetic on the __shared__
@@ -75,7 +75,7 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
   for (int t = tid; t < 3 * PTS; t += kThreadsF) {
     const int d = t / PTS, i = t - d * PTS;
     const int64_t q = (p0 + i < P) ? (perm ? (int64_t)perm[p0 + i] : p0 + i) : -1;
-    pts[t] = q >= 0 ? coord[q + d * P] : 0.0;
+    pts[t] = q >= 0 ? coord[q + d * cstride] : 0.0;
     if (d == 0) pidx[i] = q;
     rexp[t] = PIECES == 2 ? kExpMin : 0;
   }
@@ -197,7 +197,7 @@ template <int PIECES, int COMPS>
 cudaError_t launch_fused(const DevTables& T, const CUtensorMap& tb, int64_t P, const double* coord, double cutoff,
                          int n_out, int n_tile, int n_tiles, int kblocks, const uint8_t* krec, int rec_bytes,
                          const int* perm, const double* scales, const RowBound& rb, double* out, int* err,
-                         cudaStream_t s) {
+                         int64_t cstride, cudaStream_t s) {
   constexpr int PTS = BM / COMPS;
   const size_t smem = fused_smem<PIECES, COMPS>(n_tile, rec_bytes);
   auto kern = fused_mo_kernel<PIECES, COMPS>;
@@ -205,7 +205,7 @@ cudaError_t launch_fused(const DevTables& T, const CUtensorMap& tb, int64_t P, c
   if (e != cudaSuccess) return e;
   dim3 grid((unsigned)((P + PTS - 1) / PTS), (unsigned)n_tiles);
   kern<<<grid, kThreadsF, smem, s>>>(T, tb, P, coord, cutoff, n_out, n_tile, kblocks, krec, rec_bytes, perm, scales,
-                                     rb, out, err);
+                                     rb, out, err, cstride);
   count_launch();
   return cudaGetLastError();
 }
@@ -232,8 +232,9 @@ cudaError_t tc_encode_coef_map(const TcPlan& plan, const void* d_coef, CUtensorM
 
 cudaError_t tc_launch_fused(const TcPlan& plan, int64_t point_num, int comps, const double* coord, double cutoff,
                             const CUtensorMap& tb, const void* krec, int rec_bytes, const int* perm, const void* d_coef,
-                            const RowBound& rb, double* out, int* err, cudaStream_t s) {
+                            const RowBound& rb, double* out, int* err, cudaStream_t s, int64_t cstride) {
   if (point_num <= 0) return cudaSuccess;
+  if (cstride < point_num) cstride = point_num;
   if (rec_bytes <= 0 || rec_bytes % 128 != 0) return cudaErrorInvalidValue;
   const DevTables T{};   // the fused kernel reads the records only
   const int kblocks = (int)((plan.ao_num + BK - 1) / BK);
@@ -242,18 +243,18 @@ cudaError_t tc_launch_fused(const TcPlan& plan, int64_t point_num, int comps, co
   const double* sc = tc_scales(plan, d_coef);
   if (plan.pieces == 3)
     return comps == 5 ? launch_fused<3, 5>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
-                                           rec_bytes, perm, sc, rb, out, err, s)
+                                           rec_bytes, perm, sc, rb, out, err, cstride, s)
                       : launch_fused<3, 1>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
-                                           rec_bytes, perm, sc, rb, out, err, s);
+                                           rec_bytes, perm, sc, rb, out, err, cstride, s);
   return comps == 5 ? launch_fused<2, 5>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
-                                         rec_bytes, perm, sc, rb, out, err, s)
+                                         rec_bytes, perm, sc, rb, out, err, cstride, s)
                     : launch_fused<2, 1>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
-                                         rec_bytes, perm, sc, rb, out, err, s);
+                                         rec_bytes, perm, sc, rb, out, err, cstride, s);
 }
 
 cudaError_t tc_run_fused(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps, const double* coord,
                          double cutoff, const void* d_coef, const void* krec, int rec_bytes, const int* perm,
-                         const RowBound& rb, double* out, cudaStream_t s) {
+                         const RowBound& rb, double* out, cudaStream_t s, int64_t cstride) {
   (void)T;
   if (point_num <= 0) return cudaSuccess;
   CUtensorMap tb;
@@ -261,7 +262,7 @@ cudaError_t tc_run_fused(const DevTables& T, const TcPlan& plan, int64_t point_n
   if (e != cudaSuccess) return e;
   int* err = fused_err_word();
   if (!err) return cudaErrorMemoryAllocation;
-  e = tc_launch_fused(plan, point_num, comps, coord, cutoff, tb, krec, rec_bytes, perm, d_coef, rb, out, err, s);
+  e = tc_launch_fused(plan, point_num, comps, coord, cutoff, tb, krec, rec_bytes, perm, d_coef, rb, out, err, s, cstride);
   if (e != cudaSuccess) return e;
   int h = 0;
   e = cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s);
@@ -296,14 +297,14 @@ __device__ __forceinline__ unsigned int spread5(unsigned int x) {   // 5 bits ->
   return x;
 }
 
-__global__ void point_keys_kernel(const double* __restrict__ coord, int64_t P, double3 origin, double inv_cell,
-                                  int* __restrict__ keys, unsigned int* __restrict__ counts) {
+__global__ void point_keys_kernel(const double* __restrict__ coord, int64_t P, int64_t cstride, double3 origin,
+                                  double inv_cell, int* __restrict__ keys, unsigned int* __restrict__ counts) {
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += (int64_t)gridDim.x * blockDim.x) {
     int c[3];
     const double o[3] = {origin.x, origin.y, origin.z};
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      const double v = floor((coord[p + d * P] - o[d]) * inv_cell);
+      const double v = floor((coord[p + d * cstride] - o[d]) * inv_cell);
       c[d] = (int)fmin(31.0, fmax(0.0, v));
     }
     const int key = (int)(spread5(c[0]) | (spread5(c[1]) << 1) | (spread5(c[2]) << 2));
@@ -345,7 +346,8 @@ __global__ void scatter_points_kernel(const int* __restrict__ keys, int64_t P, u
 }  // namespace
 
 cudaError_t point_order(const double* coord, int64_t point_num, const double* box_lo, const double* box_hi,
-                        int* keys, unsigned int* counts, int* perm, cudaStream_t s) {
+                        int* keys, unsigned int* counts, int* perm, cudaStream_t s, int64_t cstride) {
+  if (cstride < point_num) cstride = point_num;
   // 32 cells per axis over the box of the nuclei (cells at least 1 bohr wide)
   double ext = 0.0;
   for (int d = 0; d < 3; ++d) ext = std::max(ext, box_hi[d] - box_lo[d]);
@@ -355,7 +357,7 @@ cudaError_t point_order(const double* coord, int64_t point_num, const double* bo
   cudaError_t e = cudaMemsetAsync(counts, 0, sizeof(unsigned int) * kSortCells, s);
   if (e != cudaSuccess) return e;
   const int grid = (int)std::min<int64_t>((point_num + 255) / 256, 148 * 8);
-  point_keys_kernel<<<grid, 256, 0, s>>>(coord, point_num, origin, 1.0 / cell, keys, counts);
+  point_keys_kernel<<<grid, 256, 0, s>>>(coord, point_num, cstride, origin, 1.0 / cell, keys, counts);
   scan_cells_kernel<<<1, 1024, 0, s>>>(counts);
   scatter_points_kernel<<<grid, 256, 0, s>>>(keys, point_num, counts, perm);
   count_launch(3);

@@ -64,19 +64,22 @@ cudaError_t tc_run(const DevTables& T, const TcPlan& plan, int64_t point_num, in
 // rb: the per-row scale bounds of 2-piece float16 operands (fused_common.cuh).
 cudaError_t tc_run_fused(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps, const double* coord,
                          double cutoff, const void* d_coef, const void* krec, int rec_bytes, const int* perm,
-                         const fz::RowBound& rb, double* out, cudaStream_t s);
+                         const fz::RowBound& rb, double* out, cudaStream_t s, int64_t cstride = -1);
 // TMA map of a plan's coefficient pieces (box: 64 AOs x n_tile MOs x 1 piece,
 // 128B swizzle) and a launch of the fused kernel that does not wait for it
 // (err: device error word, left for the caller to check).
 cudaError_t tc_encode_coef_map(const TcPlan& plan, const void* d_coef, CUtensorMap* map);
 cudaError_t tc_launch_fused(const TcPlan& plan, int64_t point_num, int comps, const double* coord, double cutoff,
                             const CUtensorMap& map, const void* krec, int rec_bytes, const int* perm, const void* d_coef,
-                            const fz::RowBound& rb, double* out, int* err, cudaStream_t s);
+                            const fz::RowBound& rb, double* out, int* err, cudaStream_t s, int64_t cstride = -1);
 // Spatial order of points (32^3 cells over [box_lo, box_hi], Morton order) by
 // a counting sort: perm[P]; keys[P] and counts[kSortCells + 1] are scratch.
+// cstride: distance between the x, y and z blocks of coord (default
+// point_num; larger for a slice of a bigger [3][N] array).  The fused
+// kernels take the same stride.
 constexpr int kSortCells = 1 << 15;
 cudaError_t point_order(const double* coord, int64_t point_num, const double* box_lo, const double* box_hi,
-                        int* keys, unsigned int* counts, int* perm, cudaStream_t s);
+                        int* keys, unsigned int* counts, int* perm, cudaStream_t s, int64_t cstride = -1);
 // dynamic shared memory of the fused kernel (must stay <= 227 KB)
 size_t tc_fused_smem(const TcPlan& plan, int comps, int rec_bytes);
 

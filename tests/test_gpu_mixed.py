@@ -109,3 +109,22 @@ def test_auto_form_follows_precision(chbrclf):
     assert 1e-13 < max(comp_error(m2, ref)) < 1e-4
     pq.context_destroy(c1)
     pq.context_destroy(c2)
+
+
+def test_host_getter_slices_match_device_entry():
+    """The host getter evaluates large point sets in slices whose copies overlap the next slice's
+    kernel; its result equals the device entry point's, to the last bit."""
+    import torch
+    d = gen.config(1, walk_num=64)
+    P = d["elec_coord"].shape[0] * d["elec_coord"].shape[1]
+    M = d["mo_num"]
+    ctx = make_context(d, form=pq.FORM_MIXED)
+    host = pq.get_mo_basis_mo_vgl(ctx, P * 5 * M)
+    dc = torch.tensor(np.ascontiguousarray(gen.points(d).T), dtype=torch.float64, device="cuda")
+    out = torch.empty(P * 5 * M, dtype=torch.float64, device="cuda")
+    pq.b200_mo_vgl_device(ctx, P, dc.data_ptr(), out.data_ptr())
+    pq.b200_synchronize(ctx)
+    assert np.array_equal(host, out.cpu().numpy())
+    again = pq.get_mo_basis_mo_vgl(ctx, P * 5 * M)   # cached: copied from the device array
+    assert np.array_equal(host, again)
+    pq.context_destroy(ctx)
