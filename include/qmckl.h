@@ -174,6 +174,20 @@ qmckl_exit_code qmckl_get_ao_basis_ao_value_inplace(qmckl_context context, doubl
  * coordinates (org/qmckl_ao.org:9400-9404, 9590-9720). */
 qmckl_exit_code qmckl_get_ao_basis_ao_hessian(qmckl_context context, double* const ao_hessian, const int64_t size_max);
 
+/* Orbital forces: derivatives with respect to the nuclear coordinates
+ * (org/qmckl_forces.org).  Layouts:
+ *   forces_ao_value [nucl][point][3][ao]    (5129-5160; 0 for AOs of other nuclei)
+ *   forces_mo_value [nucl][point][3][mo]    (5475-5575)
+ *   forces_mo_g     [nucl][3][point][3][mo] (5919-6000): d/dR_{a,n} of the MO gradient
+ *   forces_mo_l     [nucl][3][point][mo]    (6499-6530): d/dR_{a,n} of the MO Laplacian */
+qmckl_exit_code qmckl_get_forces_ao_value(qmckl_context context, double* const forces_ao_value, const int64_t size_max);
+qmckl_exit_code qmckl_get_forces_mo_value(qmckl_context context, double* const forces_mo_value, const int64_t size_max);
+qmckl_exit_code qmckl_get_forces_mo_value_inplace(qmckl_context context, double* const forces_mo_value,
+                                                  const int64_t size_max);
+qmckl_exit_code qmckl_get_forces_mo_g(qmckl_context context, double* const forces_mo_g, const int64_t size_max);
+qmckl_exit_code qmckl_get_forces_mo_g_inplace(qmckl_context context, double* const forces_mo_g, const int64_t size_max);
+qmckl_exit_code qmckl_get_forces_mo_l(qmckl_context context, double* const forces_mo_l, const int64_t size_max);
+
 /* ---- MO basis: org/qmckl_mo.org:192-1747, 3479 ---- */
 qmckl_exit_code qmckl_set_mo_basis_mo_num(qmckl_context context, const int64_t mo_num);
 qmckl_exit_code qmckl_set_mo_basis_coefficient(qmckl_context context, const double* coefficient, const int64_t size_max);

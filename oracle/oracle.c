@@ -832,3 +832,50 @@ int oracle_mo_vgl_adjoint(const oracle_basis* b, int32_t precision, int64_t poin
   free(fv); free(fg); free(fl); free(av); free(ah);
   return 0;
 }
+
+/* Orbital forces as full tensors (derivatives with respect to the nuclear
+ * coordinates), the reference's getters qmckl_get_forces_ao_value /
+ * _mo_value / _mo_g / _mo_l (org/qmckl_forces.org:5129-5160, 5300-5345,
+ * 5688-5800, 6132-6337, 6648-6772):
+ *   forces_ao_value[a][p][n][k] = -ao_vgl[p][1+n][k]    (k on nucleus a, else 0)
+ *   forces_mo_value[a][p][n][i] = -sum_{k on a} C[i][k] ao_vgl[p][1+n][k]
+ *   forces_mo_g[a][n][p][m][i]  = -sum_{k on a} C[i][k] ao_hessian[n][p][m][k]
+ *   forces_mo_l[a][n][p][i]     = -sum_{k on a} C[i][k] ao_hessian[n][p][3][k]
+ * coefficient [mo][ao]; any output may be NULL. */
+int oracle_forces(const oracle_basis* b, int32_t precision, int64_t point_num, const double* coord,
+                  const double* nucl_coord, int64_t mo_num, const double* coefficient, double* fao,
+                  double* fmv, double* fmg, double* fml) {
+  const int64_t N = b->nucl_num, A = b->ao_num, M = mo_num, P = point_num;
+  double* av = (double*)malloc(sizeof(double) * 5 * A * P);
+  double* ah = (double*)malloc(sizeof(double) * 12 * A * P);
+  oracle_ao_vgl_doc(b, precision, P, coord, nucl_coord, av);
+  oracle_ao_hessian_doc(b, precision, P, coord, nucl_coord, ah);
+  if (fao) memset(fao, 0, sizeof(double) * N * P * 3 * A);
+  if (fmv) memset(fmv, 0, sizeof(double) * N * P * 3 * M);
+  if (fmg) memset(fmg, 0, sizeof(double) * N * 3 * P * 3 * M);
+  if (fml) memset(fml, 0, sizeof(double) * N * 3 * P * M);
+  for (int64_t a = 0; a < N; ++a) {
+    const int64_t s0 = b->nucleus_index[a], s1 = s0 + b->nucleus_shell_num[a];
+    if (s1 <= s0) continue;
+    const int64_t k0 = b->ao_index[s0];
+    const int64_t k1 = b->ao_index[s1 - 1] + (lstart(b->shell_ang_mom[s1 - 1] + 1) - lstart(b->shell_ang_mom[s1 - 1]));
+    for (int64_t p = 0; p < P; ++p)
+      for (int n = 0; n < 3; ++n) {
+        const double* g = av + (p * 5 + 1 + n) * A;
+        const double* h = ah + (n * P + p) * 4 * A;
+        for (int64_t k = k0; k < k1; ++k) {
+          if (fao) fao[((a * P + p) * 3 + n) * A + k] = -g[k];
+          for (int64_t i = 0; i < M; ++i) {
+            const double c = coefficient[i * A + k];
+            if (fmv) fmv[((a * P + p) * 3 + n) * M + i] -= c * g[k];
+            if (fmg)
+              for (int m = 0; m < 3; ++m) fmg[(((a * 3 + n) * P + p) * 3 + m) * M + i] -= c * h[m * A + k];
+            if (fml) fml[((a * 3 + n) * P + p) * M + i] -= c * h[3 * A + k];
+          }
+        }
+      }
+  }
+  free(av);
+  free(ah);
+  return 0;
+}

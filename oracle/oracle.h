@@ -91,6 +91,13 @@ int oracle_mo_vgl_adjoint(const oracle_basis* b, int32_t precision, int64_t poin
                           const double* nucl_coord, int64_t mo_num, const double* coefficient,
                           const double* weight, double* grad_coef, double* grad_nucl, double* grad_coord);
 
+/* Orbital forces, full tensors (the reference's forces getters):
+ *   fao [nucl][point][3][ao], fmv [nucl][point][3][mo],
+ *   fmg [nucl][3][point][3][mo], fml [nucl][3][point][mo]; NULL to skip. */
+int oracle_forces(const oracle_basis* b, int32_t precision, int64_t point_num, const double* coord,
+                  const double* nucl_coord, int64_t mo_num, const double* coefficient, double* fao,
+                  double* fmv, double* fmg, double* fml);
+
 #ifdef __cplusplus
 }
 #endif

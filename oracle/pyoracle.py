@@ -44,6 +44,8 @@ def lib():
             getattr(L, f).argtypes = [C.c_void_p, C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
         L.oracle_mo_vgl_adjoint.argtypes = [C.c_void_p, C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64,
                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oracle_forces.argtypes = [C.c_void_p, C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         for f in ("oracle_mo_vgl", "oracle_mo_value"):
             getattr(L, f).argtypes = [C.c_int64, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]
         _lib = L
@@ -173,6 +175,21 @@ def mo_vgl_adjoint(basis, coord, nucl_coord, coefficient, weight, precision=53):
     gr = np.empty((3, P))
     lib().oracle_mo_vgl_adjoint(basis.h, precision, P, _p(c), _p(n), M, _p(coef), _p(w), _p(gc), _p(gn), _p(gr))
     return gc, gn, np.ascontiguousarray(gr.T)
+
+
+def forces(basis, coord, nucl_coord, coefficient, precision=53):
+    """(forces_ao_value [N][P][3][A], forces_mo_value [N][P][3][M], forces_mo_g [N][3][P][3][M],
+    forces_mo_l [N][3][P][M])."""
+    c, n = _coords(coord, nucl_coord)
+    P = c.shape[1]
+    coef = np.ascontiguousarray(coefficient, dtype=np.float64)
+    M, A, N = coef.shape[0], basis.ao_num, basis.nucl_num
+    fao = np.empty((N, P, 3, A))
+    fmv = np.empty((N, P, 3, M))
+    fmg = np.empty((N, 3, P, 3, M))
+    fml = np.empty((N, 3, P, M))
+    lib().oracle_forces(basis.h, precision, P, _p(c), _p(n), M, _p(coef), _p(fao), _p(fmv), _p(fmg), _p(fml))
+    return fao, fmv, fmg, fml
 
 
 def cutoff(precision=53):

@@ -288,7 +288,76 @@ cudaError_t launch_deriv(const DevTables& T, int64_t point_num, const double* co
   return cudaGetLastError();
 }
 
+// Orbital forces (derivatives with respect to the nuclear coordinates; the
+// reference's qmckl_get_forces_* getters, org/qmckl_forces.org:5129-6880).
+// Only the AOs of nucleus a depend on R_a, so each force is a contraction
+// over that nucleus's AO range [nuc_ao[a].x, nuc_ao[a].y):
+//   out[(a * R + r) * M + i] = -sum_k X_r[k] * Ct[k][i]
+// with the row r and its source row X_r:
+//   MODE 0 forces_mo_value [a][p][n][i]: R = 3P, r = 3p + n,         X_r = ao_vgl[p][1+n]
+//   MODE 1 forces_mo_g [a][n][p][m][i]:  R = 9P, r = 3(nP + p) + m,  X_r = ao_hessian[n][p][m]
+//   MODE 2 forces_mo_l [a][n][p][i]:     R = 3P, r = nP + p,         X_r = ao_hessian[n][p][3]
+// One thread per output element, MOs fastest (coalesced Ct reads and stores).
+template <int MODE>
+__global__ void forces_mo_kernel(const int64_t P, const int64_t A, const int64_t M, const int N,
+                                 const int2* __restrict__ nuc_ao, const double* __restrict__ X,
+                                 const double* __restrict__ Ct, double* __restrict__ out) {
+  const int64_t R = (MODE == 1 ? 9 : 3) * P;
+  const int64_t total = (int64_t)N * R * M;
+  for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < total; u += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = u % M;
+    const int64_t ar = u / M;
+    const int a = (int)(ar / R);
+    const int64_t r = ar - (int64_t)a * R;
+    const double* xr;
+    if (MODE == 0) {
+      const int64_t p = r / 3, n = r - 3 * p;
+      xr = X + (p * 5 + 1 + n) * A;
+    } else if (MODE == 1) {
+      const int64_t np = r / 3, m = r - 3 * np;
+      xr = X + (np * 4 + m) * A;
+    } else {
+      xr = X + (r * 4 + 3) * A;
+    }
+    const int2 kr = nuc_ao[a];
+    double acc = 0.0;
+    for (int k = kr.x; k < kr.y; ++k) acc -= Ct[(int64_t)k * M + i] * xr[k];
+    out[u] = acc;
+  }
+}
+
+// forces_ao_value[a][p][n][k] = -ao_vgl[p][1+n][k] for the AOs of nucleus a, 0 elsewhere
+__global__ void forces_ao_kernel(const int64_t P, const int64_t A, const int N, const int2* __restrict__ nuc_ao,
+                                 const double* __restrict__ X, double* __restrict__ out) {
+  const int64_t total = (int64_t)N * P * 3 * A;
+  for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < total; u += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = u % A;
+    const int64_t apn = u / A;
+    const int64_t n = apn % 3, ap = apn / 3;
+    const int64_t p = ap % P;
+    const int a = (int)(ap / P);
+    const int2 kr = nuc_ao[a];
+    out[u] = (k >= kr.x && k < kr.y) ? -X[(p * 5 + 1 + n) * A + k] : 0.0;
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_forces(int which, int64_t P, int64_t A, int64_t M, int N, const int2* nuc_ao, const double* X,
+                          const double* Ct, double* out, cudaStream_t s) {
+  if (P <= 0 || N <= 0) return cudaSuccess;
+  const int64_t total = which == 3 ? (int64_t)N * P * 3 * A : (int64_t)N * (which == 1 ? 9 : 3) * P * M;
+  const int grid = (int)std::min<int64_t>((total + 255) / 256, 148 * 16);
+  switch (which) {
+    case 0: forces_mo_kernel<0><<<grid, 256, 0, s>>>(P, A, M, N, nuc_ao, X, Ct, out); break;
+    case 1: forces_mo_kernel<1><<<grid, 256, 0, s>>>(P, A, M, N, nuc_ao, X, Ct, out); break;
+    case 2: forces_mo_kernel<2><<<grid, 256, 0, s>>>(P, A, M, N, nuc_ao, X, Ct, out); break;
+    case 3: forces_ao_kernel<<<grid, 256, 0, s>>>(P, A, N, nuc_ao, X, out); break;
+    default: return cudaErrorInvalidValue;
+  }
+  count_launch();
+  return cudaGetLastError();
+}
 
 cudaError_t launch_ao_hessian(const DevTables& T, int64_t point_num, const double* coord, double cutoff, bool mixed,
                               double* ao_hessian, cudaStream_t s) {

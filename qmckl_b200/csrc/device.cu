@@ -195,6 +195,9 @@ struct DeviceState {
   DevBuf tc3_coef;
   // row-bound envelopes of the float16 operands (per basis)
   DevBuf env;
+  // orbital forces: AO range of each nucleus and the output buffer
+  DevBuf nuc_ao, forces;
+  uint64_t nuc_ao_version = ~0ull;
   // host getters: slices of the evaluation copied out on a second stream
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t slice_ev[8] = {};
@@ -688,7 +691,7 @@ void dev_detach(Context* ctx) {
   for (DevBuf* b : {&ds->tables, &ds->nucl, &ds->coord, &ds->prim_vgl, &ds->shell_vgl, &ds->ao_vgl, &ds->ao_value,
                     &ds->mo_vgl, &ds->mo_value, &ds->coef_t, &ds->tc_coef, &ds->tc_a, &ds->krec, &ds->order,
                     &ds->ao_hessian, &ds->coef_rows, &ds->adj_coord, &ds->adj_buf, &ds->adj_part, &ds->adj_nucl,
-                    &ds->tc3_coef, &ds->env})
+                    &ds->tc3_coef, &ds->env, &ds->nuc_ao, &ds->forces})
     release(*b);
   if (ds->copy_stream) {
     cudaStreamSynchronize(ds->copy_stream);
@@ -840,6 +843,52 @@ qmckl_exit_code dev_provide_ao_hessian(qmckl_context context, double* host_out) 
     ctx->ao_basis.ao_hessian_date = ctx->date;
   }
   return copy_out(context, ds, host_out, ds->ao_hessian.p, bytes, "qmckl_get_ao_basis_ao_hessian");
+}
+
+// Orbital forces (org/qmckl_forces.org:5129-6880): which = 0 forces_mo_value,
+// 1 forces_mo_g, 2 forces_mo_l, 3 forces_ao_value, recomputed on every call
+// from the current ao_vgl / ao_hessian of the context's points.
+qmckl_exit_code dev_provide_forces(qmckl_context context, int which, double* host_out) {
+  static const char* const names[4] = {"qmckl_get_forces_mo_value", "qmckl_get_forces_mo_g",
+                                       "qmckl_get_forces_mo_l", "qmckl_get_forces_ao_value"};
+  const char* fname = names[which];
+  qmckl_exit_code rc = attach_all(context);
+  if (rc != QMCKL_SUCCESS) return rc;
+  Context* ctx = ctx_of(context);
+  DeviceState* ds = state(context);
+  const int64_t P = ctx->point.num, A = ctx->ao_basis.ao_num, N = ctx->nucleus.num;
+  const int64_t M = which == 3 ? 0 : ctx->mo_basis.mo_num;
+  rc = (which == 1 || which == 2) ? dev_provide_ao_hessian(context, nullptr) : dev_provide_ao_vgl(context, nullptr);
+  if (rc != QMCKL_SUCCESS) return rc;
+  if (which != 3) {
+    rc = sync_coef(context, ds);
+    if (rc != QMCKL_SUCCESS) return rc;
+  }
+  if (ds->nuc_ao_version != ctx->ao_basis.basis_version || !ds->nuc_ao.p) {
+    const AoBasisRec& B = ctx->ao_basis;
+    std::vector<int2> r((size_t)std::max<int64_t>(N, 1), make_int2(0, 0));
+    for (int64_t n = 0; n < N; ++n) {
+      const int64_t s0 = B.nucleus_index[n], s1 = s0 + B.nucleus_shell_num[n];
+      if (s1 > s0) {
+        const int l = B.shell_ang_mom[s1 - 1];
+        r[n] = make_int2((int)B.d.ao_index[s0], (int)(B.d.ao_index[s1 - 1] + (l + 1) * (l + 2) / 2));
+      }
+    }
+    rc = ensure(context, ds->nuc_ao, sizeof(int2) * r.size(), fname);
+    if (rc != QMCKL_SUCCESS) return rc;
+    QB_CUDA(cudaMemcpyAsync(ds->nuc_ao.p, r.data(), sizeof(int2) * r.size(), cudaMemcpyHostToDevice, ds->stream), fname);
+    QB_CUDA(cudaStreamSynchronize(ds->stream), fname);
+    ds->nuc_ao_version = ctx->ao_basis.basis_version;
+  }
+  const int64_t count = which == 3 ? N * P * 3 * A : N * (which == 1 ? 9 : 3) * P * M;
+  const size_t bytes = sizeof(double) * (size_t)count;
+  rc = ensure(context, ds->forces, bytes, fname);
+  if (rc != QMCKL_SUCCESS) return rc;
+  const double* X = (which == 1 || which == 2) ? (const double*)ds->ao_hessian.p : (const double*)ds->ao_vgl.p;
+  QB_CUDA(launch_forces(which, P, A, M, (int)N, (const int2*)ds->nuc_ao.p, X, (const double*)ds->coef_t.p,
+                        (double*)ds->forces.p, ds->stream),
+          fname);
+  return copy_out(context, ds, host_out, ds->forces.p, bytes, fname);
 }
 
 qmckl_exit_code dev_provide_mo_vgl(qmckl_context context, double* host_out) {
@@ -1048,6 +1097,57 @@ qmckl_exit_code qmckl_b200_mo_vgl_device(qmckl_context context, const int64_t po
 qmckl_exit_code qmckl_b200_mo_value_device(qmckl_context context, const int64_t point_num, const double* d_coord,
                                            double* d_mo_value) {
   return mo_device(context, "qmckl_b200_mo_value_device", point_num, d_coord, d_mo_value, 1);
+}
+
+// ---- orbital forces (org/qmckl_forces.org:5129-5160, 5475-5575, 5919-6000, 6499-6530)
+
+static qmckl_exit_code forces_getter(qmckl_context context, int which, double* out, int64_t size_max, bool need_mo,
+                                     int64_t per_point_nucl) {
+  static const char* const names[4] = {"qmckl_get_forces_mo_value", "qmckl_get_forces_mo_g",
+                                       "qmckl_get_forces_mo_l", "qmckl_get_forces_ao_value"};
+  if (qmckl_context_check(context) == QMCKL_NULL_CONTEXT) return QMCKL_NULL_CONTEXT;
+  Context* ctx = ctx_of(context);
+  if (!ctx->ao_basis.provided) return qmckl_failwith(context, QMCKL_NOT_PROVIDED, names[which], "AO basis not provided");
+  if (need_mo && !ctx->mo_basis.provided)
+    return qmckl_failwith(context, QMCKL_NOT_PROVIDED, names[which], "MO basis not provided");
+  const int64_t sze = per_point_nucl * ctx->point.num * ctx->nucleus.num;
+  if (size_max < sze)
+    return qmckl_failwith(context, QMCKL_INVALID_ARG_3, names[which],
+                          which == 3 ? "Array too small. Expected walk_num*nucl_num*point_num*3" : "input array too small");
+  if (out == nullptr) return qmckl_failwith(context, QMCKL_INVALID_ARG_2, names[which], "NULL pointer");
+  return dev_provide_forces(context, which, out);
+}
+
+qmckl_exit_code qmckl_get_forces_ao_value(qmckl_context context, double* const forces_ao_value,
+                                          const int64_t size_max) {
+  if (qmckl_context_check(context) == QMCKL_NULL_CONTEXT) return QMCKL_NULL_CONTEXT;
+  return forces_getter(context, 3, forces_ao_value, size_max, false, 3 * ctx_of(context)->ao_basis.ao_num);
+}
+
+qmckl_exit_code qmckl_get_forces_mo_value(qmckl_context context, double* const forces_mo_value,
+                                          const int64_t size_max) {
+  if (qmckl_context_check(context) == QMCKL_NULL_CONTEXT) return QMCKL_NULL_CONTEXT;
+  return forces_getter(context, 0, forces_mo_value, size_max, true, 3 * ctx_of(context)->mo_basis.mo_num);
+}
+
+qmckl_exit_code qmckl_get_forces_mo_value_inplace(qmckl_context context, double* const forces_mo_value,
+                                                  const int64_t size_max) {
+  return qmckl_get_forces_mo_value(context, forces_mo_value, size_max);
+}
+
+qmckl_exit_code qmckl_get_forces_mo_g(qmckl_context context, double* const forces_mo_g, const int64_t size_max) {
+  if (qmckl_context_check(context) == QMCKL_NULL_CONTEXT) return QMCKL_NULL_CONTEXT;
+  return forces_getter(context, 1, forces_mo_g, size_max, true, 9 * ctx_of(context)->mo_basis.mo_num);
+}
+
+qmckl_exit_code qmckl_get_forces_mo_g_inplace(qmckl_context context, double* const forces_mo_g,
+                                              const int64_t size_max) {
+  return qmckl_get_forces_mo_g(context, forces_mo_g, size_max);
+}
+
+qmckl_exit_code qmckl_get_forces_mo_l(qmckl_context context, double* const forces_mo_l, const int64_t size_max) {
+  if (qmckl_context_check(context) == QMCKL_NULL_CONTEXT) return QMCKL_NULL_CONTEXT;
+  return forces_getter(context, 2, forces_mo_l, size_max, true, 3 * ctx_of(context)->mo_basis.mo_num);
 }
 
 qmckl_exit_code qmckl_b200_ao_hessian_device(qmckl_context context, const int64_t point_num, const double* d_coord,

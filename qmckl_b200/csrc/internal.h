@@ -132,6 +132,7 @@ qmckl_exit_code dev_provide_shell_vgl(qmckl_context context, double* host_out);
 qmckl_exit_code dev_provide_ao_vgl(qmckl_context context, double* host_out);
 qmckl_exit_code dev_provide_ao_value(qmckl_context context, double* host_out);
 qmckl_exit_code dev_provide_ao_hessian(qmckl_context context, double* host_out);
+qmckl_exit_code dev_provide_forces(qmckl_context context, int which, double* host_out);
 qmckl_exit_code dev_provide_mo_vgl(qmckl_context context, double* host_out);
 qmckl_exit_code dev_provide_mo_value(qmckl_context context, double* host_out);
 qmckl_exit_code dev_invalidate_mo(qmckl_context context);

@@ -83,6 +83,12 @@ cudaError_t launch_add_transposed(const double* part, int splits, int64_t M, int
 // [3][cstride].  `mixed` selects FP32 exponentials where a r^2 <= 30.
 cudaError_t launch_ao_hessian(const DevTables& T, int64_t point_num, const double* coord, double cutoff, bool mixed,
                               double* ao_hessian, cudaStream_t s);
+// Orbital forces (adjoint.cu): which = 0 forces_mo_value, 1 forces_mo_g,
+// 2 forces_mo_l (from X = ao_vgl for 0, ao_hessian for 1 and 2, and
+// Ct = coefficient_t [ao][mo]), 3 forces_ao_value (from X = ao_vgl).
+// nuc_ao[a] = AO range of nucleus a.
+cudaError_t launch_forces(int which, int64_t P, int64_t A, int64_t M, int N, const int2* nuc_ao, const double* X,
+                          const double* Ct, double* out, cudaStream_t s);
 cudaError_t launch_mo_adjoint_nuclear(const DevTables& T, int64_t point_num, const double* coord, int64_t cstride,
                                       double cutoff, bool mixed, const double* G, double* grad_nucl,
                                       double* grad_coord, int64_t gstride, cudaStream_t s);

@@ -307,6 +307,12 @@ get_ao_basis_ao_vgl_inplace = _array_getter("qmckl_get_ao_basis_ao_vgl_inplace")
 get_ao_basis_ao_value = _array_getter("qmckl_get_ao_basis_ao_value")
 get_ao_basis_ao_value_inplace = _array_getter("qmckl_get_ao_basis_ao_value_inplace")
 get_ao_basis_ao_hessian = _array_getter("qmckl_get_ao_basis_ao_hessian")
+get_forces_ao_value = _array_getter("qmckl_get_forces_ao_value")
+get_forces_mo_value = _array_getter("qmckl_get_forces_mo_value")
+get_forces_mo_value_inplace = _array_getter("qmckl_get_forces_mo_value_inplace")
+get_forces_mo_g = _array_getter("qmckl_get_forces_mo_g")
+get_forces_mo_g_inplace = _array_getter("qmckl_get_forces_mo_g_inplace")
+get_forces_mo_l = _array_getter("qmckl_get_forces_mo_l")
 
 # ------------------------------------------------------------- MO basis
 

@@ -85,3 +85,47 @@ def test_adjoint_matches_finite_difference():
     av = O.ao_vgl(basis, pts, nucl, path="doc")
     ref = np.einsum("pci,pck->ik", w, av)
     assert np.abs(gc - ref).max() < 1e-12 * np.abs(ref).max()
+
+
+def test_orbital_forces_match_nuclear_finite_differences(chbrclf, basis):
+    """The reference's forces tests (org/qmckl_forces.org:5800-5917, 6370-6480, 6780-6880):
+    forces_mo_value / _mo_g / _mo_l against a 9-point finite difference of mo_value /
+    the MO gradient rows / the MO Laplacian rows over the nuclear coordinates
+    (step 1e-5, |diff| < 1e-9); forces_ao_value is minus the AO gradient on each nucleus."""
+    pts = chbrclf["elec_coord"][0][:12]
+    nucl = np.array(chbrclf["nucl_coord"], dtype=np.float64)
+    coef = chbrclf["mo_coef"]
+    N, P, M = nucl.shape[1], pts.shape[0], coef.shape[0]
+    fao, fmv, fmg, fml = O.forces(basis, pts, nucl, coef)
+    dx = 1.0e-5
+    fd_v = np.zeros((N, P, 3, M))
+    fd_g = np.zeros((N, 3, P, 3, M))
+    fd_l = np.zeros((N, 3, P, M))
+    for a in range(N):
+        for k in range(3):
+            for m in range(-4, 5):
+                if m == 0:
+                    continue
+                t = nucl.copy()
+                t[k, a] += m * dx
+                mo = O.mo_vgl(coef, O.ao_vgl(basis, pts, t, path="doc"))     # [P][5][M]
+                w = STENCIL[m + 4] / dx
+                fd_v[a, :, k, :] += w * mo[:, 0, :]
+                fd_g[a, k] += w * mo[:, 1:4, :]
+                fd_l[a, k] += w * mo[:, 4, :]
+    assert np.abs(fd_v - fmv).max() < 1e-9
+    assert np.abs(fd_g - fmg).max() < 1e-9
+    assert np.abs(fd_l - fml).max() < 1e-9
+    av = O.ao_vgl(basis, pts, nucl, path="doc")
+    for a in range(N):
+        s0, ns = int(chbrclf["nucleus_index"][a]), int(chbrclf["nucleus_shell_num"][a])
+        mask = np.zeros(basis.ao_num, bool)
+        k = 0
+        for s in range(chbrclf["shell_ang_mom"].size):
+            l = int(chbrclf["shell_ang_mom"][s])
+            nk = (l + 1) * (l + 2) // 2
+            if s0 <= s < s0 + ns:
+                mask[k:k + nk] = True
+            k += nk
+        assert np.array_equal(fao[a][:, :, mask], -av[:, 1:4, mask])
+        assert not fao[a][:, :, ~mask].any()
