@@ -30,6 +30,7 @@
 //                 device atomic per nucleus and CTA at the end); the sum over
 //                 all AOs gives dL/dr of the point.
 #include <algorithm>
+#include <type_traits>
 
 #include "kernels.cuh"
 
@@ -46,11 +47,12 @@ struct DerivSmem {
 };
 
 // x^a and its first three derivatives (Leibniz, one factor x at a time)
-__device__ __forceinline__ void pow_derivs(double x, int a, double (&q)[4]) {
-  q[0] = 1.0; q[1] = 0.0; q[2] = 0.0; q[3] = 0.0;
+template <typename F>
+__device__ __forceinline__ void pow_derivs(F x, int a, F (&q)[4]) {
+  q[0] = F(1); q[1] = F(0); q[2] = F(0); q[3] = F(0);
   for (int i = 0; i < a; ++i) {
-    q[3] = q[3] * x + 3.0 * q[2];
-    q[2] = q[2] * x + 2.0 * q[1];
+    q[3] = q[3] * x + F(3) * q[2];
+    q[2] = q[2] * x + F(2) * q[1];
     q[1] = q[1] * x + q[0];
     q[0] = q[0] * x;
   }
@@ -101,44 +103,45 @@ __device__ __forceinline__ void stage_deriv(const DevTables& T, DerivSmem& sm, c
 }
 
 // Hessian H[d][e] and gradient of the Laplacian T[d] of one AO (times its
-// factor f), plus its gradient g[d].
-__device__ __forceinline__ void ao_derivs(int code, double f, const double (&v)[3], double s, const double (&R)[4],
-                                          double (&g)[3], double (&H)[3][3], double (&Tl)[3]) {
+// factor f), plus its gradient g[d], in arithmetic F.  The radial
+// combinations that cancel near their zeros, lap R = 4 s R2 + 6 R1 and
+// k3 = 20 R2 + 8 s R3, come in formed in FP64.
+template <typename F>
+__device__ __forceinline__ void ao_derivs(int code, F f, const F (&v)[3], const F (&R)[3], F lapR, F k3,
+                                          F (&g)[3], F (&H)[3][3], F (&Tl)[3]) {
   const int ax = code & 15, by = (code >> 4) & 15, cz = (code >> 8) & 15, l = (code >> 12) & 15;
-  double X[4], Y[4], Z[4];
-  pow_derivs(v[0], ax, X);
-  pow_derivs(v[1], by, Y);
-  pow_derivs(v[2], cz, Z);
-  const double P = X[0] * Y[0] * Z[0] + (l >= 1 ? kShiftD : 0.0);
-  const double Pd[3] = {X[1] * Y[0] * Z[0], X[0] * Y[1] * Z[0], X[0] * Y[0] * Z[1]};
-  double Pdd[3][3];
+  F X[4], Y[4], Z[4];
+  pow_derivs<F>(v[0], ax, X);
+  pow_derivs<F>(v[1], by, Y);
+  pow_derivs<F>(v[2], cz, Z);
+  const F P = X[0] * Y[0] * Z[0] + (l >= 1 ? F(kShiftD) : F(0));
+  const F Pd[3] = {X[1] * Y[0] * Z[0], X[0] * Y[1] * Z[0], X[0] * Y[0] * Z[1]};
+  F Pdd[3][3];
   Pdd[0][0] = X[2] * Y[0] * Z[0];
   Pdd[1][1] = X[0] * Y[2] * Z[0];
   Pdd[2][2] = X[0] * Y[0] * Z[2];
   Pdd[0][1] = Pdd[1][0] = X[1] * Y[1] * Z[0];
   Pdd[0][2] = Pdd[2][0] = X[1] * Y[0] * Z[1];
   Pdd[1][2] = Pdd[2][1] = X[0] * Y[1] * Z[1];
-  const double lapP = Pdd[0][0] + Pdd[1][1] + Pdd[2][2];
-  const double dlapP[3] = {X[3] * Y[0] * Z[0] + X[1] * Y[2] * Z[0] + X[1] * Y[0] * Z[2],
-                           X[2] * Y[1] * Z[0] + X[0] * Y[3] * Z[0] + X[0] * Y[1] * Z[2],
-                           X[2] * Y[0] * Z[1] + X[0] * Y[2] * Z[1] + X[0] * Y[0] * Z[3]};
-  const double Rd[3] = {2.0 * v[0] * R[1], 2.0 * v[1] * R[1], 2.0 * v[2] * R[1]};
-  double Rdd[3][3];
+  const F lapP = Pdd[0][0] + Pdd[1][1] + Pdd[2][2];
+  const F dlapP[3] = {X[3] * Y[0] * Z[0] + X[1] * Y[2] * Z[0] + X[1] * Y[0] * Z[2],
+                      X[2] * Y[1] * Z[0] + X[0] * Y[3] * Z[0] + X[0] * Y[1] * Z[2],
+                      X[2] * Y[0] * Z[1] + X[0] * Y[2] * Z[1] + X[0] * Y[0] * Z[3]};
+  const F Rd[3] = {F(2) * v[0] * R[1], F(2) * v[1] * R[1], F(2) * v[2] * R[1]};
+  F Rdd[3][3];
 #pragma unroll
   for (int d = 0; d < 3; ++d)
 #pragma unroll
-    for (int e = 0; e < 3; ++e) Rdd[d][e] = 4.0 * v[d] * v[e] * R[2] + (d == e ? 2.0 * R[1] : 0.0);
-  const double lapR = 4.0 * s * R[2] + 6.0 * R[1];
-  const double k3 = 20.0 * R[2] + 8.0 * s * R[3];
+    for (int e = 0; e < 3; ++e) Rdd[d][e] = F(4) * v[d] * v[e] * R[2] + (d == e ? F(2) * R[1] : F(0));
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     g[d] = f * (Pd[d] * R[0] + P * Rd[d]);
 #pragma unroll
     for (int e = 0; e < 3; ++e) H[d][e] = f * (Pdd[d][e] * R[0] + Pd[d] * Rd[e] + Pd[e] * Rd[d] + P * Rdd[d][e]);
-    double t = 0.0;
+    F t = F(0);
 #pragma unroll
     for (int e = 0; e < 3; ++e) t += Pdd[d][e] * Rd[e] + Pd[e] * Rdd[d][e];
-    Tl[d] = f * (dlapP[d] * R[0] + lapP * Rd[d] + 2.0 * t + Pd[d] * lapR + P * v[d] * k3);
+    Tl[d] = f * (dlapP[d] * R[0] + lapP * Rd[d] + F(2) * t + Pd[d] * lapR + P * v[d] * k3);
   }
 }
 
@@ -147,12 +150,17 @@ __device__ __forceinline__ void ao_derivs(int code, double f, const double (&v)[
 // MODE_ADJOINT: G = [point_num][5][ao]; grad_nucl [nucl][3] -= sum q (per-CTA
 //   shared accumulators when use_smem, else device atomics); grad_coord
 //   ([3][gstride], may be null) += sum q.
+// MIXED: FP32 exponentials where a r^2 <= 30; in MODE_ADJOINT also G in FP32
+//   and the per-AO derivative arithmetic in FP32 (displacements, r^2, radial
+//   sums and the cancelling radial combinations in FP64; q summed in FP64).
 template <int MODE, bool MIXED>
 __global__ void __launch_bounds__(kWarpsD * 32)
 deriv_kernel(const DevTables T, const int64_t point_num, const double* __restrict__ coord, const int64_t cstride,
-             const double cutoff, double* __restrict__ out, const double* __restrict__ G,
+             const double cutoff, double* __restrict__ out, const void* __restrict__ Gv,
              double* __restrict__ grad_nucl, double* __restrict__ grad_coord, const int64_t gstride,
              const bool use_smem) {
+  using F = typename std::conditional<MIXED && MODE == MODE_ADJOINT, float, double>::type;
+  const F* __restrict__ G = (const F*)Gv;
   __shared__ DerivSmem smem[kWarpsD];
   extern __shared__ double sacc[];   // [nucl][3] (MODE_ADJOINT with use_smem)
   const int lane = threadIdx.x & 31;
@@ -176,16 +184,20 @@ deriv_kernel(const DevTables T, const int64_t point_num, const double* __restric
       const int k = k0 + lane;
       const bool valid = k < blk.w;
       int nl = kBlockNuc;   // past-the-end lanes form their own (last) segment
-      double g[3] = {0., 0., 0.}, H[3][3] = {{0., 0., 0.}, {0., 0., 0.}, {0., 0., 0.}}, Tl[3] = {0., 0., 0.};
+      F g[3] = {F(0), F(0), F(0)}, H[3][3] = {{F(0), F(0), F(0)}, {F(0), F(0), F(0)}, {F(0), F(0), F(0)}},
+        Tl[3] = {F(0), F(0), F(0)};
       if (valid) {
         const int code = T.ao_code[k];
         const int slot = (code >> 16) & 255;
         nl = (code >> 24) & 31;
         const double r2 = sm.nuc[nl][3];
-        const double R[4] = {sm.rad[slot][0], sm.rad[slot][1], sm.rad[slot][2], sm.rad[slot][3]};
-        if (r2 >= 0.0 && R[0] != 0.0) {
-          const double v[3] = {sm.nuc[nl][0], sm.nuc[nl][1], sm.nuc[nl][2]};
-          ao_derivs(code, T.ao_factor[k], v, r2, R, g, H, Tl);
+        const double* Rs = sm.rad[slot];
+        if (r2 >= 0.0 && Rs[0] != 0.0) {
+          const double lapR = 4.0 * r2 * Rs[2] + 6.0 * Rs[1];
+          const double k3 = 20.0 * Rs[2] + 8.0 * r2 * Rs[3];
+          const F v[3] = {(F)sm.nuc[nl][0], (F)sm.nuc[nl][1], (F)sm.nuc[nl][2]};
+          const F R[3] = {(F)Rs[0], (F)Rs[1], (F)Rs[2]};
+          ao_derivs<F>(code, (F)T.ao_factor[k], v, R, (F)lapR, (F)k3, g, H, Tl);
         }
       }
       if (MODE == MODE_HESSIAN) {
@@ -202,10 +214,11 @@ deriv_kernel(const DevTables T, const int64_t point_num, const double* __restric
       } else {
         double q[3] = {0., 0., 0.};
         if (valid) {
-          const double* gr = G + p * 5 * A + k;
-          const double G0 = gr[0], G1 = gr[A], G2 = gr[2 * A], G3 = gr[3 * A], G4 = gr[4 * A];
+          const F* gr = G + p * 5 * A + k;
+          const F G0 = gr[0], G1 = gr[A], G2 = gr[2 * A], G3 = gr[3 * A], G4 = gr[4 * A];
 #pragma unroll
-          for (int d = 0; d < 3; ++d) q[d] = G0 * g[d] + G1 * H[0][d] + G2 * H[1][d] + G3 * H[2][d] + G4 * Tl[d];
+          for (int d = 0; d < 3; ++d)
+            q[d] = (double)(G0 * g[d] + G1 * H[0][d] + G2 * H[1][d] + G3 * H[2][d] + G4 * Tl[d]);
         }
 #pragma unroll
         for (int d = 0; d < 3; ++d) pg[d] += q[d];
@@ -258,7 +271,7 @@ deriv_kernel(const DevTables T, const int64_t point_num, const double* __restric
 
 template <int MODE>
 cudaError_t launch_deriv(const DevTables& T, int64_t point_num, const double* coord, int64_t cstride, double cutoff,
-                         bool mixed, double* out, const double* G, double* grad_nucl, double* grad_coord,
+                         bool mixed, double* out, const void* G, double* grad_nucl, double* grad_coord,
                          int64_t gstride, cudaStream_t s) {
   if (point_num <= 0) return cudaSuccess;
   const int64_t items = point_num * (int64_t)T.nblock;
@@ -366,7 +379,7 @@ cudaError_t launch_ao_hessian(const DevTables& T, int64_t point_num, const doubl
 }
 
 cudaError_t launch_mo_adjoint_nuclear(const DevTables& T, int64_t point_num, const double* coord, int64_t cstride,
-                                      double cutoff, bool mixed, const double* G, double* grad_nucl,
+                                      double cutoff, bool mixed, const void* G, double* grad_nucl,
                                       double* grad_coord, int64_t gstride, cudaStream_t s) {
   return launch_deriv<MODE_ADJOINT>(T, point_num, coord, cstride, cutoff, mixed, nullptr, G, grad_nucl, grad_coord,
                                     gstride, s);

@@ -21,6 +21,7 @@
 #include <cuda_bf16.h>
 
 #include "kernels.cuh"
+#include "split.cuh"
 
 namespace qb {
 
@@ -123,11 +124,14 @@ __device__ __forceinline__ void stage_block(const DevTables& T, WarpSmem& sm, co
   __syncwarp();
 }
 
-// FP64 AO VGL (COMPS = 5) or AO value (COMPS = 1).
-template <int COMPS>
+// FP64 AO VGL (COMPS = 5) or AO value (COMPS = 1).  SPLIT: each value
+// stored as 3 bfloat16 pieces (split.cuh) at pieces[q * pstride + row * lda
+// + ao], rows p * COMPS + c, instead of FP64 in `out`.
+template <int COMPS, bool SPLIT = false>
 __global__ void __launch_bounds__(kWarps * 32)
 ao_f64_kernel(const DevTables T, const int64_t point_num, const double* __restrict__ coord,
-              const double cutoff, const bool dp_exp, double* __restrict__ out) {
+              const double cutoff, const bool dp_exp, double* __restrict__ out,
+              uint16_t* __restrict__ pieces = nullptr, const int64_t lda = 0, const int64_t pstride = 0) {
   __shared__ WarpSmem smem[kWarps];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
@@ -175,12 +179,24 @@ ao_f64_kernel(const DevTables T, const int64_t point_num, const double* __restri
           }
         }
       }
-      row[k] = v[0];
-      if (COMPS == 5) {
-        row[A + k] = v[1];
-        row[2 * A + k] = v[2];
-        row[3 * A + k] = v[3];
-        row[4 * A + k] = v[4];
+      if constexpr (SPLIT) {
+#pragma unroll
+        for (int c = 0; c < COMPS; ++c) {
+          uint16_t pc[3];
+          split3_bf16(v[c], pc);
+          uint16_t* dst = pieces + (p * COMPS + c) * lda + k;
+          dst[0] = pc[0];
+          dst[pstride] = pc[1];
+          dst[2 * pstride] = pc[2];
+        }
+      } else {
+        row[k] = v[0];
+        if (COMPS == 5) {
+          row[A + k] = v[1];
+          row[2 * A + k] = v[2];
+          row[3 * A + k] = v[3];
+          row[4 * A + k] = v[4];
+        }
       }
     }
     __syncwarp();
@@ -276,6 +292,17 @@ cudaError_t launch_ao_vgl_f64(const DevTables& T, int64_t point_num, const doubl
   if (point_num <= 0) return cudaSuccess;
   const int grid = grid_for(point_num * T.nblock);
   ao_f64_kernel<5><<<grid, kWarps * 32, 0, s>>>(T, point_num, coord, cutoff, dp_exp, ao_vgl);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ao_vgl_pieces(const DevTables& T, int64_t point_num, const double* coord, double cutoff,
+                                 bool dp_exp, void* pieces, int64_t lda, int64_t pstride, cudaStream_t s) {
+  if (point_num <= 0) return cudaSuccess;
+  if (lda < T.ao_num || lda % 8 != 0 || pstride % 8 != 0) return cudaErrorInvalidValue;
+  const int grid = grid_for(point_num * T.nblock);
+  ao_f64_kernel<5, true><<<grid, kWarps * 32, 0, s>>>(T, point_num, coord, cutoff, dp_exp, nullptr,
+                                                      (uint16_t*)pieces, lda, pstride);
   count_launch();
   return cudaGetLastError();
 }

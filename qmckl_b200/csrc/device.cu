@@ -216,6 +216,10 @@ struct DeviceState {
   DevBuf ao_hessian;
   uint64_t coef_rows_version = ~0ull;
   DevBuf coef_rows, adj_coord, adj_buf, adj_part, adj_nucl;
+  // mixed-form adjoint: bfloat16 pieces of the weights and of coefficient_t,
+  // the error word of its tensor-core kernels
+  uint64_t adj_ct_version = ~0ull;
+  DevBuf adj_wp, adj_ct, adj_err;
 };
 
 namespace {
@@ -691,7 +695,7 @@ void dev_detach(Context* ctx) {
   for (DevBuf* b : {&ds->tables, &ds->nucl, &ds->coord, &ds->prim_vgl, &ds->shell_vgl, &ds->ao_vgl, &ds->ao_value,
                     &ds->mo_vgl, &ds->mo_value, &ds->coef_t, &ds->tc_coef, &ds->tc_a, &ds->krec, &ds->order,
                     &ds->ao_hessian, &ds->coef_rows, &ds->adj_coord, &ds->adj_buf, &ds->adj_part, &ds->adj_nucl,
-                    &ds->tc3_coef, &ds->env, &ds->nuc_ao, &ds->forces})
+                    &ds->tc3_coef, &ds->env, &ds->nuc_ao, &ds->forces, &ds->adj_wp, &ds->adj_ct, &ds->adj_err})
     release(*b);
   if (ds->copy_stream) {
     cudaStreamSynchronize(ds->copy_stream);
@@ -1171,6 +1175,101 @@ qmckl_exit_code qmckl_b200_ao_hessian_device(qmckl_context context, const int64_
 // order), the AO buffer is then overwritten with G = W C ([point][5][ao]) and
 // the derivative kernel contracts G with the AO Hessian and Laplacian
 // gradient into grad_nucl / grad_coord.
+}  // extern "C"
+
+namespace qb {
+namespace {
+
+// Rows of W and of the AO matrix per K slice of the coefficient-gradient
+// contraction: each slice accumulates in FP32 in one CTA, the slices are
+// summed in FP64.  On the adjoint workload (40,704 points, 2000 AOs, 160 MOs)
+// the largest error of dL/dC against the FP64 form is 4.0e-7 of the largest
+// entry with 2048 rows, 7.0e-7 with 4096 and 1.7e-6 with 16384.
+constexpr int kAdjointSliceRows = 2048;
+
+// Mixed-form adjoint: the two contractions on the tensor cores.  Per chunk
+// of points: the weights W[(p,c)][mo] as 3 bfloat16 pieces; the AOs in FP64
+// arithmetic (FP32 exponentials where a r^2 <= 30, as in the derivative
+// kernel) stored as 3 bfloat16 pieces of rows p*5 + c; dC += AO^T W by the
+// split-K TN kernel, the partials summed in a fixed order into the [mo][ao]
+// layout; G = W C^T (FP32) from the pieces of coefficient_t; then the
+// derivative kernel in its mixed form.  Synchronizes once at the end to read
+// the kernels' error word.
+qmckl_exit_code adjoint_mixed(qmckl_context context, DeviceState* ds, int64_t P, const double* d_coord,
+                              const double* d_weight, double* d_grad_coef, double* d_grad_nucl, double* d_grad_coord) {
+  const char* fname = "qmckl_b200_mo_vgl_adjoint_device";
+  Context* ctx = ctx_of(context);
+  const int64_t A = ctx->ao_basis.ao_num, M = ctx->mo_basis.mo_num, N = ctx->nucleus.num;
+  const double cutoff = cutoff_of(ctx);
+  cudaStream_t s = ds->stream;
+  const int64_t ldw = (M + 7) / 8 * 8, lda = (A + 7) / 8 * 8;
+  const int kps = kAdjointSliceRows / 32;
+  qmckl_exit_code rc = sync_coef(context, ds);
+  if (rc != QMCKL_SUCCESS) return rc;
+  if (ds->adj_ct_version != ctx->mo_basis.coef_version || !ds->adj_ct.p) {
+    rc = ensure(context, ds->adj_ct, sizeof(uint16_t) * 3 * A * ldw, fname);
+    if (rc != QMCKL_SUCCESS) return rc;
+    QB_CUDA(tc_split_rows((const double*)ds->coef_t.p, A, (int)M, M, ds->adj_ct.p, (int)ldw, A * ldw, s), fname);
+    ds->adj_ct_version = ctx->mo_basis.coef_version;
+  }
+  const int64_t budget = (int64_t)2 << 30;
+  const int64_t row_bytes = std::max<int64_t>(20 * A, 30 * lda);   // G (FP32) or the AO pieces, per point
+  const int64_t max_chunk = std::min<int64_t>(P, std::max<int64_t>(64, budget / row_bytes));
+  const int64_t nchunks = (P + max_chunk - 1) / max_chunk;
+  const int64_t chunk = (P + nchunks - 1) / nchunks;   // equal chunks keep every launch full
+  const int splits = tc_tn_splits(5 * chunk, kps);
+  rc = ensure(context, ds->adj_coord, sizeof(double) * 3 * chunk, fname);
+  if (rc == QMCKL_SUCCESS) rc = ensure(context, ds->adj_buf, (size_t)row_bytes * chunk, fname);
+  if (rc == QMCKL_SUCCESS) rc = ensure(context, ds->adj_wp, sizeof(uint16_t) * 3 * 5 * chunk * ldw, fname);
+  if (rc == QMCKL_SUCCESS) rc = ensure(context, ds->adj_err, sizeof(int), fname);
+  if (rc == QMCKL_SUCCESS && d_grad_coef) rc = ensure(context, ds->adj_part, sizeof(double) * splits * A * M, fname);
+  if (rc == QMCKL_SUCCESS && !d_grad_nucl) rc = ensure(context, ds->adj_nucl, sizeof(double) * 3 * N, fname);
+  if (rc != QMCKL_SUCCESS) return rc;
+  double* gnucl = d_grad_nucl ? d_grad_nucl : (double*)ds->adj_nucl.p;
+  void* buf = ds->adj_buf.p;
+  double* cc = (double*)ds->adj_coord.p;
+  int* err = (int*)ds->adj_err.p;
+  QB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s), fname);
+  for (int64_t p0 = 0; p0 < P; p0 += chunk) {
+    const int64_t n = std::min<int64_t>(chunk, P - p0), rows = 5 * n;
+    const double* w = d_weight + p0 * 5 * M;
+    QB_CUDA(cudaMemcpy2DAsync(cc, sizeof(double) * n, d_coord + p0, sizeof(double) * P, sizeof(double) * n, 3,
+                              cudaMemcpyDeviceToDevice, s), fname);
+    QB_CUDA(tc_split_rows(w, rows, (int)M, M, ds->adj_wp.p, (int)ldw, rows * ldw, s), fname);
+    if (d_grad_coef) {
+      QB_CUDA(launch_ao_vgl_pieces(ds->T, n, cc, cutoff, false, buf, lda, rows * lda, s), fname);
+      QB_CUDA(tc_gemm_tn_split(buf, lda, rows * lda, A, ds->adj_wp.p, ldw, rows * ldw, (int)M, rows, kps,
+                               (double*)ds->adj_part.p, err, s),
+              fname);
+      QB_CUDA(launch_add_transposed((const double*)ds->adj_part.p, tc_tn_splits(rows, kps), A, M, d_grad_coef, true,
+                                    s),
+              fname);
+    }
+    if (d_grad_nucl || d_grad_coord) {
+      QB_CUDA(tc_gemm_nt(ds->adj_wp.p, ldw, rows * ldw, rows, M, ds->adj_ct.p, ldw, A * ldw, A, (float*)buf, A, err,
+                         s),
+              fname);
+      QB_CUDA(launch_mo_adjoint_nuclear(ds->T, n, cc, n, cutoff, true, buf, gnucl,
+                                        d_grad_coord ? d_grad_coord + p0 : nullptr, P, s),
+              fname);
+    }
+  }
+  int h = 0;
+  QB_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s), fname);
+  QB_CUDA(cudaStreamSynchronize(s), fname);
+  if (h != 0) {
+    char msg[QMCKL_MAX_MSG_LEN];
+    std::snprintf(msg, sizeof msg, "a tensor-core kernel of the adjoint gave up waiting (code %d)", h);
+    return qmckl_failwith(context, QMCKL_FAILURE, fname, msg);
+  }
+  return QMCKL_SUCCESS;
+}
+
+}  // namespace
+}  // namespace qb
+
+extern "C" {
+
 qmckl_exit_code qmckl_b200_mo_vgl_adjoint_device(qmckl_context context, const int64_t point_num,
                                                  const double* d_coord, const double* d_weight, double* d_grad_coef,
                                                  double* d_grad_nucl, double* d_grad_coord) {
@@ -1187,6 +1286,7 @@ qmckl_exit_code qmckl_b200_mo_vgl_adjoint_device(qmckl_context context, const in
   if (d_grad_nucl) QB_CUDA(cudaMemsetAsync(d_grad_nucl, 0, sizeof(double) * 3 * N, s), fname);
   if (d_grad_coord) QB_CUDA(cudaMemsetAsync(d_grad_coord, 0, sizeof(double) * 3 * P, s), fname);
   if (P == 0 || (!d_grad_coef && !d_grad_nucl && !d_grad_coord)) return QMCKL_SUCCESS;
+  if (mixed) return adjoint_mixed(context, ds, P, d_coord, d_weight, d_grad_coef, d_grad_nucl, d_grad_coord);
   // FP64 coefficient rows [mo][ao] for G = W C
   if (ds->coef_rows_version != ctx->mo_basis.coef_version || !ds->coef_rows.p) {
     rc = ensure(context, ds->coef_rows, sizeof(double) * M * A, fname);

@@ -50,6 +50,10 @@ void count_launch(int n = 1);
 // cudaGetLastError() after the launch.
 cudaError_t launch_ao_vgl_f64(const DevTables& T, int64_t point_num, const double* coord,
                               double cutoff, bool dp_exp, double* ao_vgl, cudaStream_t s);
+// The same FP64 AO VGL stored as 3 bfloat16 pieces (split.cuh) of rows
+// p*5 + c: pieces[q * pstride + row * lda + ao] (lda, pstride multiples of 8).
+cudaError_t launch_ao_vgl_pieces(const DevTables& T, int64_t point_num, const double* coord, double cutoff,
+                                 bool dp_exp, void* pieces, int64_t lda, int64_t pstride, cudaStream_t s);
 cudaError_t launch_ao_value_f64(const DevTables& T, int64_t point_num, const double* coord,
                                 double cutoff, bool dp_exp, double* ao_value, cudaStream_t s);
 cudaError_t launch_primitive_vgl(const DevTables& T, int64_t point_num, const double* coord,
@@ -80,7 +84,9 @@ cudaError_t launch_add_transposed(const double* part, int splits, int64_t M, int
 // Derivative kernels (adjoint.cu).  ao_hessian: [3][point_num][4][ao]
 // (coord [3][point_num]).  Adjoint: G [point_num][5][ao]; grad_nucl
 // [nucl][3] -= and grad_coord [3][gstride] += (may be null); coord
-// [3][cstride].  `mixed` selects FP32 exponentials where a r^2 <= 30.
+// [3][cstride].  `mixed` selects FP32 exponentials where a r^2 <= 30; for
+// the adjoint it also means G in FP32 (float*, else double*) and FP32
+// per-AO derivative arithmetic.
 cudaError_t launch_ao_hessian(const DevTables& T, int64_t point_num, const double* coord, double cutoff, bool mixed,
                               double* ao_hessian, cudaStream_t s);
 // Orbital forces (adjoint.cu): which = 0 forces_mo_value, 1 forces_mo_g,
@@ -90,7 +96,7 @@ cudaError_t launch_ao_hessian(const DevTables& T, int64_t point_num, const doubl
 cudaError_t launch_forces(int which, int64_t P, int64_t A, int64_t M, int N, const int2* nuc_ao, const double* X,
                           const double* Ct, double* out, cudaStream_t s);
 cudaError_t launch_mo_adjoint_nuclear(const DevTables& T, int64_t point_num, const double* coord, int64_t cstride,
-                                      double cutoff, bool mixed, const double* G, double* grad_nucl,
+                                      double cutoff, bool mixed, const void* G, double* grad_nucl,
                                       double* grad_coord, int64_t gstride, cudaStream_t s);
 
 }  // namespace qb

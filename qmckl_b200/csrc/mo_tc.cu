@@ -53,11 +53,11 @@ constexpr int kThreads = 32 * (kEpiWarps + 2);
 
 // ------------------------------------------------------------ GEMM kernel
 
-template <int PIECES, int STAGES>
+template <int PIECES, int STAGES, typename OutT = double>
 __global__ void __launch_bounds__(kThreads, 1)
 tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                const int64_t M, const int n_out, const int n_tile, const int kblocks, const int comps,
-               const double* __restrict__ scales, double* __restrict__ out, const int64_t ldo,
+               const double* __restrict__ scales, OutT* __restrict__ out, const int64_t ldo,
                int* __restrict__ err) {
   constexpr int NPROD = PIECES == 3 ? 6 : 3;
   constexpr int A_TILE = BM * BK * 2;             // bytes of one A piece tile
@@ -182,7 +182,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
             double v = stage[rr * 16 + ((cc + rr) & 15)];
             // float16 operands carry power-of-two component and MO scales
             if constexpr (PIECES == 2) v *= scales[(int)(row % comps)] * scales[kScaleCols + col];
-            out[row * ldo + col] = v;
+            out[row * ldo + col] = (OutT)v;
           }
         }
         __syncwarp();
@@ -194,6 +194,181 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
   if (warp == kEpiWarps + 1) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols));
+  }
+}
+
+// ------------------------------------------------------------ TN GEMM, split K
+//
+// part[z][a][b] = sum over the rows r of K slice z of X[r][a] * Y[r][b]: the
+// contraction over the rows of two row-major matrices (the coefficient
+// gradient of the adjoint, AO^T W).  Both operands are read as they lie,
+// MN-major: a stage holds BKR rows of 64-column boxes (128B swizzle), and the
+// shared-memory descriptors step from one 64-column box to the next by the
+// leading byte offset (one box) and from one 8-row group to the next by the
+// stride byte offset (1024 B).  The K range is cut into slices of kps stages
+// (one CTA each); the slices' FP32 accumulators are written as FP64 partials
+// and summed in a fixed order by the caller, so the FP32 accumulation of a
+// CTA stays short.
+constexpr int BKR = 32;                 // rows (K) per stage of the MN-major kernel
+constexpr int MN_BOX = 64 * BKR * 2;    // one {64 columns, BKR rows} bf16 box: 4 KB
+constexpr int kMnStages = 3;
+
+__device__ __forceinline__ uint64_t smem_desc_mn(uint32_t addr) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)(MN_BOX >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+tc_gemm_mn_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmY,
+                  const int64_t a_num, const int b_num, const int n_tile, const int kblocks, const int kps,
+                  double* __restrict__ part, int* __restrict__ err) {
+  constexpr int PIECES = 3, NPROD = 6, STAGES = kMnStages;
+  constexpr int A_BOXES = BM / 64;
+  constexpr int A_T = A_BOXES * MN_BOX;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = smem_raw + ((1024u - (tcx::smem_addr(smem_raw) & 1023u)) & 1023u);
+  const int b_boxes = n_tile / 64;
+  const int B_T = b_boxes * MN_BOX;
+  const int STAGE = PIECES * (A_T + B_T);
+  uint64_t* full = (uint64_t*)(smem + STAGES * STAGE);
+  uint64_t* empty = full + STAGES;
+  uint64_t* acc_full = empty + STAGES;
+  uint32_t* tmem_slot = (uint32_t*)(acc_full + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t a0 = (int64_t)blockIdx.x * BM;
+  const int n0 = blockIdx.y * n_tile;
+  const int kb0 = blockIdx.z * kps;
+  const int nk = min(kps, kblocks - kb0);          // >= 1: the host sizes the grid
+  // accumulators: A1*Y1 in two halves of the slice when three fit in TMEM
+  // (n_tile <= 128), else one; the corrections in the last
+  const bool halves = 3 * n_tile <= 512;
+  const uint32_t corr = (uint32_t)((halves ? 2 : 1) * n_tile);
+  uint32_t tmem_cols = 32;
+  while (tmem_cols < corr + (uint32_t)n_tile) tmem_cols <<= 1;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(acc_full, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == kEpiWarps + 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
+                 "r"(tmem_cols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == kEpiWarps) {
+    // ---------------- TMA producer
+    if (lane == 0) {
+      for (int j = 0; j < nk; ++j) {
+        const int s = j % STAGES;
+        const uint32_t phase = (uint32_t)(j / STAGES) & 1u;
+        if (!mbar_wait(&empty[s], phase ^ 1u, err, 1)) break;
+        uint8_t* st = smem + s * STAGE;
+        mbar_expect_tx(&full[s], (uint32_t)STAGE);
+        const int r = (kb0 + j) * BKR;
+        for (int p = 0; p < PIECES; ++p) {
+          for (int q = 0; q < A_BOXES; ++q)
+            tma_load_3d(st + p * A_T + q * MN_BOX, &tmX, &full[s], (int)a0 + 64 * q, r, p);
+          for (int q = 0; q < b_boxes; ++q)
+            tma_load_3d(st + PIECES * A_T + p * B_T + q * MN_BOX, &tmY, &full[s], n0 + 64 * q, r, p);
+        }
+      }
+    }
+  } else if (warp == kEpiWarps + 1) {
+    // ---------------- MMA issuer (both operands MN-major: bits 15 and 16)
+    if (lane == 0) {
+      const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) |
+                             ((uint32_t)(n_tile >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+      constexpr int pa[6] = {2, 1, 0, 1, 0, 0}, pb[6] = {0, 1, 2, 0, 1, 0};
+      for (int j = 0; j < nk; ++j) {
+        const int s = j % STAGES;
+        const uint32_t phase = (uint32_t)(j / STAGES) & 1u;
+        if (!mbar_wait(&full[s], phase, err, 2)) break;
+        tc_fence_after();
+        const uint32_t base = smem_addr(smem + s * STAGE);
+        for (int kk = 0; kk < BKR / UMMA_K; ++kk) {
+#pragma unroll
+          for (int t = 0; t < NPROD; ++t) {
+            // UMMA_K rows of 128 bytes per K step
+            const uint32_t a_addr = base + pa[t] * A_T + kk * UMMA_K * 128;
+            const uint32_t b_addr = base + PIECES * A_T + pb[t] * B_T + kk * UMMA_K * 128;
+            const bool lead = (t == NPROD - 1);
+            const bool second = halves && lead && (2 * j >= nk);
+            const uint32_t d = tmem + (lead ? (second ? (uint32_t)n_tile : 0u) : corr);
+            const bool first_use = lead ? (second ? (j == (nk + 1) / 2 && kk == 0) : (j == 0 && kk == 0))
+                                        : (j == 0 && kk == 0 && t == 0);
+            umma_bf16(d, smem_desc_mn(a_addr), smem_desc_mn(b_addr), idesc, first_use ? 0u : 1u);
+          }
+        }
+        umma_commit(&empty[s]);
+      }
+      umma_commit(acc_full);
+    }
+  } else {
+    // ---------------- epilogue (warps 0..3: TMEM lanes = rows a of the tile)
+    bool ok = mbar_wait(acc_full, 0, err, 3);
+    ok = __all_sync(0xffffffffu, ok && *(volatile int*)err == 0);
+    tc_fence_after();
+    if (ok) {
+      double* stage = (double*)smem + warp * 32 * 16;
+      const int row_base = warp * 32;
+      const bool has_second = halves && nk >= 2;
+      double* out = part + (int64_t)blockIdx.z * a_num * b_num;
+      for (int c0 = 0; c0 < n_tile && n0 + c0 < b_num; c0 += 16) {
+        uint32_t r0[16], r1[16], r2[16];
+        const uint32_t ta = tmem + ((uint32_t)row_base << 16) + (uint32_t)c0;
+        tmem_ld16(ta, r0);
+        if (has_second) tmem_ld16(ta + (uint32_t)n_tile, r1);
+        tmem_ld16(ta + corr, r2);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          double v = (double)__uint_as_float(r0[j]) + (double)__uint_as_float(r2[j]);
+          if (has_second) v += (double)__uint_as_float(r1[j]);
+          stage[lane * 16 + ((j + lane) & 15)] = v;
+        }
+        __syncwarp();
+        for (int q = 0; q < 16; ++q) {
+          const int rr = 2 * q + (lane >> 4);
+          const int cc = lane & 15;
+          const int64_t row = a0 + row_base + rr;
+          const int col = n0 + c0 + cc;
+          if (row < a_num && col < b_num) out[row * b_num + col] = stage[rr * 16 + ((cc + rr) & 15)];
+        }
+        __syncwarp();
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == kEpiWarps + 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols));
+  }
+}
+
+// FP64 rows -> 3 bfloat16 pieces (x = x1 + x2 + x3, each the rounding of the
+// remainder, formed in FP64), zero beyond `cols` up to the pitch ldo.
+__global__ void split_rows_kernel(const double* __restrict__ x, int64_t rows, int cols, int64_t ldx,
+                                  uint16_t* __restrict__ out, int ldo, int64_t pstride) {
+  const int64_t total = rows * (int64_t)ldo;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = i / ldo;
+    const int c = (int)(i - r * ldo);
+    uint16_t p[3];
+    split3_bf16(c < cols ? x[r * ldx + c] : 0.0, p);
+    out[i] = p[0];
+    out[pstride + i] = p[1];
+    out[2 * pstride + i] = p[2];
   }
 }
 
@@ -374,13 +549,13 @@ int* err_word() {
   return words[dev];
 }
 
-template <int PIECES, int STAGES>
+template <int PIECES, int STAGES, typename OutT = double>
 cudaError_t launch_gemm(const CUtensorMap& ta, const CUtensorMap& tb, int64_t M, int n_out, int n_tile, int n_tiles,
-                        int kblocks, int comps, const double* scales, double* out, int64_t ldo, int* err,
+                        int kblocks, int comps, const double* scales, OutT* out, int64_t ldo, int* err,
                         cudaStream_t s) {
   const size_t stage = (size_t)PIECES * (BM * BK * 2 + (size_t)n_tile * BK * 2);
   const size_t smem = 1024 + STAGES * stage + (2 * STAGES + 1) * 8 + 16;
-  auto kern = tc_gemm_kernel<PIECES, STAGES>;
+  auto kern = tc_gemm_kernel<PIECES, STAGES, OutT>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid((unsigned)((M + BM - 1) / BM), (unsigned)n_tiles);
@@ -595,6 +770,63 @@ cudaError_t tc_run_scratch(const DevTables& T, const TcPlan& plan, int64_t point
   e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return e;
   return h != 0 ? cudaErrorLaunchTimeout : cudaSuccess;
+}
+
+// ------------------------------------------------------------ adjoint contractions
+
+cudaError_t tc_split_rows(const double* x, int64_t rows, int cols, int64_t ldx, void* pieces, int ldp,
+                          int64_t pstride, cudaStream_t s) {
+  if (rows <= 0) return cudaSuccess;
+  if (ldp < cols || ldp % 8 != 0 || pstride % 8 != 0) return cudaErrorInvalidValue;
+  const int64_t total = rows * (int64_t)ldp;
+  const int grid = (int)std::min<int64_t>((total + 255) / 256, (int64_t)sm_count() * 16);
+  split_rows_kernel<<<grid, 256, 0, s>>>(x, rows, cols, ldx, (uint16_t*)pieces, ldp, pstride);
+  count_launch();
+  return cudaGetLastError();
+}
+
+int tc_tn_splits(int64_t rows, int kps) {
+  const int64_t kblocks = (rows + BKR - 1) / BKR;
+  return (int)((kblocks + kps - 1) / kps);
+}
+
+cudaError_t tc_gemm_tn_split(const void* x, int64_t ldx, int64_t x_pstride, int64_t a_num, const void* y, int64_t ldy,
+                             int64_t y_pstride, int b_num, int64_t rows, int kps, double* part, int* err,
+                             cudaStream_t s) {
+  if (rows <= 0 || a_num <= 0 || b_num <= 0) return cudaSuccess;
+  if (kps < 1 || ldx % 8 != 0 || ldy % 8 != 0 || x_pstride % 8 != 0 || y_pstride % 8 != 0)
+    return cudaErrorInvalidValue;
+  // N tiles of at most 192 columns, multiples of the 64-column box
+  const int n_tiles = (b_num + 191) / 192;
+  const int n_tile = ((b_num + n_tiles - 1) / n_tiles + 63) / 64 * 64;
+  const int64_t kblocks64 = (rows + BKR - 1) / BKR;
+  if (kblocks64 > (int64_t)1 << 30) return cudaErrorInvalidValue;
+  const int kblocks = (int)kblocks64;
+  const int splits = (kblocks + kps - 1) / kps;
+  CUtensorMap tx, ty;
+  if (!make_map(&tx, x, a_num, rows, ldx, 3, x_pstride, BKR)) return cudaErrorInvalidValue;
+  if (!make_map(&ty, y, b_num, rows, ldy, 3, y_pstride, BKR)) return cudaErrorInvalidValue;
+  const size_t stage = (size_t)3 * ((BM / 64) * MN_BOX + (size_t)(n_tile / 64) * MN_BOX);
+  const size_t smem = 1024 + kMnStages * stage + (2 * kMnStages + 1) * 8 + 16;
+  cudaError_t e = cudaFuncSetAttribute(tc_gemm_mn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid((unsigned)((a_num + BM - 1) / BM), (unsigned)n_tiles, (unsigned)splits);
+  tc_gemm_mn_kernel<<<grid, kThreads, smem, s>>>(tx, ty, a_num, b_num, n_tile, kblocks, kps, part, err);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t tc_gemm_nt(const void* x, int64_t ldx, int64_t x_pstride, int64_t rows, int64_t k, const void* y,
+                       int64_t ldy, int64_t y_pstride, int64_t n, float* out, int64_t ldo, int* err, cudaStream_t s) {
+  if (rows <= 0 || n <= 0) return cudaSuccess;
+  if (ldx % 8 != 0 || ldy % 8 != 0 || x_pstride % 8 != 0 || y_pstride % 8 != 0) return cudaErrorInvalidValue;
+  const TcPlan tiles = tc_plan(k, n, 3);   // N tiling of the forward contraction
+  CUtensorMap tx, ty;
+  if (!make_map(&tx, x, k, rows, ldx, 3, x_pstride, BM)) return cudaErrorInvalidValue;
+  if (!make_map(&ty, y, k, n, ldy, 3, y_pstride, tiles.n_tile)) return cudaErrorInvalidValue;
+  const int kblocks = (int)((k + BK - 1) / BK);
+  return launch_gemm<3, 2, float>(tx, ty, rows, (int)n, tiles.n_tile, tiles.n_tiles, kblocks, 1, nullptr, out, ldo,
+                                  err, s);
 }
 
 }  // namespace qb

@@ -90,6 +90,25 @@ cudaError_t tc_run_scratch(const DevTables& T, const TcPlan& plan, int64_t point
                            const double* coord, double cutoff, const void* d_coef, void* d_a, int* d_err,
                            double* out, cudaStream_t s);
 
+// Contractions of the mixed-form adjoint on the tensor cores (3 bfloat16
+// pieces, FP32 accumulation in TMEM, FP64 results).  Piece buffers are
+// [3][rows][ld] 16-bit values (ld and pstride multiples of 8, 16-byte
+// aligned base); columns beyond the logical width read as zero.
+//   tc_split_rows : FP64 x[rows][cols] (pitch ldx) -> pieces [3][rows][ldp]
+//   tc_gemm_tn_split : part[z][a][b] = sum over the rows of K slice z of
+//                   X[r][a] Y[r][b], z < tc_tn_splits(rows, kps); slices of
+//                   kps * 32 rows (the caller sums the partials)
+//   tc_gemm_nt    : out[r][j] (FP32, pitch ldo) = sum_k X[r][k] Y[j][k]
+// err: a device error word set by a timed-out barrier wait.
+cudaError_t tc_split_rows(const double* x, int64_t rows, int cols, int64_t ldx, void* pieces, int ldp,
+                          int64_t pstride, cudaStream_t s);
+int tc_tn_splits(int64_t rows, int kps);
+cudaError_t tc_gemm_tn_split(const void* x, int64_t ldx, int64_t x_pstride, int64_t a_num, const void* y, int64_t ldy,
+                             int64_t y_pstride, int b_num, int64_t rows, int kps, double* part, int* err,
+                             cudaStream_t s);
+cudaError_t tc_gemm_nt(const void* x, int64_t ldx, int64_t x_pstride, int64_t rows, int64_t k, const void* y,
+                       int64_t ldy, int64_t y_pstride, int64_t n, float* out, int64_t ldo, int* err, cudaStream_t s);
+
 // What the fixed-scratch entry point needs from a context whose basis and
 // coefficient pieces are already on the device (device.cu).
 struct PreparedMixed {

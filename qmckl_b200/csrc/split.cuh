@@ -69,11 +69,23 @@ __device__ __forceinline__ void split_one(float v, float inv_scale, uint16_t (&o
   }
 }
 
-// Reciprocal AO-component scales (exact: powers of two) for the producers.
+// One FP64 value -> 3 bfloat16 pieces, each the rounding of the remainder
+// (formed exactly in FP64): x = x1 + x2 + x3 to ~2^-24 relative.
+__device__ __forceinline__ void split3_bf16(double v, uint16_t (&o)[3]) {
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const __nv_bfloat16 h = __double2bfloat16(v);
+    o[q] = __bfloat16_as_ushort(h);
+    v -= (double)__bfloat162float(h);
+  }
+}
+
+// Reciprocal AO-component scales (exact: powers of two) for the producers;
+// all 1 when no scale block is given (3 bfloat16 pieces need none).
 template <int COMPS>
 __device__ __forceinline__ void load_inv_scales(const double* scales, float (&inv)[5]) {
 #pragma unroll
-  for (int c = 0; c < 5; ++c) inv[c] = (float)(1.0 / scales[c < COMPS ? c : 0]);
+  for (int c = 0; c < 5; ++c) inv[c] = scales ? (float)(1.0 / scales[c < COMPS ? c : 0]) : 1.f;
 }
 
 }  // namespace qb
