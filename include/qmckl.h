@@ -126,6 +126,9 @@ qmckl_exit_code qmckl_get_electron_down_num(const qmckl_context context, int64_t
 qmckl_exit_code qmckl_get_electron_walk_num(const qmckl_context context, int64_t* const walk_num);
 qmckl_exit_code qmckl_get_electron_coord(const qmckl_context context, const char transp,
                                          double* const coord, const int64_t size_max);
+/* point-nucleus distances [point][nucl] (org/qmckl_electron.org:1205-1262) */
+qmckl_exit_code qmckl_get_electron_en_distance(qmckl_context context, double* const distance,
+                                               const int64_t size_max);
 
 /* ---- AO basis: org/qmckl_ao.org:419-2266 (setters/getters), 3415-3798 (arrays) ---- */
 qmckl_exit_code qmckl_set_ao_basis_type(qmckl_context context, const char basis_type);
@@ -188,9 +191,11 @@ qmckl_exit_code qmckl_get_forces_mo_g(qmckl_context context, double* const force
 qmckl_exit_code qmckl_get_forces_mo_g_inplace(qmckl_context context, double* const forces_mo_g, const int64_t size_max);
 qmckl_exit_code qmckl_get_forces_mo_l(qmckl_context context, double* const forces_mo_l, const int64_t size_max);
 
-/* ---- MO basis: org/qmckl_mo.org:192-1747, 3479 ---- */
+/* ---- MO basis: org/qmckl_mo.org:192-1747, 2362-2400, 3479 ---- */
 qmckl_exit_code qmckl_set_mo_basis_mo_num(qmckl_context context, const int64_t mo_num);
 qmckl_exit_code qmckl_set_mo_basis_coefficient(qmckl_context context, const double* coefficient, const int64_t size_max);
+/* cusp adjustment radius per nucleus (org/qmckl_mo.org:479-700) */
+qmckl_exit_code qmckl_set_mo_basis_r_cusp(qmckl_context context, const double* r_cusp, const int64_t size_max);
 qmckl_exit_code qmckl_get_mo_basis_mo_num(const qmckl_context context, int64_t* mo_num);
 qmckl_exit_code qmckl_get_mo_basis_coefficient(const qmckl_context context, double* const coefficient, const int64_t size_max);
 bool            qmckl_mo_basis_provided(const qmckl_context context);
@@ -200,6 +205,8 @@ qmckl_exit_code qmckl_get_mo_basis_mo_value(qmckl_context context, double* const
 qmckl_exit_code qmckl_get_mo_basis_mo_value_inplace(qmckl_context context, double* const mo_value, const int64_t size_max);
 qmckl_exit_code qmckl_get_mo_basis_mo_vgl(qmckl_context context, double* const mo_vgl, const int64_t size_max);
 qmckl_exit_code qmckl_get_mo_basis_mo_vgl_inplace(qmckl_context context, double* const mo_vgl, const int64_t size_max);
+/* [3][point][3][mo] */
+qmckl_exit_code qmckl_get_mo_basis_mo_hessian(qmckl_context context, double* const mo_hessian, const int64_t size_max);
 
 #ifdef __cplusplus
 }

@@ -194,3 +194,155 @@ def forces(basis, coord, nucl_coord, coefficient, precision=53):
 
 def cutoff(precision=53):
     return lib().oracle_cutoff(precision)
+
+
+# ---------------------------------------------------------------- cusp-corrected MOs, MO Hessian
+#
+# numpy restatements of the reference's cusp adjustment and MO Hessian
+# (org/qmckl_mo.org); the AO quantities they read come from the C restatement.
+
+def ao_nucl_ang_mom(sysd):
+    """(ao_nucl [A], ao_ang_mom [A]) as finalized by the reference
+    (qmckl_finalize_basis, org/qmckl_ao.org:2965-3226): cartesian AOs shell by
+    shell, (l+1)(l+2)/2 per shell."""
+    nidx = np.asarray(sysd["nucleus_index"])
+    nsh = np.asarray(sysd["nucleus_shell_num"])
+    lsh = np.asarray(sysd["shell_ang_mom"])
+    shell_nucl = np.empty(lsh.size, dtype=np.int64)
+    for n in range(nidx.size):
+        shell_nucl[nidx[n]:nidx[n] + nsh[n]] = n
+    nucl, lval = [], []
+    for s in range(lsh.size):
+        k = (int(lsh[s]) + 1) * (int(lsh[s]) + 2) // 2
+        nucl += [shell_nucl[s]] * k
+        lval += [int(lsh[s])] * k
+    return np.array(nucl, dtype=np.int64), np.array(lval, dtype=np.int32)
+
+
+def en_distance(coord, nucl_coord):
+    """[P][N] point-nucleus distances (qmckl_compute_en_distance,
+    org/qmckl_electron.org:1357-1393, through qmckl_distance
+    org/qmckl_distance.org:488-640: x = R - r, sqrt(x*x + y*y + z*z))."""
+    c = np.asarray(coord, dtype=np.float64)               # [P][3]
+    n = np.asarray(nucl_coord, dtype=np.float64)          # [3][N]
+    x = n[0][None, :] - c[:, 0][:, None]
+    y = n[1][None, :] - c[:, 1][:, None]
+    z = n[2][None, :] - c[:, 2][:, None]
+    return np.sqrt(x * x + y * y + z * z)
+
+
+def mo_value_cusp(coefficient, ao_value_arr, ao_nucl, ao_l, en_dist, r_cusp, cusp_param):
+    """qmckl_compute_mo_basis_mo_value_cusp_doc (org/qmckl_mo.org:2807-2860):
+    the s AOs of a nucleus are left out at points closer than r_cusp (strictly),
+    and the cubic c0 + c1 r + c2 r^2 + c3 r^3 of that nucleus is added where
+    r <= r_cusp.  cusp_param [N][4][M]; returns [P][M]."""
+    C = np.asarray(coefficient, dtype=np.float64)          # [M][A]
+    rc = np.asarray(r_cusp, dtype=np.float64)
+    skip = (ao_l[None, :] == 0) & (en_dist[:, ao_nucl] < rc[ao_nucl][None, :])
+    mo = np.where(skip, 0.0, ao_value_arr) @ C.T
+    for n in range(rc.size):
+        inside = en_dist[:, n] <= rc[n]
+        r = en_dist[inside, n][:, None]
+        p = cusp_param[n]
+        mo[inside] += p[0][None, :] + r * (p[1][None, :] + r * (p[2][None, :] + r * p[3][None, :]))
+    return mo
+
+
+def mo_vgl_cusp(coefficient, ao_vgl_arr, ao_nucl, ao_l, coord, nucl_coord, r_cusp, cusp_param):
+    """qmckl_compute_mo_basis_mo_vgl_cusp_doc (org/qmckl_mo.org:3099-3185): AOs
+    kept where r > r_cusp or l > 0; where r < r_cusp the cubic's value,
+    gradient (c1/r + 2 c2 + 3 c3 r) (r - R) and Laplacian
+    2 c1/r + 6 c2 + 12 c3 r are added.  Returns [P][5][M]."""
+    C = np.asarray(coefficient, dtype=np.float64)
+    rc = np.asarray(r_cusp, dtype=np.float64)
+    pts = np.asarray(coord, dtype=np.float64)
+    nuc = np.asarray(nucl_coord, dtype=np.float64)
+    en = en_distance(pts, nuc)
+    keep = (en[:, ao_nucl] > rc[ao_nucl][None, :]) | (ao_l[None, :] > 0)          # [P][A]
+    mo = np.einsum("pck,ik->pci", np.where(keep[:, None, :], ao_vgl_arr, 0.0), C)
+    for n in range(rc.size):
+        inside = en[:, n] < rc[n]
+        if not inside.any():
+            continue
+        r = en[inside, n][:, None]
+        rv = pts[inside] - nuc[:, n][None, :]                                        # [p][3]
+        p = cusp_param[n]
+        mo[inside, 0] += p[0] + r * (p[1] + r * (p[2] + r * p[3]))
+        c1 = p[1] / r + 2.0 * p[2] + r * 3.0 * p[3]
+        for d in range(3):
+            mo[inside, 1 + d] += rv[:, d][:, None] * c1
+        mo[inside, 4] += 2.0 * p[1] / r + 6.0 * p[2] + 12.0 * p[3] * r
+    return mo
+
+
+def cusp_param(basis, sysd, r_cusp, precision=53):
+    """Parameters of the cusp cubic of every (nucleus, MO), [N][4][M], as
+    qmckl_set_mo_basis_r_cusp forms them (org/qmckl_mo.org:479-700): eta = the
+    MO at the nucleus without the s AOs left out there (mo_value_cusp with
+    zero parameters), phi / grad_phi / lap_phi = the nucleus's own s-AO part
+    of the MO at distance r_cusp along z (value, z derivative, Laplacian);
+    nuclei with charge < 0.1 keep zero parameters."""
+    C = np.asarray(sysd["mo_coef"], dtype=np.float64)
+    M = C.shape[0]
+    nuc = np.asarray(sysd["nucl_coord"], dtype=np.float64)
+    N = nuc.shape[1]
+    rc = np.asarray(r_cusp, dtype=np.float64)
+    Z = np.asarray(sysd["charge"], dtype=np.float64)
+    ao_nucl, ao_l = ao_nucl_ang_mom(sysd)
+    at = np.ascontiguousarray(nuc.T)                       # the nuclei as points
+    eta = mo_value_cusp(C, ao_value(basis, at, nuc, precision), ao_nucl, ao_l, en_distance(at, nuc), rc,
+                        np.zeros((N, 4, M)))               # [N][M]
+    shifted = at.copy()
+    shifted[:, 2] += rc
+    av = ao_vgl(basis, shifted, nuc, precision)            # [N][5][A]
+    out = np.zeros((N, 4, M))
+    for n in range(N):
+        s = (ao_nucl == n) & (ao_l == 0)
+        phi = C[:, s] @ av[n, 0, s]
+        gphi = C[:, s] @ av[n, 3, s]
+        lphi = C[:, s] @ av[n, 4, s]
+        if Z[n] < 0.1:
+            continue
+        R, z, e = rc[n], Z[n], eta[n]
+        out[n, 0] = -(R * (2. * e * z - 6. * gphi) + lphi * R * R + 6. * phi) / (2. * R * z - 6.)
+        out[n, 1] = (lphi * R * R * z - 6. * gphi * R * z + 6. * phi * z + 6. * e * z) / (2. * R * z - 6.)
+        out[n, 2] = -(R * (-5. * gphi * z - 1.5 * lphi) + lphi * R * R * z + 3. * phi * z + 3. * e * z
+                      + 6. * gphi) / (R * R * z - 3. * R)
+        out[n, 3] = (R * (-2. * gphi * z - lphi) + 0.5 * lphi * R * R * z + phi * z + e * z + 3. * gphi) / \
+            (R * R * R * z - 3. * R * R)
+    return out
+
+
+def mo_hessian(coefficient, ao_hessian_arr, ao_nucl=None, ao_l=None, coord=None, nucl_coord=None, r_cusp=None,
+               cusp_param_arr=None):
+    """MO Hessian [3][P][3][M] from ao_hessian [3][P][4][A]
+    (qmckl_compute_mo_basis_mo_hessian_doc_f, org/qmckl_mo.org:2540-2575);
+    with r_cusp, qmckl_compute_mo_basis_mo_hessian_cusp_doc_f (2629-2697):
+    AOs kept where ao_hessian[jj][p][0][k] != 0 and (r > r_cusp or l > 0), and
+    where r < r_cusp the cubic's Hessian
+    c1 (delta/r - x x'/r^3) + 2 c2 delta + 3 c3 (delta r + x x'/r)."""
+    C = np.asarray(coefficient, dtype=np.float64)
+    H = np.asarray(ao_hessian_arr, dtype=np.float64)
+    if r_cusp is None:
+        return np.einsum("jpkq,iq->jpki", H[:, :, :3, :], C)
+    rc = np.asarray(r_cusp, dtype=np.float64)
+    pts = np.asarray(coord, dtype=np.float64)
+    nuc = np.asarray(nucl_coord, dtype=np.float64)
+    en = en_distance(pts, nuc)
+    keep = ((en[:, ao_nucl] > rc[ao_nucl][None, :]) | (ao_l[None, :] > 0))[None, :, :] & (H[:, :, 0, :] != 0.0)
+    out = np.einsum("jpkq,iq->jpki", np.where(keep[:, :, None, :], H[:, :, :3, :], 0.0), C)
+    for n in range(rc.size):
+        inside = en[:, n] < rc[n]
+        if not inside.any():
+            continue
+        r = en[inside, n][:, None]
+        rv = pts[inside] - nuc[:, n][None, :]
+        p = cusp_param_arr[n]
+        for jj in range(3):
+            for kk in range(3):
+                t = -p[1] * rv[:, kk][:, None] * rv[:, jj][:, None] / r ** 3 + \
+                    p[3] * 3 * rv[:, kk][:, None] * rv[:, jj][:, None] / r
+                if kk == jj:
+                    t = t + p[1] / r + p[2] * 2 + p[3] * 3 * r
+                out[jj, inside, kk] += t
+    return out

@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(kWarpsD * 32)
 deriv_kernel(const DevTables T, const int64_t point_num, const double* __restrict__ coord, const int64_t cstride,
              const double cutoff, double* __restrict__ out, const void* __restrict__ Gv,
              double* __restrict__ grad_nucl, double* __restrict__ grad_coord, const int64_t gstride,
-             const bool use_smem) {
+             const bool use_smem, const double* __restrict__ cusp_r) {
   using F = typename std::conditional<MIXED && MODE == MODE_ADJOINT, float, double>::type;
   const F* __restrict__ G = (const F*)Gv;
   __shared__ DerivSmem smem[kWarpsD];
@@ -192,7 +192,7 @@ deriv_kernel(const DevTables T, const int64_t point_num, const double* __restric
         nl = (code >> 24) & 31;
         const double r2 = sm.nuc[nl][3];
         const double* Rs = sm.rad[slot];
-        if (r2 >= 0.0 && Rs[0] != 0.0) {
+        if (r2 >= 0.0 && Rs[0] != 0.0 && !cusp_masked(cusp_r, (code >> 12) & 15, blk.x + nl, r2, false)) {
           const double lapR = 4.0 * r2 * Rs[2] + 6.0 * Rs[1];
           const double k3 = 20.0 * Rs[2] + 8.0 * r2 * Rs[3];
           const F v[3] = {(F)sm.nuc[nl][0], (F)sm.nuc[nl][1], (F)sm.nuc[nl][2]};
@@ -272,7 +272,7 @@ deriv_kernel(const DevTables T, const int64_t point_num, const double* __restric
 template <int MODE>
 cudaError_t launch_deriv(const DevTables& T, int64_t point_num, const double* coord, int64_t cstride, double cutoff,
                          bool mixed, double* out, const void* G, double* grad_nucl, double* grad_coord,
-                         int64_t gstride, cudaStream_t s) {
+                         int64_t gstride, cudaStream_t s, const double* cusp_r = nullptr) {
   if (point_num <= 0) return cudaSuccess;
   const int64_t items = point_num * (int64_t)T.nblock;
   const int grid = (int)std::min<int64_t>((items + kWarpsD - 1) / kWarpsD, 148 * 8);
@@ -289,13 +289,13 @@ cudaError_t launch_deriv(const DevTables& T, int64_t point_num, const double* co
     if (dyn > 48 * 1024) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
     if (e != cudaSuccess) return e;
     k<<<grid, kWarpsD * 32, dyn, s>>>(T, point_num, coord, cstride, cutoff, out, G, grad_nucl, grad_coord, gstride,
-                                      use_smem);
+                                      use_smem, cusp_r);
   } else {
     auto k = deriv_kernel<MODE, false>;
     if (dyn > 48 * 1024) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
     if (e != cudaSuccess) return e;
     k<<<grid, kWarpsD * 32, dyn, s>>>(T, point_num, coord, cstride, cutoff, out, G, grad_nucl, grad_coord, gstride,
-                                      use_smem);
+                                      use_smem, cusp_r);
   }
   count_launch();
   return cudaGetLastError();
@@ -373,9 +373,9 @@ cudaError_t launch_forces(int which, int64_t P, int64_t A, int64_t M, int N, con
 }
 
 cudaError_t launch_ao_hessian(const DevTables& T, int64_t point_num, const double* coord, double cutoff, bool mixed,
-                              double* ao_hessian, cudaStream_t s) {
+                              double* ao_hessian, cudaStream_t s, const double* cusp_r) {
   return launch_deriv<MODE_HESSIAN>(T, point_num, coord, point_num, cutoff, mixed, ao_hessian, nullptr, nullptr,
-                                    nullptr, 0, s);
+                                    nullptr, 0, s, cusp_r);
 }
 
 cudaError_t launch_mo_adjoint_nuclear(const DevTables& T, int64_t point_num, const double* coord, int64_t cstride,

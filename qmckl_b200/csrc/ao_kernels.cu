@@ -131,7 +131,8 @@ template <int COMPS, bool SPLIT = false>
 __global__ void __launch_bounds__(kWarps * 32)
 ao_f64_kernel(const DevTables T, const int64_t point_num, const double* __restrict__ coord,
               const double cutoff, const bool dp_exp, double* __restrict__ out,
-              uint16_t* __restrict__ pieces = nullptr, const int64_t lda = 0, const int64_t pstride = 0) {
+              uint16_t* __restrict__ pieces = nullptr, const int64_t lda = 0, const int64_t pstride = 0,
+              const double* __restrict__ cusp_r = nullptr) {
   __shared__ WarpSmem smem[kWarps];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
@@ -153,7 +154,7 @@ ao_f64_kernel(const DevTables T, const int64_t point_num, const double* __restri
       const int slot = (code >> 16) & 255, nl = (code >> 24) & 31;
       double v[5] = {0., 0., 0., 0., 0.};
       const double s1 = sm.rad[slot][0];
-      if (sm.nuc[nl][3] >= 0.0 && s1 != 0.0) {
+      if (sm.nuc[nl][3] >= 0.0 && s1 != 0.0 && !cusp_masked(cusp_r, l, blk.x + nl, sm.nuc[nl][3], COMPS == 1)) {
         const double f = T.ao_factor[k];
         const double s2 = sm.rad[slot][1], s3 = sm.rad[slot][2], s4 = sm.rad[slot][3], s5 = sm.rad[slot][4];
         if (l == 0) {
@@ -288,10 +289,10 @@ int grid_for(int64_t items_per_warp_unit) {
 }  // namespace
 
 cudaError_t launch_ao_vgl_f64(const DevTables& T, int64_t point_num, const double* coord,
-                              double cutoff, bool dp_exp, double* ao_vgl, cudaStream_t s) {
+                              double cutoff, bool dp_exp, double* ao_vgl, cudaStream_t s, const double* cusp_r) {
   if (point_num <= 0) return cudaSuccess;
   const int grid = grid_for(point_num * T.nblock);
-  ao_f64_kernel<5><<<grid, kWarps * 32, 0, s>>>(T, point_num, coord, cutoff, dp_exp, ao_vgl);
+  ao_f64_kernel<5><<<grid, kWarps * 32, 0, s>>>(T, point_num, coord, cutoff, dp_exp, ao_vgl, nullptr, 0, 0, cusp_r);
   count_launch();
   return cudaGetLastError();
 }
@@ -308,10 +309,11 @@ cudaError_t launch_ao_vgl_pieces(const DevTables& T, int64_t point_num, const do
 }
 
 cudaError_t launch_ao_value_f64(const DevTables& T, int64_t point_num, const double* coord,
-                                double cutoff, bool dp_exp, double* ao_value, cudaStream_t s) {
+                                double cutoff, bool dp_exp, double* ao_value, cudaStream_t s, const double* cusp_r) {
   if (point_num <= 0) return cudaSuccess;
   const int grid = grid_for(point_num * T.nblock);
-  ao_f64_kernel<1><<<grid, kWarps * 32, 0, s>>>(T, point_num, coord, cutoff, dp_exp, ao_value);
+  ao_f64_kernel<1><<<grid, kWarps * 32, 0, s>>>(T, point_num, coord, cutoff, dp_exp, ao_value, nullptr, 0, 0,
+                                                cusp_r);
   count_launch();
   return cudaGetLastError();
 }

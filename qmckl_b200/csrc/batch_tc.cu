@@ -559,6 +559,8 @@ qmckl_exit_code qmckl_b200_batch_create(const qmckl_context* contexts, const int
       return qmckl_failwith(c0, QMCKL_NOT_PROVIDED, fname, "a context has no AO or MO basis");
     if (ctx->ao_basis.type != 'G') return fail(c0, fname, "only Gaussian basis sets are implemented");
     if (point_num[s] < 0) return qmckl_failwith(c0, QMCKL_INVALID_ARG_2, fname, "negative point count");
+    if (!ctx->mo_basis.r_cusp.empty())
+      return qmckl_failwith(c0, QMCKL_INVALID_ARG_1, fname, "cusp-adjusted MOs (r_cusp set) are not batched");
   }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {

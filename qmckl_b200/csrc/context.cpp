@@ -86,7 +86,7 @@ qmckl_context qmckl_context_copy(const qmckl_context context) {
   // context gets its own device state and recomputes on first use.
   dst->ao_basis.primitive_vgl_date = dst->ao_basis.shell_vgl_date = 0;
   dst->ao_basis.ao_vgl_date = dst->ao_basis.ao_value_date = dst->ao_basis.ao_hessian_date = 0;
-  dst->mo_basis.mo_vgl_date = dst->mo_basis.mo_value_date = 0;
+  dst->mo_basis.mo_vgl_date = dst->mo_basis.mo_value_date = dst->mo_basis.mo_hessian_date = 0;
   dst->extra = nullptr;
   return (qmckl_context)dst;
 }

@@ -53,7 +53,8 @@ bool build_krec_records(const Context* ctx, std::vector<uint8_t>& h, int& rec_by
   for (int64_t k = 0; k < A; ++k)
     if (aosh[k] < 0 || (k > 0 && aosh[k] < aosh[k - 1])) return false;
   const int64_t nkb = (A + 63) / 64;
-  struct KRecShell { double x, y, z, range; int32_t pb, pe, pad0, pad1; };
+  struct KRecShell { double x, y, z, range; int32_t pb, pe; float cusp_r2; int32_t pad; };
+  const std::vector<double>& rc = ctx->mo_basis.r_cusp;   // empty: no cusp adjustment
   size_t rec = 0;
   for (int64_t kb = 0; kb < nkb; ++kb) {
     const int64_t k0 = kb * 64, k1 = std::min<int64_t>(k0 + 64, A);
@@ -92,6 +93,8 @@ bool build_krec_records(const Context* ctx, std::vector<uint8_t>& h, int& rec_by
       e.y = ctx->nucleus.coord[n + N];
       e.z = ctx->nucleus.coord[n + 2 * N];
       e.range = d.nucleus_range[n];
+      e.cusp_r2 = (!rc.empty() && B.shell_ang_mom[q] == 0) ? (float)(rc[n] * rc[n]) : -1.f;
+      e.pad = 0;
       e.pb = np;
       for (int j = d.shell_coef_start[q]; j < d.shell_coef_start[q + 1]; ++j) {
         prm[2 * np] = d.expo_sorted[d.nuc_prim_start[n] + d.coef_prim[j]];
@@ -220,6 +223,11 @@ struct DeviceState {
   // the error word of its tensor-core kernels
   uint64_t adj_ct_version = ~0ull;
   DevBuf adj_wp, adj_ct, adj_err;
+  // cusp adjustment: radii [nucl] followed by the cubics' parameters
+  // [nucl][4][mo]; AO arrays with the left-out AOs zeroed, which feed only the
+  // MO step; point-nucleus distances; MO Hessian
+  uint64_t cusp_version = ~0ull, krec_cusp_version = ~0ull;
+  DevBuf cusp, ao_masked, en_dist, mo_hessian;
 };
 
 namespace {
@@ -446,9 +454,9 @@ qmckl_exit_code upload_tables(qmckl_context context, DeviceState* ds) {
   return QMCKL_SUCCESS;
 }
 
-qmckl_exit_code sync_inputs(qmckl_context context, DeviceState* ds, bool need_points) {
+qmckl_exit_code sync_inputs(qmckl_context context, DeviceState* ds, bool need_points, bool need_tables = true) {
   Context* ctx = ctx_of(context);
-  if (ds->basis_version != ctx->ao_basis.basis_version || ds->tables.p == nullptr) {
+  if (need_tables && (ds->basis_version != ctx->ao_basis.basis_version || ds->tables.p == nullptr)) {
     qmckl_exit_code rc = upload_tables(context, ds);
     if (rc != QMCKL_SUCCESS) return rc;
   }
@@ -488,6 +496,29 @@ qmckl_exit_code sync_coef(qmckl_context context, DeviceState* ds) {
   return QMCKL_SUCCESS;
 }
 
+// Radii and cubic parameters of the cusp adjustment on the device (*r, *prm);
+// both null when the context has none.
+qmckl_exit_code sync_cusp(qmckl_context context, DeviceState* ds, const double** r, const double** prm) {
+  Context* ctx = ctx_of(context);
+  *r = *prm = nullptr;
+  if (ctx->mo_basis.r_cusp.empty()) return QMCKL_SUCCESS;
+  const int64_t N = ctx->nucleus.num, M = ctx->mo_basis.mo_num;
+  const size_t nb = sizeof(double) * (size_t)N, pb = sizeof(double) * (size_t)(N * 4 * M);
+  if (ds->cusp_version != ctx->mo_basis.cusp_version || !ds->cusp.p || ds->cusp.cap < nb + pb) {
+    qmckl_exit_code rc = ensure(context, ds->cusp, nb + pb, "qmckl_b200_upload_cusp");
+    if (rc != QMCKL_SUCCESS) return rc;
+    QB_CUDA(cudaMemcpyAsync(ds->cusp.p, ctx->mo_basis.r_cusp.data(), nb, cudaMemcpyHostToDevice, ds->stream),
+            "qmckl_b200_upload_cusp");
+    QB_CUDA(cudaMemcpyAsync((char*)ds->cusp.p + nb, ctx->mo_basis.cusp_param.data(), pb, cudaMemcpyHostToDevice,
+                            ds->stream),
+            "qmckl_b200_upload_cusp");
+    ds->cusp_version = ctx->mo_basis.cusp_version;
+  }
+  *r = (const double*)ds->cusp.p;
+  *prm = (const double*)((const char*)ds->cusp.p + nb);
+  return QMCKL_SUCCESS;
+}
+
 qmckl_exit_code copy_out(qmckl_context context, DeviceState* ds, double* host, const void* dev, size_t bytes,
                          const char* where) {
   if (host != nullptr && bytes > 0)
@@ -500,15 +531,20 @@ DeviceState* state(qmckl_context context) { return ctx_of(context)->extra; }
 
 // ---- compute steps on the device (no date logic) ----
 
-qmckl_exit_code run_ao_vgl(qmckl_context context, DeviceState* ds, int64_t P, const double* coord, double* out) {
+// cusp_r (optional): zero the AOs that the cusp adjustment leaves out of the
+// MOs (the array then only feeds the MO step).
+qmckl_exit_code run_ao_vgl(qmckl_context context, DeviceState* ds, int64_t P, const double* coord, double* out,
+                           const double* cusp_r = nullptr) {
   Context* ctx = ctx_of(context);
-  QB_CUDA(launch_ao_vgl_f64(ds->T, P, coord, cutoff_of(ctx), ctx->precision > 23, out, ds->stream), "qmckl_b200_ao_vgl");
+  QB_CUDA(launch_ao_vgl_f64(ds->T, P, coord, cutoff_of(ctx), ctx->precision > 23, out, ds->stream, cusp_r),
+          "qmckl_b200_ao_vgl");
   return QMCKL_SUCCESS;
 }
 
-qmckl_exit_code run_ao_value(qmckl_context context, DeviceState* ds, int64_t P, const double* coord, double* out) {
+qmckl_exit_code run_ao_value(qmckl_context context, DeviceState* ds, int64_t P, const double* coord, double* out,
+                             const double* cusp_r = nullptr) {
   Context* ctx = ctx_of(context);
-  QB_CUDA(launch_ao_value_f64(ds->T, P, coord, cutoff_of(ctx), ctx->precision > 23, out, ds->stream),
+  QB_CUDA(launch_ao_value_f64(ds->T, P, coord, cutoff_of(ctx), ctx->precision > 23, out, ds->stream, cusp_r),
           "qmckl_b200_ao_value");
   return QMCKL_SUCCESS;
 }
@@ -526,6 +562,7 @@ bool build_krec(qmckl_context context, DeviceState* ds) {
   ds->rec_bytes = rec;
   ds->krec_basis_version = ctx->ao_basis.basis_version;
   ds->krec_nucl_version = ctx->nucleus.coord_version;
+  ds->krec_cusp_version = ctx->mo_basis.cusp_version;
   return true;
 }
 
@@ -577,9 +614,14 @@ qmckl_exit_code run_mo_mixed(qmckl_context context, DeviceState* ds, int64_t P, 
   if (copied) *copied = false;
   qmckl_exit_code rc0 = prepare_mixed(context, ds);
   if (rc0 != QMCKL_SUCCESS) return rc0;
+  const double *cr = nullptr, *cprm = nullptr;   // cusp adjustment (none: null)
+  rc0 = sync_cusp(context, ds, &cr, &cprm);
+  if (rc0 != QMCKL_SUCCESS) return rc0;
+  const int NN = (int)ctx->nucleus.num, MM = (int)ctx->mo_basis.mo_num;
   if (ds->fused) {
     bool ok = ds->krec.p != nullptr && ds->krec_basis_version == ctx->ao_basis.basis_version &&
-              ds->krec_nucl_version == ctx->nucleus.coord_version;
+              ds->krec_nucl_version == ctx->nucleus.coord_version &&
+              ds->krec_cusp_version == ctx->mo_basis.cusp_version;
     if (!ok) ok = build_krec(context, ds);
     if (ok && tc_fused_smem(ds->tc, comps, ds->rec_bytes) <= 232448) {
       // spatial order of the points, then the fused AO -> MO kernel (the AO
@@ -613,6 +655,9 @@ qmckl_exit_code run_mo_mixed(qmckl_context context, DeviceState* ds, int64_t P, 
         QB_CUDA(tc_run_fused(ds->T, ds->tc, n, comps, coord + a, cutoff_of(ctx), ds->tc_coef.p, ds->krec.p,
                              ds->rec_bytes, perm, rb, o, ds->stream, P),
                 "qmckl_b200_mo_mixed");
+        if (cr != nullptr)
+          QB_CUDA(launch_cusp_mo(n, comps, coord + a, P, NN, (const double*)ds->nucl.p, cr, cprm, MM, o, ds->stream),
+                  "qmckl_b200_mo_mixed");
         if (slices) {
           cudaEvent_t ev = ds->slice_ev[slice % kSlices];
           QB_CUDA(cudaEventRecord(ev, ds->stream), "qmckl_b200_mo_mixed");
@@ -634,8 +679,11 @@ qmckl_exit_code run_mo_mixed(qmckl_context context, DeviceState* ds, int64_t P, 
   qmckl_exit_code rc = ensure(context, ds->tc_a, abytes, "qmckl_b200_mo_mixed");
   if (rc != QMCKL_SUCCESS) return rc;
   QB_CUDA(tc_run(ds->T, ds->tc3, P, comps, coord, cutoff_of(ctx), ds->tc3_coef.p, ds->tc_a.p, out, ds->stream,
-                 ds->tiles.ntiles > 0 ? &ds->tiles : nullptr),
+                 ds->tiles.ntiles > 0 ? &ds->tiles : nullptr, cr),
           "qmckl_b200_mo_mixed");
+  if (cr != nullptr)
+    QB_CUDA(launch_cusp_mo(P, comps, coord, P, NN, (const double*)ds->nucl.p, cr, cprm, MM, out, ds->stream),
+            "qmckl_b200_mo_mixed");
   return QMCKL_SUCCESS;
 }
 
@@ -646,10 +694,18 @@ qmckl_exit_code run_mo(qmckl_context context, DeviceState* ds, int64_t P, const 
   if (use_mixed(ctx)) return run_mo_mixed(context, ds, P, coord, out, comps);
   qmckl_exit_code rc = sync_coef(context, ds);
   if (rc != QMCKL_SUCCESS) return rc;
-  rc = comps == 5 ? run_ao_vgl(context, ds, P, coord, ao_scratch) : run_ao_value(context, ds, P, coord, ao_scratch);
+  const double *cr = nullptr, *cprm = nullptr;
+  rc = sync_cusp(context, ds, &cr, &cprm);
+  if (rc != QMCKL_SUCCESS) return rc;
+  rc = comps == 5 ? run_ao_vgl(context, ds, P, coord, ao_scratch, cr)
+                  : run_ao_value(context, ds, P, coord, ao_scratch, cr);
   if (rc != QMCKL_SUCCESS) return rc;
   QB_CUDA(launch_gemm_f64(comps * P, M, A, ao_scratch, A, (const double*)ds->coef_t.p, M, out, M, ds->stream),
           "qmckl_b200_mo");
+  if (cr != nullptr)
+    QB_CUDA(launch_cusp_mo(P, comps, coord, P, (int)ctx->nucleus.num, (const double*)ds->nucl.p, cr, cprm, (int)M, out,
+                           ds->stream),
+            "qmckl_b200_mo");
   return QMCKL_SUCCESS;
 }
 
@@ -695,7 +751,8 @@ void dev_detach(Context* ctx) {
   for (DevBuf* b : {&ds->tables, &ds->nucl, &ds->coord, &ds->prim_vgl, &ds->shell_vgl, &ds->ao_vgl, &ds->ao_value,
                     &ds->mo_vgl, &ds->mo_value, &ds->coef_t, &ds->tc_coef, &ds->tc_a, &ds->krec, &ds->order,
                     &ds->ao_hessian, &ds->coef_rows, &ds->adj_coord, &ds->adj_buf, &ds->adj_part, &ds->adj_nucl,
-                    &ds->tc3_coef, &ds->env, &ds->nuc_ao, &ds->forces, &ds->adj_wp, &ds->adj_ct, &ds->adj_err})
+                    &ds->tc3_coef, &ds->env, &ds->nuc_ao, &ds->forces, &ds->adj_wp, &ds->adj_ct, &ds->adj_err,
+                    &ds->cusp, &ds->ao_masked, &ds->en_dist, &ds->mo_hessian})
     release(*b);
   if (ds->copy_stream) {
     cudaStreamSynchronize(ds->copy_stream);
@@ -736,6 +793,14 @@ qmckl_exit_code dev_prepared_mixed(qmckl_context context, PreparedMixed* out) {
   out->coef = ds->tc3_coef.p;
   out->stream = ds->stream;
   out->cutoff = cutoff_of(ctx);
+  if (!ctx->mo_basis.r_cusp.empty()) {
+    if (ds->cusp.p == nullptr || ds->cusp_version != ctx->mo_basis.cusp_version)
+      return qmckl_failwith(context, QMCKL_NOT_PROVIDED, fname,
+                            "cusp parameters not on the device yet: run one regular mixed-form evaluation of this "
+                            "context first");
+    out->cusp_r = (const double*)ds->cusp.p;
+    out->cusp_prm = out->cusp_r + ctx->nucleus.num;
+  }
   return QMCKL_SUCCESS;
 }
 
@@ -914,6 +979,12 @@ qmckl_exit_code dev_provide_mo_vgl(qmckl_context context, double* host_out) {
     if (rc != QMCKL_SUCCESS) return rc;
     if (use_mixed(ctx)) {
       rc = run_mo_mixed(context, ds, P, (const double*)ds->coord.p, (double*)ds->mo_vgl.p, 5, host_out, &copied);
+    } else if (!ctx->mo_basis.r_cusp.empty()) {
+      // FP64 form with the cusp adjustment: the AOs that it leaves out are
+      // zeroed in a separate AO array (the cached ao_vgl stays the plain one)
+      rc = ensure(context, ds->ao_masked, sizeof(double) * 5 * A * P, "qmckl_provide_mo_basis_mo_vgl");
+      if (rc != QMCKL_SUCCESS) return rc;
+      rc = run_mo(context, ds, P, (const double*)ds->coord.p, (double*)ds->ao_masked.p, (double*)ds->mo_vgl.p, 5);
     } else {
       // FP64 form: the AO array is materialised (and cached) as in the reference
       rc = sync_coef(context, ds);
@@ -958,6 +1029,10 @@ qmckl_exit_code dev_provide_mo_value(qmckl_context context, double* host_out) {
       if (rc != QMCKL_SUCCESS) return rc;
       if (use_mixed(ctx)) {
         rc = run_mo_mixed(context, ds, P, (const double*)ds->coord.p, (double*)ds->mo_value.p, 1);
+      } else if (!ctx->mo_basis.r_cusp.empty()) {
+        rc = ensure(context, ds->ao_masked, sizeof(double) * A * P, "qmckl_provide_mo_basis_mo_value");
+        if (rc != QMCKL_SUCCESS) return rc;
+        rc = run_mo(context, ds, P, (const double*)ds->coord.p, (double*)ds->ao_masked.p, (double*)ds->mo_value.p, 1);
       } else {
         rc = sync_coef(context, ds);
         if (rc != QMCKL_SUCCESS) return rc;
@@ -977,6 +1052,74 @@ qmckl_exit_code dev_provide_mo_value(qmckl_context context, double* host_out) {
     ctx->mo_basis.mo_value_date = ctx->date;
   }
   return copy_out(context, ds, host_out, ds->mo_value.p, bytes, "qmckl_get_mo_basis_mo_value");
+}
+
+// MO Hessian (org/qmckl_mo.org:2428-2600, FP64 in both forms, as the AO
+// Hessian): mo_hessian[jj][p][kk][i] = sum_k ao_hessian[jj][p][kk][k] *
+// coefficient_t[k][i], kk < 3, as three GEMMs (one per kk: rows (jj, p) of
+// stride 4 ao_num); with the cusp adjustment from an AO Hessian whose
+// left-out AOs are zeroed, plus the cubics' Hessians.
+qmckl_exit_code dev_provide_mo_hessian(qmckl_context context, double* host_out) {
+  const char* fname = "qmckl_provide_mo_basis_mo_hessian";
+  qmckl_exit_code rc = attach_all(context);
+  if (rc != QMCKL_SUCCESS) return rc;
+  Context* ctx = ctx_of(context);
+  DeviceState* ds = state(context);
+  if (ctx->ao_basis.type != 'G') return qmckl_failwith(context, QMCKL_FAILURE, fname, "only Gaussian basis sets are implemented");
+  if (!ctx->ao_basis.provided) return qmckl_failwith(context, QMCKL_NOT_PROVIDED, "qmckl_ao_basis", NULL);
+  const int64_t P = ctx->point.num, A = ctx->ao_basis.ao_num, M = ctx->mo_basis.mo_num;
+  const size_t bytes = sizeof(double) * 9 * M * P;
+  if (ctx->point.date > ctx->mo_basis.mo_hessian_date || ds->mo_hessian.cap < bytes) {
+    rc = sync_inputs(context, ds, true);
+    if (rc == QMCKL_SUCCESS) rc = sync_coef(context, ds);
+    const double *cr = nullptr, *cprm = nullptr;
+    if (rc == QMCKL_SUCCESS) rc = sync_cusp(context, ds, &cr, &cprm);
+    if (rc == QMCKL_SUCCESS) rc = ensure(context, ds->mo_hessian, bytes, fname);
+    if (rc != QMCKL_SUCCESS) return rc;
+    const double* H = nullptr;
+    if (cr != nullptr) {
+      rc = ensure(context, ds->ao_masked, sizeof(double) * 12 * A * P, fname);
+      if (rc != QMCKL_SUCCESS) return rc;
+      QB_CUDA(launch_ao_hessian(ds->T, P, (const double*)ds->coord.p, cutoff_of(ctx), ctx->precision <= 23,
+                                (double*)ds->ao_masked.p, ds->stream, cr),
+              fname);
+      H = (const double*)ds->ao_masked.p;
+    } else {
+      rc = dev_provide_ao_hessian(context, nullptr);
+      if (rc != QMCKL_SUCCESS) return rc;
+      H = (const double*)ds->ao_hessian.p;
+    }
+    double* out = (double*)ds->mo_hessian.p;
+    for (int kk = 0; kk < 3; ++kk)
+      QB_CUDA(launch_gemm_f64(3 * P, M, A, H + kk * A, 4 * A, (const double*)ds->coef_t.p, M, out + kk * M, 3 * M,
+                              ds->stream),
+              fname);
+    if (cr != nullptr)
+      QB_CUDA(launch_cusp_hessian(P, (const double*)ds->coord.p, (int)ctx->nucleus.num, (const double*)ds->nucl.p, cr,
+                                  cprm, (int)M, out, ds->stream),
+              fname);
+    ctx->mo_basis.mo_hessian_date = ctx->date;
+  }
+  return copy_out(context, ds, host_out, ds->mo_hessian.p, bytes, "qmckl_get_mo_basis_mo_hessian");
+}
+
+// en_distance[point][nucl] (org/qmckl_electron.org:1270-1393), recomputed on
+// every call.
+qmckl_exit_code dev_en_distance(qmckl_context context, double* host_out) {
+  qmckl_exit_code rc = attach_all(context);
+  if (rc != QMCKL_SUCCESS) return rc;
+  Context* ctx = ctx_of(context);
+  DeviceState* ds = state(context);
+  const int64_t P = ctx->point.num, N = ctx->nucleus.num;
+  rc = sync_inputs(context, ds, true, false);
+  if (rc != QMCKL_SUCCESS) return rc;
+  const size_t bytes = sizeof(double) * P * N;
+  rc = ensure(context, ds->en_dist, std::max<size_t>(bytes, 8), "qmckl_provide_en_distance");
+  if (rc != QMCKL_SUCCESS) return rc;
+  QB_CUDA(launch_en_distance(P, (const double*)ds->coord.p, (int)N, (const double*)ds->nucl.p, (double*)ds->en_dist.p,
+                             ds->stream),
+          "qmckl_provide_en_distance");
+  return copy_out(context, ds, host_out, ds->en_dist.p, bytes, "qmckl_get_electron_en_distance");
 }
 
 }  // namespace qb
@@ -1276,6 +1419,9 @@ qmckl_exit_code qmckl_b200_mo_vgl_adjoint_device(qmckl_context context, const in
   const char* fname = "qmckl_b200_mo_vgl_adjoint_device";
   qmckl_exit_code rc = device_entry(context, fname, point_num, d_coord, (void*)d_weight, true);
   if (rc != QMCKL_SUCCESS) return rc;
+  if (!ctx_of(context)->mo_basis.r_cusp.empty())
+    return qmckl_failwith(context, QMCKL_FAILURE, fname,
+                          "the adjoint is that of the MOs without the cusp adjustment, and r_cusp is set");
   Context* ctx = ctx_of(context);
   DeviceState* ds = state(context);
   const int64_t P = point_num, A = ctx->ao_basis.ao_num, M = ctx->mo_basis.mo_num, N = ctx->nucleus.num;

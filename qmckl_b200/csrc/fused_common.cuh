@@ -38,9 +38,14 @@ constexpr int A_TILE = BM * BK * 2;
 //   [16]   64 x {int32 code (a|b<<4|c<<8|l<<12|local_shell<<16, -1 past ao_num), float ao_factor}
 //   [528]  nsh x KRecShell
 //   [...]  nprim x {double exponent, double coefficient} (sorted per shell)
+// cusp_r2: the squared cusp radius of the shell's nucleus when the shell is
+// an s shell that the cusp adjustment leaves out of the MOs within it
+// (kernels.cuh cusp_masked; compared with r^2 <= cusp_r2), else -1.
 struct KRecShell {
   double x, y, z, range;
-  int32_t pb, pe, pad0, pad1;
+  int32_t pb, pe;
+  float cusp_r2;
+  int32_t pad;
 };
 constexpr int kRecAoOff = 16;
 constexpr int kRecShellOff = 16 + 64 * 8;
@@ -60,7 +65,7 @@ __device__ __forceinline__ void radial_rec(const KRecShell& S, const double2* pr
   // Laplacian sum_j c_j (-2 a_j e_j)(3 - 2 a_j r^2) = 4 r^2 S2 - 6 S1, all in
   // FP64 (the Laplacian's cancellation happens before the FP32 rounding).
   double S0 = 0.0, S1 = 0.0, S2 = 0.0;
-  live = !(r2 > cutoff * S.range);
+  live = !(r2 > cutoff * S.range) && !(r2 <= (double)S.cusp_r2);
   if (live) {
     for (int j = S.pb; j < S.pe; ++j) {
       const double2 pc = prm[j];

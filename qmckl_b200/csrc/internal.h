@@ -95,7 +95,12 @@ struct MoBasisRec {               // org/qmckl_mo.org:127-145
   std::vector<double> coefficient;    // [mo][ao]
   std::vector<double> coefficient_t;  // [ao][mo]
   uint64_t coef_version = 0;
-  uint64_t mo_vgl_date = 0, mo_value_date = 0;
+  uint64_t mo_vgl_date = 0, mo_value_date = 0, mo_hessian_date = 0;
+  // cusp adjustment (org/qmckl_mo.org:479-700): radius per nucleus (empty:
+  // none) and the cubic's parameters [nucl][4][mo]
+  std::vector<double> r_cusp;
+  std::vector<double> cusp_param;
+  uint64_t cusp_version = 0;          // bumped whenever either changes
   int32_t uninitialized = (1 << 2) - 1;
   bool provided = false;
 };
@@ -135,6 +140,8 @@ qmckl_exit_code dev_provide_ao_hessian(qmckl_context context, double* host_out);
 qmckl_exit_code dev_provide_forces(qmckl_context context, int which, double* host_out);
 qmckl_exit_code dev_provide_mo_vgl(qmckl_context context, double* host_out);
 qmckl_exit_code dev_provide_mo_value(qmckl_context context, double* host_out);
+qmckl_exit_code dev_provide_mo_hessian(qmckl_context context, double* host_out);
+qmckl_exit_code dev_en_distance(qmckl_context context, double* host_out);
 qmckl_exit_code dev_invalidate_mo(qmckl_context context);
 struct PreparedMixed;
 qmckl_exit_code dev_prepared_mixed(qmckl_context context, PreparedMixed* out);

@@ -46,16 +46,43 @@ struct DevTables {
 // Global count of kernels launched by this library.
 void count_launch(int n = 1);
 
+// Cusp adjustment of the MOs (org/qmckl_mo.org:2839, 3133, 2659): the s AOs
+// of a nucleus are left out of the MO sums at points closer to it than its
+// radius cusp_r[nucl] (strictly for MO values, r <= r_cusp for the VGL and the
+// Hessian).  r2 < 0 marks a nucleus screened out (its AOs vanish anyway).
+__device__ __forceinline__ bool cusp_masked(const double* cusp_r, int l, int nucl, double r2, bool strict) {
+  if (cusp_r == nullptr || l != 0 || r2 < 0.0) return false;
+  const double r = sqrt(r2), R = cusp_r[nucl];
+  return strict ? (r < R) : (r <= R);
+}
+
 // AO kernels (ao_kernels.cu).  coord is [3][point_num].  All return
 // cudaGetLastError() after the launch.
+// cusp_r (optional, [nucl]): the AOs that the cusp adjustment leaves out of
+// the MO sums are written as zero (the arrays then only feed the MO step).
 cudaError_t launch_ao_vgl_f64(const DevTables& T, int64_t point_num, const double* coord,
-                              double cutoff, bool dp_exp, double* ao_vgl, cudaStream_t s);
+                              double cutoff, bool dp_exp, double* ao_vgl, cudaStream_t s,
+                              const double* cusp_r = nullptr);
 // The same FP64 AO VGL stored as 3 bfloat16 pieces (split.cuh) of rows
 // p*5 + c: pieces[q * pstride + row * lda + ao] (lda, pstride multiples of 8).
 cudaError_t launch_ao_vgl_pieces(const DevTables& T, int64_t point_num, const double* coord, double cutoff,
                                  bool dp_exp, void* pieces, int64_t lda, int64_t pstride, cudaStream_t s);
 cudaError_t launch_ao_value_f64(const DevTables& T, int64_t point_num, const double* coord,
-                                double cutoff, bool dp_exp, double* ao_value, cudaStream_t s);
+                                double cutoff, bool dp_exp, double* ao_value, cudaStream_t s,
+                                const double* cusp_r = nullptr);
+// Cusp adjustment (cusp.cu, org/qmckl_mo.org:2807-2860, 3099-3185,
+// 2629-2697): adds, for every nucleus closer to a point than its radius, the
+// cubic c0 + c1 r + c2 r^2 + c3 r^3 (prm [nucl][4][mo]) to the point's MO
+// values (comps 1, r <= r_cusp) or its value, gradient and Laplacian
+// (comps 5, r < r_cusp) in out[point][comps][mo]; its Hessian to
+// out[3][point][3][mo].  coord [3][cstride].
+cudaError_t launch_cusp_mo(int64_t P, int comps, const double* coord, int64_t cstride, int N, const double* nucl,
+                           const double* r_cusp, const double* prm, int M, double* out, cudaStream_t s);
+cudaError_t launch_cusp_hessian(int64_t P, const double* coord, int N, const double* nucl, const double* r_cusp,
+                                const double* prm, int M, double* out, cudaStream_t s);
+// en_distance[point][nucl] (org/qmckl_electron.org:1357-1393)
+cudaError_t launch_en_distance(int64_t P, const double* coord, int N, const double* nucl, double* out,
+                               cudaStream_t s);
 cudaError_t launch_primitive_vgl(const DevTables& T, int64_t point_num, const double* coord,
                                  double cutoff, double* prim_vgl, cudaStream_t s);
 cudaError_t launch_shell_vgl(const DevTables& T, int64_t point_num, const double* coord,
@@ -88,7 +115,7 @@ cudaError_t launch_add_transposed(const double* part, int splits, int64_t M, int
 // the adjoint it also means G in FP32 (float*, else double*) and FP32
 // per-AO derivative arithmetic.
 cudaError_t launch_ao_hessian(const DevTables& T, int64_t point_num, const double* coord, double cutoff, bool mixed,
-                              double* ao_hessian, cudaStream_t s);
+                              double* ao_hessian, cudaStream_t s, const double* cusp_r = nullptr);
 // Orbital forces (adjoint.cu): which = 0 forces_mo_value, 1 forces_mo_g,
 // 2 forces_mo_l (from X = ao_vgl for 0, ao_hessian for 1 and 2, and
 // Ct = coefficient_t [ao][mo]), 3 forces_ao_value (from X = ao_vgl).

@@ -390,7 +390,7 @@ template <int PIECES, int COMPS>
 __global__ void __launch_bounds__(kAoWarps * 32)
 ao_split_kernel(const DevTables T, const int64_t point_num, const double* __restrict__ coord, const double cutoff,
                 const double* __restrict__ scales, uint16_t* __restrict__ a, const int64_t lda,
-                const int64_t piece_stride) {
+                const int64_t piece_stride, const double* __restrict__ cusp_r) {
   __shared__ MixSmem smem[kAoWarps];
   float inv[5];
   load_inv_scales<COMPS>(scales, inv);
@@ -454,7 +454,7 @@ ao_split_kernel(const DevTables T, const int64_t point_num, const double* __rest
       const int slot = (code >> 16) & 255, nl = (code >> 24) & 31;
       float v[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
       const float s1 = sm.rad[slot][0];
-      if (sm.nuc[nl][3] >= 0.0 && s1 != 0.0f) {
+      if (sm.nuc[nl][3] >= 0.0 && s1 != 0.0f && !cusp_masked(cusp_r, l, blk.x + nl, sm.nuc[nl][3], COMPS == 1)) {
         const float f = (float)T.ao_factor[k];
         const float s2 = sm.rad[slot][1], s3 = sm.rad[slot][2], s4 = sm.rad[slot][3], s5 = sm.rad[slot][4];
         if (l == 0) {
@@ -690,7 +690,7 @@ void tc_envelope(const ShellBound* shells, int nshell, double r_max, float r0, f
 
 cudaError_t tc_run(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps, const double* coord,
                    double cutoff, const void* d_coef, void* d_a, double* out, cudaStream_t s,
-                   const AoTiles* tiles) {
+                   const AoTiles* tiles, const double* cusp_r) {
   if (point_num <= 0) return cudaSuccess;
   if (plan.pieces != 3) return cudaErrorInvalidValue;   // the unfused kernels take 3 bfloat16 pieces
   const int64_t rows = (int64_t)comps * point_num;
@@ -699,15 +699,17 @@ cudaError_t tc_run(const DevTables& T, const TcPlan& plan, int64_t point_num, in
   uint16_t* a = (uint16_t*)d_a;
   const double* sc = tc_scales(plan, d_coef);
   // 1) AO pieces
-  if (tiles != nullptr) {
+  if (tiles != nullptr && cusp_r == nullptr) {   // the tiled producer knows no cusp adjustment
     cudaError_t e =
         launch_ao_tile_split(T, *tiles, point_num, coord, cutoff, comps, plan.pieces, sc, a, lda, pstride, s);
     if (e != cudaSuccess) return e;
   } else {
     const int64_t items = point_num * T.nblock;
     const int grid = (int)std::min<int64_t>((items + kAoWarps - 1) / kAoWarps, (int64_t)sm_count() * 8);
-    if (comps == 5) ao_split_kernel<3, 5><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, sc, a, lda, pstride);
-    else ao_split_kernel<3, 1><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, sc, a, lda, pstride);
+    if (comps == 5)
+      ao_split_kernel<3, 5><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, sc, a, lda, pstride, cusp_r);
+    else
+      ao_split_kernel<3, 1><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, sc, a, lda, pstride, cusp_r);
     count_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -739,7 +741,7 @@ cudaError_t tc_run(const DevTables& T, const TcPlan& plan, int64_t point_num, in
 
 cudaError_t tc_run_scratch(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps,
                            const double* coord, double cutoff, const void* d_coef, void* d_a, int* d_err,
-                           double* out, cudaStream_t s) {
+                           double* out, cudaStream_t s, const double* cusp_r) {
   if (point_num <= 0) return cudaSuccess;
   if (plan.pieces != 3) return cudaErrorInvalidValue;   // the unfused kernels take 3 bfloat16 pieces
   cudaError_t e = cudaMemsetAsync(d_err, 0, sizeof(int), s);
@@ -751,8 +753,10 @@ cudaError_t tc_run_scratch(const DevTables& T, const TcPlan& plan, int64_t point
   const double* sc = tc_scales(plan, d_coef);
   const int64_t items = point_num * T.nblock;
   const int grid = (int)std::min<int64_t>((items + kAoWarps - 1) / kAoWarps, (int64_t)sm_count() * 8);
-  if (comps == 5) ao_split_kernel<3, 5><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, sc, a, lda, pstride);
-  else ao_split_kernel<3, 1><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, sc, a, lda, pstride);
+  if (comps == 5)
+    ao_split_kernel<3, 5><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, sc, a, lda, pstride, cusp_r);
+  else
+    ao_split_kernel<3, 1><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, sc, a, lda, pstride, cusp_r);
   count_launch();
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;

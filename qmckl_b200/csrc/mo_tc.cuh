@@ -51,11 +51,13 @@ struct ShellBound {
 };
 void tc_envelope(const ShellBound* shells, int nshell, double r_max, float r0, float inv_log2q, float* env);
 // AO (mixed) -> A pieces -> tensor-core GEMM -> out[(point*comps + c)][mo] FP64
-// `tiles` selects the tiled AO kernel (ao_tile.cu) for the pieces when given.
+// `tiles` selects the tiled AO kernel (ao_tile.cu) for the pieces when given;
+// cusp_r ([nucl], optional) leaves out the AOs of the cusp adjustment
+// (kernels.cuh cusp_masked; the untiled producer is used then).
 struct AoTiles;
 cudaError_t tc_run(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps, const double* coord,
                    double cutoff, const void* d_coef, void* d_a, double* out, cudaStream_t s,
-                   const AoTiles* tiles = nullptr);
+                   const AoTiles* tiles = nullptr, const double* cusp_r = nullptr);
 
 // Fused form of tc_run: the AO pieces are produced in shared memory by the
 // GEMM kernel itself and never written to device memory (fused_tc.cu).
@@ -88,7 +90,7 @@ size_t tc_fused_smem(const TcPlan& plan, int comps, int rec_bytes);
 // device allocation.
 cudaError_t tc_run_scratch(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps,
                            const double* coord, double cutoff, const void* d_coef, void* d_a, int* d_err,
-                           double* out, cudaStream_t s);
+                           double* out, cudaStream_t s, const double* cusp_r = nullptr);
 
 // Contractions of the mixed-form adjoint on the tensor cores (3 bfloat16
 // pieces, FP32 accumulation in TMEM, FP64 results).  Piece buffers are
@@ -117,6 +119,10 @@ struct PreparedMixed {
   const void* coef = nullptr;
   cudaStream_t stream = nullptr;
   double cutoff = 0.0;
+  // cusp adjustment (null when the context has none): radii [nucl] and the
+  // cubics' parameters [nucl][4][mo] on the device
+  const double* cusp_r = nullptr;
+  const double* cusp_prm = nullptr;
 };
 
 }  // namespace qb

@@ -84,7 +84,13 @@ extern "C" qmckl_exit_code qmckl_b200_mo_vgl_device_noalloc(qmckl_context contex
   }
   int* d_err = (int*)base;
   void* d_a = (unsigned char*)base + kWordBytes;
-  e = tc_run_scratch(pm.T, pm.plan, point_num, 5, d_coord, pm.cutoff, pm.coef, d_a, d_err, d_mo_vgl, pm.stream);
+  e = tc_run_scratch(pm.T, pm.plan, point_num, 5, d_coord, pm.cutoff, pm.coef, d_a, d_err, d_mo_vgl, pm.stream,
+                     pm.cusp_r);
+  if (e == cudaSuccess && pm.cusp_r != nullptr) {
+    e = launch_cusp_mo(point_num, 5, d_coord, point_num, pm.T.nucl_num, pm.T.nucl_coord, pm.cusp_r, pm.cusp_prm,
+                       (int)pm.plan.mo_num, d_mo_vgl, pm.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(pm.stream);
+  }
   if (e != cudaSuccess) {
     char msg[QMCKL_MAX_MSG_LEN];
     std::snprintf(msg, sizeof msg, "CUDA error: %s", cudaGetErrorString(e));

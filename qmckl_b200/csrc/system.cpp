@@ -314,4 +314,17 @@ qmckl_exit_code qmckl_get_electron_coord(const qmckl_context context, const char
   return qmckl_get_point(context, transp, coord, size_max);
 }
 
+qmckl_exit_code qmckl_get_electron_en_distance(qmckl_context context, double* const distance, const int64_t size_max) {
+  // org/qmckl_electron.org:1226-1262, 1270-1340: distances between the
+  // context's points and the nuclei, [point][nucl], computed on the GPU
+  if (qmckl_context_check(context) == QMCKL_NULL_CONTEXT) return QMCKL_NULL_CONTEXT;
+  Context* ctx = ctx_of(context);
+  if (!ctx->nucleus.provided) return qmckl_failwith(context, QMCKL_NOT_PROVIDED, "qmckl_provide_en_distance", NULL);
+  if (distance == NULL)
+    return qmckl_failwith(context, QMCKL_INVALID_ARG_2, "qmckl_get_electron_en_distance", "distance is a null pointer");
+  if (size_max < ctx->point.num * ctx->nucleus.num)
+    return qmckl_failwith(context, QMCKL_INVALID_ARG_3, "qmckl_get_electron_en_distance", "size_max < num*nucl_num");
+  return dev_en_distance(context, distance);
+}
+
 }  // extern "C"

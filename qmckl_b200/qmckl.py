@@ -351,10 +351,17 @@ def mo_basis_rescale(ctx, factor):
     _call("qmckl_mo_basis_rescale", ctx, C.c_double(factor))
 
 
+def set_mo_basis_r_cusp(ctx, r_cusp):
+    a, p, n = _arr(r_cusp, np.float64)
+    _call("qmckl_set_mo_basis_r_cusp", ctx, p, n)
+
+
 get_mo_basis_mo_vgl = _array_getter("qmckl_get_mo_basis_mo_vgl")
 get_mo_basis_mo_vgl_inplace = _array_getter("qmckl_get_mo_basis_mo_vgl_inplace")
 get_mo_basis_mo_value = _array_getter("qmckl_get_mo_basis_mo_value")
 get_mo_basis_mo_value_inplace = _array_getter("qmckl_get_mo_basis_mo_value_inplace")
+get_mo_basis_mo_hessian = _array_getter("qmckl_get_mo_basis_mo_hessian")
+get_electron_en_distance = _array_getter("qmckl_get_electron_en_distance")
 
 # -------------------------------------------------- B200 extensions
 
