@@ -25,12 +25,35 @@
 
 namespace qb {
 
+// Squared radius beyond which every AO of shell s (on nucleus n) vanishes in
+// the fused producers: the nucleus is screened out (r^2 > cutoff * range) or
+// the shell's smallest exponent a_min, its first primitive, already breaks
+// the primitive loop (a_min r^2 > cutoff).  Widened by 1e-12 so that the
+// comparison in the kernel is conservative against rounding; -1 for a shell
+// without primitives.
+double shell_r2max(const Context* ctx, int s, int n, double cutoff) {
+  const AoDerived& d = ctx->ao_basis.d;
+  if (d.shell_coef_start[s] >= d.shell_coef_start[s + 1]) return -1.0;
+  const double a_min = d.expo_sorted[d.nuc_prim_start[n] + d.coef_prim[d.shell_coef_start[s]]];
+  const double r2 = std::min(cutoff * d.nucleus_range[n], a_min > 0.0 ? cutoff / a_min : 1e300);
+  return r2 * (1.0 + 1e-12);
+}
+
 // Records of the fused kernels: one per 64-AO K block, everything its AO
 // producers read (layout in fused_common.cuh), from the finalized basis and
 // the nuclear coordinates of a context.  rec_bytes is the common record size
 // (a multiple of 128).  Returns false when the AOs are not numbered shell by
 // shell in increasing order.
-bool build_krec_records(const Context* ctx, std::vector<uint8_t>& h, int& rec_bytes) {
+//
+// `order` (optional) is the sequence of shells along the K dimension (the
+// identity when null); then *ao_perm[k] is the AO at K position k, and, for
+// the tile skipping of the fused kernel, *kb_sh[kb] the range of positions
+// in `order` of block kb's shells and *sph[q] the screening sphere of shell
+// order[q]: its nucleus and the squared radius beyond which all its AOs
+// vanish (shell_r2max).
+bool build_krec_records(const Context* ctx, std::vector<uint8_t>& h, int& rec_bytes,
+                        const std::vector<int32_t>* order, std::vector<int64_t>* ao_perm, std::vector<int2>* kb_sh,
+                        std::vector<double4>* sph, double cutoff) {
   const AoBasisRec& B = ctx->ao_basis;
   const AoDerived& d = B.d;
   const int64_t A = B.ao_num, N = ctx->nucleus.num, S = B.shell_num;
@@ -52,33 +75,58 @@ bool build_krec_records(const Context* ctx, std::vector<uint8_t>& h, int& rec_by
   }
   for (int64_t k = 0; k < A; ++k)
     if (aosh[k] < 0 || (k > 0 && aosh[k] < aosh[k - 1])) return false;
+  // K positions: kq[k] = position in the shell sequence, korig[k] = AO
+  std::vector<int32_t> seq(S);
+  if (order) {
+    if ((int64_t)order->size() != S) return false;
+    seq = *order;
+  } else {
+    for (int64_t q = 0; q < S; ++q) seq[q] = (int32_t)q;
+  }
+  std::vector<int32_t> kq(A);
+  std::vector<int64_t> korig(A);
+  {
+    int64_t k = 0;
+    for (int64_t q = 0; q < S; ++q) {
+      const int s = seq[q];
+      const int64_t nk = (int64_t)(B.shell_ang_mom[s] + 1) * (B.shell_ang_mom[s] + 2) / 2;
+      for (int64_t t = 0; t < nk; ++t, ++k) {
+        if (k >= A) return false;
+        kq[k] = (int32_t)q;
+        korig[k] = d.ao_index[s] + t;
+      }
+    }
+    if (k != A) return false;
+  }
   const int64_t nkb = (A + 63) / 64;
   struct KRecShell { double x, y, z, range; int32_t pb, pe; float cusp_r2; int32_t pad; };
   const std::vector<double>& rc = ctx->mo_basis.r_cusp;   // empty: no cusp adjustment
   size_t rec = 0;
   for (int64_t kb = 0; kb < nkb; ++kb) {
     const int64_t k0 = kb * 64, k1 = std::min<int64_t>(k0 + 64, A);
-    const int s0 = aosh[k0], s1 = aosh[k1 - 1];
+    const int q0 = kq[k0], q1 = kq[k1 - 1];
     size_t np = 0;
-    for (int sh = s0; sh <= s1; ++sh) np += d.shell_coef_start[sh + 1] - d.shell_coef_start[sh];
-    rec = std::max(rec, 16 + 64 * 8 + (size_t)(s1 - s0 + 1) * sizeof(KRecShell) + np * 16);
+    for (int q = q0; q <= q1; ++q) np += d.shell_coef_start[seq[q] + 1] - d.shell_coef_start[seq[q]];
+    rec = std::max(rec, 16 + 64 * 8 + (size_t)(q1 - q0 + 1) * sizeof(KRecShell) + np * 16);
   }
   rec = (rec + 127) / 128 * 128;
   h.assign(rec * nkb, 0);
+  if (kb_sh) kb_sh->assign(nkb, make_int2(0, 0));
   for (int64_t kb = 0; kb < nkb; ++kb) {
     uint8_t* r = h.data() + kb * rec;
     const int64_t k0 = kb * 64, k1 = std::min<int64_t>(k0 + 64, A);
-    const int s0 = aosh[k0], s1 = aosh[k1 - 1];
+    const int q0 = kq[k0], q1 = kq[k1 - 1];
+    if (kb_sh) (*kb_sh)[kb] = make_int2(q0, q1 + 1);
     int32_t* hdr = (int32_t*)r;
     int32_t* ao = (int32_t*)(r + 16);
     KRecShell* sh = (KRecShell*)(r + 16 + 64 * 8);
-    double* prm = (double*)(r + 16 + 64 * 8 + (size_t)(s1 - s0 + 1) * sizeof(KRecShell));
-    hdr[0] = s1 - s0 + 1;
+    double* prm = (double*)(r + 16 + 64 * 8 + (size_t)(q1 - q0 + 1) * sizeof(KRecShell));
+    hdr[0] = q1 - q0 + 1;
     for (int64_t t = 0; t < 64; ++t) {
       const int64_t k = k0 + t;
       if (k < k1) {
-        const float f = (float)B.ao_factor[k];
-        ao[2 * t] = code[k] | ((aosh[k] - s0) << 16);
+        const float f = (float)B.ao_factor[korig[k]];
+        ao[2 * t] = code[korig[k]] | ((kq[k] - q0) << 16);
         std::memcpy(&ao[2 * t + 1], &f, 4);
       } else {
         ao[2 * t] = -1;
@@ -86,17 +134,18 @@ bool build_krec_records(const Context* ctx, std::vector<uint8_t>& h, int& rec_by
       }
     }
     int np = 0;
-    for (int q = s0; q <= s1; ++q) {
-      const int n = shell_nuc[q];
-      KRecShell& e = sh[q - s0];
+    for (int q = q0; q <= q1; ++q) {
+      const int sq = seq[q];
+      const int n = shell_nuc[sq];
+      KRecShell& e = sh[q - q0];
       e.x = ctx->nucleus.coord[n];
       e.y = ctx->nucleus.coord[n + N];
       e.z = ctx->nucleus.coord[n + 2 * N];
       e.range = d.nucleus_range[n];
-      e.cusp_r2 = (!rc.empty() && B.shell_ang_mom[q] == 0) ? (float)(rc[n] * rc[n]) : -1.f;
+      e.cusp_r2 = (!rc.empty() && B.shell_ang_mom[sq] == 0) ? (float)(rc[n] * rc[n]) : -1.f;
       e.pad = 0;
       e.pb = np;
-      for (int j = d.shell_coef_start[q]; j < d.shell_coef_start[q + 1]; ++j) {
+      for (int j = d.shell_coef_start[sq]; j < d.shell_coef_start[sq + 1]; ++j) {
         prm[2 * np] = d.expo_sorted[d.nuc_prim_start[n] + d.coef_prim[j]];
         prm[2 * np + 1] = d.coef_val[j];
         ++np;
@@ -105,8 +154,67 @@ bool build_krec_records(const Context* ctx, std::vector<uint8_t>& h, int& rec_by
     }
     hdr[1] = np;
   }
+  if (ao_perm) *ao_perm = korig;
+  if (sph) {
+    sph->resize(S);
+    for (int64_t q = 0; q < S; ++q) {
+      const int sq = seq[q];
+      const int n = shell_nuc[sq];
+      (*sph)[q] = make_double4(ctx->nucleus.coord[n], ctx->nucleus.coord[n + N], ctx->nucleus.coord[n + 2 * N],
+                               shell_r2max(ctx, sq, n, cutoff));
+    }
+  }
   rec_bytes = (int)rec;
   return true;
+}
+
+bool build_krec_records(const Context* ctx, std::vector<uint8_t>& h, int& rec_bytes) {
+  return build_krec_records(ctx, h, rec_bytes, nullptr, nullptr, nullptr, nullptr, 0.0);
+}
+
+// Shell order of the fused kernel's K dimension: the shells in three classes
+// of their screening radius (the largest third first), each class in Morton
+// order (5 bits per axis) of its nucleus over the nuclei's bounding box, ties
+// in shell order.  The 64-AO K blocks of the compact classes then hold shells
+// of nearby nuclei, which vanish together over a tile of spatially close
+// points; on the config-1 molecule 48% of (tile, K block) pairs are then
+// entirely zero and skipped, against 5% in the basis order.
+std::vector<int32_t> fused_shell_order(const Context* ctx, double cutoff) {
+  const AoBasisRec& B = ctx->ao_basis;
+  const int64_t S = B.shell_num, N = ctx->nucleus.num;
+  std::vector<int32_t> shell_nuc(S, 0);
+  for (int64_t m = 0; m < N; ++m)
+    for (int64_t s = B.nucleus_index[m]; s < B.nucleus_index[m] + B.nucleus_shell_num[m]; ++s) shell_nuc[s] = (int32_t)m;
+  std::vector<double> r2(S);
+  for (int64_t s = 0; s < S; ++s) r2[s] = shell_r2max(ctx, (int)s, shell_nuc[s], cutoff);
+  std::vector<double> sorted_r2 = r2;
+  std::sort(sorted_r2.begin(), sorted_r2.end());
+  const double t1 = sorted_r2[S / 3], t2 = sorted_r2[(2 * S) / 3];
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int64_t n = 0; n < N; ++n)
+    for (int c = 0; c < 3; ++c) {
+      lo[c] = std::min(lo[c], ctx->nucleus.coord[n + c * N]);
+      hi[c] = std::max(hi[c], ctx->nucleus.coord[n + c * N]);
+    }
+  auto morton = [&](int n) {
+    uint32_t key = 0;
+    for (int c = 0; c < 3; ++c) {
+      const double w = hi[c] - lo[c];
+      int cell = w > 0.0 ? (int)std::floor((ctx->nucleus.coord[n + c * N] - lo[c]) / w * 32.0) : 0;
+      cell = std::min(31, std::max(0, cell));
+      for (int b = 0; b < 5; ++b) key |= (uint32_t)((cell >> b) & 1) << (3 * b + c);
+    }
+    return key;
+  };
+  std::vector<int64_t> key(S);
+  for (int64_t s = 0; s < S; ++s) {
+    const int cls = r2[s] >= t2 ? 0 : (r2[s] >= t1 ? 1 : 2);
+    key[s] = ((int64_t)cls << 40) | ((int64_t)morton(shell_nuc[s]) << 20) | s;
+  }
+  std::vector<int32_t> order(S);
+  for (int64_t s = 0; s < S; ++s) order[s] = (int32_t)s;
+  std::sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return key[a] < key[b]; });
+  return order;
 }
 
 // Row-bound envelopes of the 2-piece float16 operands (fused_common.cuh
@@ -228,6 +336,11 @@ struct DeviceState {
   // MO step; point-nucleus distances; MO Hessian
   uint64_t cusp_version = ~0ull, krec_cusp_version = ~0ull;
   DevBuf cusp, ao_masked, en_dist, mo_hessian;
+  // fused kernel: K order (AO at each K position; the coefficient pieces of
+  // the fused plan follow it), tile-skipping tables, cutoff they were built for
+  std::vector<int64_t> fused_perm;
+  DevBuf kskip;
+  double krec_cutoff = -1.0;
 };
 
 namespace {
@@ -549,38 +662,79 @@ qmckl_exit_code run_ao_value(qmckl_context context, DeviceState* ds, int64_t P, 
   return QMCKL_SUCCESS;
 }
 
-// Device copy of the K-block records of the fused kernel (built by
-// build_krec_records).  Returns false when the AO numbering does not allow
-// them (then the unfused kernels are used).
-bool build_krec(qmckl_context context, DeviceState* ds) {
+// The fused kernel's device tables: K-block records in the shell order of
+// fused_shell_order (or the basis order when the reordered records do not fit
+// the kernel's shared memory), the tile-skipping tables, and the coefficient
+// pieces of the fused plan in the same K order.  *usable = false when the AO
+// numbering allows no records or the kernel does not fit (the unfused kernels
+// are used then).
+qmckl_exit_code prepare_fused(qmckl_context context, DeviceState* ds, bool* usable) {
+  const char* fname = "qmckl_b200_mo_mixed";
   Context* ctx = ctx_of(context);
-  std::vector<uint8_t> h;
-  int rec = 0;
-  if (!build_krec_records(ctx, h, rec)) return false;
-  if (ensure(context, ds->krec, h.size(), "qmckl_b200_mo_mixed") != QMCKL_SUCCESS) return false;
-  if (cudaMemcpy(ds->krec.p, h.data(), h.size(), cudaMemcpyHostToDevice) != cudaSuccess) return false;
-  ds->rec_bytes = rec;
-  ds->krec_basis_version = ctx->ao_basis.basis_version;
-  ds->krec_nucl_version = ctx->nucleus.coord_version;
-  ds->krec_cusp_version = ctx->mo_basis.cusp_version;
-  return true;
-}
-
-// Coefficient pieces of the fused plan (split_pieces) and of the unfused
-// plan (3 bfloat16 pieces), and the row-bound envelopes, on the device.
-qmckl_exit_code prepare_mixed(qmckl_context context, DeviceState* ds) {
-  Context* ctx = ctx_of(context);
-  const int64_t A = ctx->ao_basis.ao_num, M = ctx->mo_basis.mo_num;
+  *usable = false;
+  const int64_t A = ctx->ao_basis.ao_num, M = ctx->mo_basis.mo_num, S = ctx->ao_basis.shell_num;
   const int pieces = ds->split_pieces;
-  if (ds->tc_coef_version != ctx->mo_basis.coef_version || ds->tc_pieces != pieces || !ds->tc_coef.p) {
-    TcPlan plan = tc_plan(A, M, pieces);
-    qmckl_exit_code rc = ensure(context, ds->tc_coef, plan.coef_bytes, "qmckl_b200_mo_mixed");
+  const double cutoff = cutoff_of(ctx);
+  const TcPlan plan = tc_plan(A, M, pieces);
+  // the VGL kernel decides the order; the value kernel (128-point tiles) may
+  // still not fit, which run_mo_mixed checks per call
+  auto fits = [&](int rec) { return tc_fused_smem(plan, 5, rec) <= 232448; };
+  const bool fresh = ds->krec.p != nullptr && ds->kskip.p != nullptr &&
+                     ds->krec_basis_version == ctx->ao_basis.basis_version &&
+                     ds->krec_nucl_version == ctx->nucleus.coord_version &&
+                     ds->krec_cusp_version == ctx->mo_basis.cusp_version && ds->krec_cutoff == cutoff;
+  if (!fresh) {
+    std::vector<uint8_t> h;
+    std::vector<int64_t> perm;
+    std::vector<int2> kb_sh;
+    std::vector<double4> sph;
+    int rec = 0;
+    const std::vector<int32_t> order = fused_shell_order(ctx, cutoff);
+    bool ok = build_krec_records(ctx, h, rec, &order, &perm, &kb_sh, &sph, cutoff) && fits(rec);
+    if (!ok && !build_krec_records(ctx, h, rec, nullptr, &perm, &kb_sh, &sph, cutoff)) return QMCKL_SUCCESS;
+    qmckl_exit_code rc = ensure(context, ds->krec, h.size(), fname);
     if (rc != QMCKL_SUCCESS) return rc;
-    QB_CUDA(tc_prepare_coef(plan, ctx->mo_basis.coefficient.data(), ds->tc_coef.p, ds->stream), "qmckl_b200_mo_mixed");
+    const size_t kbytes = tc_kskip_bytes(A, S);
+    rc = ensure(context, ds->kskip, kbytes, fname);
+    if (rc != QMCKL_SUCCESS) return rc;
+    std::vector<uint8_t> ks(kbytes, 0);
+    std::memcpy(ks.data(), kb_sh.data(), sizeof(int2) * kb_sh.size());
+    std::memcpy(ks.data() + (kbytes - sizeof(double4) * (size_t)S), sph.data(), sizeof(double4) * sph.size());
+    QB_CUDA(cudaMemcpy(ds->krec.p, h.data(), h.size(), cudaMemcpyHostToDevice), fname);
+    QB_CUDA(cudaMemcpy(ds->kskip.p, ks.data(), kbytes, cudaMemcpyHostToDevice), fname);
+    ds->rec_bytes = rec;
+    ds->krec_basis_version = ctx->ao_basis.basis_version;
+    ds->krec_nucl_version = ctx->nucleus.coord_version;
+    ds->krec_cusp_version = ctx->mo_basis.cusp_version;
+    ds->krec_cutoff = cutoff;
+    if (perm != ds->fused_perm) {
+      ds->fused_perm = std::move(perm);
+      ds->tc_coef_version = ~0ull;   // the coefficient pieces follow the K order
+    }
+  }
+  if (!fits(ds->rec_bytes)) return QMCKL_SUCCESS;
+  if (ds->tc_coef_version != ctx->mo_basis.coef_version || ds->tc_pieces != pieces || !ds->tc_coef.p) {
+    // coefficient columns in the K order of the records
+    std::vector<double> cp((size_t)(M * A));
+    const std::vector<double>& c = ctx->mo_basis.coefficient;
+    for (int64_t i = 0; i < M; ++i)
+      for (int64_t k = 0; k < A; ++k) cp[i * A + k] = c[i * A + ds->fused_perm[k]];
+    qmckl_exit_code rc = ensure(context, ds->tc_coef, plan.coef_bytes, fname);
+    if (rc != QMCKL_SUCCESS) return rc;
+    QB_CUDA(tc_prepare_coef(plan, cp.data(), ds->tc_coef.p, ds->stream), fname);
     ds->tc = plan;
     ds->tc_coef_version = ctx->mo_basis.coef_version;
     ds->tc_pieces = pieces;
   }
+  *usable = true;
+  return QMCKL_SUCCESS;
+}
+
+// Coefficient pieces of the unfused plan (3 bfloat16 pieces) and the
+// row-bound envelopes on the device.
+qmckl_exit_code prepare_mixed(qmckl_context context, DeviceState* ds) {
+  Context* ctx = ctx_of(context);
+  const int64_t A = ctx->ao_basis.ao_num, M = ctx->mo_basis.mo_num;
   if (ds->tc3_coef_version != ctx->mo_basis.coef_version || !ds->tc3_coef.p) {
     TcPlan plan = tc_plan(A, M, 3);
     qmckl_exit_code rc = ensure(context, ds->tc3_coef, plan.coef_bytes, "qmckl_b200_mo_mixed");
@@ -619,10 +773,9 @@ qmckl_exit_code run_mo_mixed(qmckl_context context, DeviceState* ds, int64_t P, 
   if (rc0 != QMCKL_SUCCESS) return rc0;
   const int NN = (int)ctx->nucleus.num, MM = (int)ctx->mo_basis.mo_num;
   if (ds->fused) {
-    bool ok = ds->krec.p != nullptr && ds->krec_basis_version == ctx->ao_basis.basis_version &&
-              ds->krec_nucl_version == ctx->nucleus.coord_version &&
-              ds->krec_cusp_version == ctx->mo_basis.cusp_version;
-    if (!ok) ok = build_krec(context, ds);
+    bool ok = false;
+    rc0 = prepare_fused(context, ds, &ok);
+    if (rc0 != QMCKL_SUCCESS) return rc0;
     if (ok && tc_fused_smem(ds->tc, comps, ds->rec_bytes) <= 232448) {
       // spatial order of the points, then the fused AO -> MO kernel (the AO
       // pieces never leave shared memory)
@@ -653,7 +806,7 @@ qmckl_exit_code run_mo_mixed(qmckl_context context, DeviceState* ds, int64_t P, 
         double* o = out + a * comps * M;
         QB_CUDA(point_order(coord + a, n, lo, hi, keys, counts, perm, ds->stream, P), "qmckl_b200_mo_mixed");
         QB_CUDA(tc_run_fused(ds->T, ds->tc, n, comps, coord + a, cutoff_of(ctx), ds->tc_coef.p, ds->krec.p,
-                             ds->rec_bytes, perm, rb, o, ds->stream, P),
+                             ds->rec_bytes, perm, rb, o, ds->stream, P, ds->kskip.p),
                 "qmckl_b200_mo_mixed");
         if (cr != nullptr)
           QB_CUDA(launch_cusp_mo(n, comps, coord + a, P, NN, (const double*)ds->nucl.p, cr, cprm, MM, o, ds->stream),
@@ -752,7 +905,7 @@ void dev_detach(Context* ctx) {
                     &ds->mo_vgl, &ds->mo_value, &ds->coef_t, &ds->tc_coef, &ds->tc_a, &ds->krec, &ds->order,
                     &ds->ao_hessian, &ds->coef_rows, &ds->adj_coord, &ds->adj_buf, &ds->adj_part, &ds->adj_nucl,
                     &ds->tc3_coef, &ds->env, &ds->nuc_ao, &ds->forces, &ds->adj_wp, &ds->adj_ct, &ds->adj_err,
-                    &ds->cusp, &ds->ao_masked, &ds->en_dist, &ds->mo_hessian})
+                    &ds->cusp, &ds->ao_masked, &ds->en_dist, &ds->mo_hessian, &ds->kskip})
     release(*b);
   if (ds->copy_stream) {
     cudaStreamSynchronize(ds->copy_stream);

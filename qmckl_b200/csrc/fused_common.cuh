@@ -279,7 +279,15 @@ __device__ __forceinline__ void produce_kblock(const uint8_t* rec, const double*
 // accumulator 0 (first K half) or 1 (second half), corrections into 2.
 template <int PIECES>
 __device__ __forceinline__ void mma_kblock(uint32_t base, uint32_t a_bytes, uint32_t b_tile, uint32_t tmem,
-                                           int n_tile, uint32_t idesc, int kb, int kblocks) {
+                                           int n_tile, uint32_t idesc, int kb, int kblocks, int first_lo = 0,
+                                           int first_hi = -1, int first_any = 0) {
+  // kb: this K block; the leading product goes to accumulator 0 for the
+  // first half of the K blocks (2 kb < kblocks), to accumulator 1 for the
+  // second half, whatever blocks a tile skips, so that a row's sums never
+  // depend on the other rows of its tile.  first_lo / first_hi / first_any:
+  // the first block of the first half, of the second half and overall that
+  // the tile evaluates (they overwrite instead of accumulating).
+  if (first_hi < 0) first_hi = (kblocks + 1) / 2;
   constexpr int NPROD = PIECES == 3 ? 6 : 3;
   constexpr int pa3[6] = {2, 1, 0, 1, 0, 0}, pb3[6] = {0, 1, 2, 0, 1, 0};
   constexpr int pa2[3] = {1, 0, 0}, pb2[3] = {0, 1, 0};
@@ -293,8 +301,8 @@ __device__ __forceinline__ void mma_kblock(uint32_t base, uint32_t a_bytes, uint
       const bool lead = (t == NPROD - 1);
       const bool second = lead && (2 * kb >= kblocks);
       const uint32_t d = tmem + (uint32_t)((lead ? (second ? 1 : 0) : 2) * n_tile);
-      const bool first_use = lead ? (second ? (kb == (kblocks + 1) / 2 && kk == 0) : (kb == 0 && kk == 0))
-                                  : (kb == 0 && kk == 0 && t == 0);
+      const bool first_use = lead ? (second ? (kb == first_hi && kk == 0) : (kb == first_lo && kk == 0))
+                                  : (kb == first_any && kk == 0 && t == 0);
       umma_bf16(d, smem_desc(a_addr), smem_desc(b_addr), idesc, first_use ? 0u : 1u);
     }
   }
@@ -318,7 +326,7 @@ template <int PIECES, int COMPS>
 __device__ __forceinline__ void epilogue_warp(uint32_t tmem, int n_tile, int n0, int n_out, bool has_second,
                                               const int64_t* pidx, const int* rexp, const double* scales,
                                               double* out, double* stage, int warp, int lane, int chunk0 = 0,
-                                              int chunk_step = 1) {
+                                              int chunk_step = 1, bool has_first = true) {
   constexpr int PTS = BM / COMPS;
   const int row_base = (warp & 3) * 32;   // a warp reads the TMEM lanes of its quadrant
   for (int c0 = 16 * chunk0; c0 < n_tile; c0 += 16 * chunk_step) {
@@ -329,7 +337,8 @@ __device__ __forceinline__ void epilogue_warp(uint32_t tmem, int n_tile, int n0,
     tmem_ld16(ta + (uint32_t)(2 * n_tile), r2);
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
-      double v = (double)__uint_as_float(r0[j]) + (double)__uint_as_float(r2[j]);
+      double v = has_first ? (double)__uint_as_float(r0[j]) + (double)__uint_as_float(r2[j])
+                           : (double)__uint_as_float(r2[j]);
       if (has_second) v += (double)__uint_as_float(r1[j]);
       stage[lane * 16 + ((j + lane) & 15)] = v;
     }

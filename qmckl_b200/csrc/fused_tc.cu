@@ -32,13 +32,22 @@ constexpr int kMmaWarp = kProdWarps + 1;
 constexpr int kThreadsF = (kProdWarps + 2) * 32;
 constexpr int STAGES = 2;
 
+// Tile skipping: kskip (optional) holds int2 kb_sh[kblocks] (the range of
+// shell spheres of each K block) and, from byte kskip_sph_offset(kblocks) on,
+// double4 sph[] (nucleus of the shell, squared radius beyond which its AOs
+// vanish in the producers; see shell_r2max in device.cu).  A K block whose
+// shells are all beyond their radius at every point of the tile contributes
+// exact zeros and is left out of the producer, TMA and MMA loops.
+__host__ __device__ constexpr int kskip_sph_offset(int kblocks) { return (kblocks * 8 + 31) / 32 * 32; }
+
 template <int PIECES, int COMPS>
 __global__ void __launch_bounds__(kThreadsF, 1)
 fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, const int64_t P,
                 const double* __restrict__ coord, const double cutoff, const int n_out, const int n_tile,
                 const int kblocks, const uint8_t* __restrict__ krec, const int rec_bytes,
                 const int* __restrict__ perm, const double* __restrict__ scales, const RowBound rb,
-                double* __restrict__ out, int* __restrict__ err, const int64_t cstride) {
+                double* __restrict__ out, int* __restrict__ err, const int64_t cstride,
+                const uint8_t* __restrict__ kskip) {
   constexpr int PTS = BM / COMPS;            // 25 points (VGL) or 128 (value)
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   // 1024-byte aligned base, kept as pointer arithmetic on the __shared__
@@ -56,6 +65,9 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
   double* pts = (double*)(acc_full + 2);      // [3][PTS]
   int64_t* pidx = (int64_t*)(pts + 3 * PTS);  // [PTS] original index of each tile point
   int* rexp = (int*)(pidx + PTS);             // [3][PTS] row scale exponents (2 pieces)
+  int* act = rexp + 3 * PTS;                  // [kblocks] the K blocks of this tile, [kblocks] flags,
+  int* kflag = act + kblocks;                 // then: count, first block of each half, first block
+  int* nact_p = kflag + kblocks;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int64_t p0 = (int64_t)blockIdx.x * PTS;
@@ -79,9 +91,50 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
     if (d == 0) pidx[i] = q;
     rexp[t] = PIECES == 2 ? kExpMin : 0;
   }
-  if (PIECES == 2) {
-    __syncthreads();
-    row_exponents<PTS>(rb, pts, pidx, rexp, tid, kThreadsF);
+  __syncthreads();
+  if (PIECES == 2) row_exponents<PTS>(rb, pts, pidx, rexp, tid, kThreadsF);
+  // K blocks that are not identically zero over the tile's points
+  {
+    const int2* kb_sh = (const int2*)kskip;
+    const double4* sph = (const double4*)(kskip + kskip_sph_offset(kblocks));
+    for (int kb = warp; kb < kblocks; kb += kThreadsF / 32) {
+      bool live = kskip == nullptr;
+      if (!live) {
+        const int2 r = kb_sh[kb];
+        for (int g = 0; g < (PTS + 31) / 32; ++g) {
+          const int i = lane + 32 * g;
+          if (i < PTS && p0 + i < P) {
+            const double px = pts[i], py = pts[PTS + i], pz = pts[2 * PTS + i];
+            for (int q = r.x; q < r.y && !live; ++q) {
+              const double4 c = sph[q];
+              const double x = px - c.x, y = py - c.y, z = pz - c.z;
+              live = x * x + y * y + z * z <= c.w;
+            }
+          }
+        }
+      }
+      live = __any_sync(0xffffffffu, live);
+      if (lane == 0) kflag[kb] = live ? 1 : 0;
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int n = 0;
+    int lo = -1, hi = -1;
+    for (int kb = 0; kb < kblocks; ++kb)
+      if (kflag[kb]) {
+        act[n++] = kb;
+        if (2 * kb >= kblocks) { if (hi < 0) hi = kb; }
+        else if (lo < 0) lo = kb;
+      }
+    if (n == 0) {   // all outputs zero: one (zero) block initialises the accumulators
+      act[n++] = 0;
+      lo = 0;
+    }
+    nact_p[0] = n;
+    nact_p[1] = lo;   // -1: no block of the first half (accumulator 0 unused)
+    nact_p[2] = hi;   // -1: none of the second half
+    nact_p[3] = act[0];
   }
   // rows PTS*COMPS .. 127 of the A tiles stay zero for the whole kernel
   zero_pad_rows<PIECES, COMPS, STAGES>(smem, STAGE, tid, kThreadsF);
@@ -95,14 +148,15 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
+  const int nact = *nact_p;
 
   if (warp < kProdWarps) {
     // ---------------- AO producers: warp w owns AOs [4w, 4w+4) of each K block,
     // its lanes are the tile's points (uniform control flow within the warp)
     const int j = warp;
-    for (int kb = 0; kb < kblocks; ++kb) {
-      const int s = kb & 1;
-      const uint32_t phase = (uint32_t)(kb >> 1) & 1u;
+    for (int it = 0; it < nact; ++it) {
+      const int s = it & 1;
+      const uint32_t phase = (uint32_t)(it >> 1) & 1u;
       // warp-uniform outcome: every lane must take the same path
       bool ok = mbar_wait(&empty[s], phase ^ 1u, err, 11);
       ok = ok && mbar_wait(&rec_full[s], phase, err, 15);
@@ -115,9 +169,10 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
   } else if (warp == kTmaWarp) {
     // ---------------- coefficient pieces
     if (lane == 0) {
-      for (int kb = 0; kb < kblocks; ++kb) {
-        const int s = kb & 1;
-        const uint32_t phase = (uint32_t)(kb >> 1) & 1u;
+      for (int it = 0; it < nact; ++it) {
+        const int kb = act[it];
+        const int s = it & 1;
+        const uint32_t phase = (uint32_t)(it >> 1) & 1u;
         if (!mbar_wait(&empty[s], phase ^ 1u, err, 12)) break;
         mbar_expect_tx(&rec_full[s], (uint32_t)rec_bytes);
         bulk_load(recs + s * rec_bytes, krec + (size_t)kb * rec_bytes, (uint32_t)rec_bytes, &rec_full[s]);
@@ -130,13 +185,13 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
     // ---------------- MMA issuer
     if (lane == 0) {
       const uint32_t idesc = mma_idesc<PIECES>(n_tile);
-      for (int kb = 0; kb < kblocks; ++kb) {
-        const int s = kb & 1;
-        const uint32_t phase = (uint32_t)(kb >> 1) & 1u;
+      for (int it = 0; it < nact; ++it) {
+        const int s = it & 1;
+        const uint32_t phase = (uint32_t)(it >> 1) & 1u;
         if (!mbar_wait(&full[s], phase, err, 13)) break;
         tc_fence_after();
-        mma_kblock<PIECES>(smem_addr(smem + s * STAGE), (uint32_t)A_BYTES, (uint32_t)B_TILE, tmem, n_tile, idesc, kb,
-                           kblocks);
+        mma_kblock<PIECES>(smem_addr(smem + s * STAGE), (uint32_t)A_BYTES, (uint32_t)B_TILE, tmem, n_tile, idesc,
+                           act[it], kblocks, nact_p[1], nact_p[2] < 0 ? kblocks : nact_p[2], nact_p[3]);
         umma_commit(&empty[s]);
       }
       umma_commit(acc_full);
@@ -150,8 +205,9 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
     ok = __all_sync(0xffffffffu, ok && *(volatile int*)err == 0);
     tc_fence_after();
     if (ok)
-      epilogue_warp<PIECES, COMPS>(tmem, n_tile, n0, n_out, kblocks >= 2, pidx, rexp, scales, out,
-                                   (double*)smem + warp * 32 * 16, warp, lane, warp >> 2, kProdWarps / 4);
+      epilogue_warp<PIECES, COMPS>(tmem, n_tile, n0, n_out, nact_p[2] >= 0, pidx, rexp, scales, out,
+                                   (double*)smem + warp * 32 * 16, warp, lane, warp >> 2, kProdWarps / 4,
+                                   nact_p[1] >= 0);
   }
   tc_fence_before();
   __syncthreads();
@@ -187,25 +243,26 @@ int* fused_err_word() {
 }
 
 template <int PIECES, int COMPS>
-size_t fused_smem(int n_tile, int rec_bytes) {
+size_t fused_smem(int n_tile, int rec_bytes, int kblocks) {
   constexpr int PTS = BM / COMPS;
   const size_t stage = (size_t)PIECES * (A_TILE + (size_t)n_tile * BK * 2);
-  return 1024 + STAGES * stage + (size_t)STAGES * rec_bytes + (3 * STAGES + 2) * 8 + 4 * PTS * 8 + 3 * PTS * 4 + 16;
+  return 1024 + STAGES * stage + (size_t)STAGES * rec_bytes + (3 * STAGES + 2) * 8 + 4 * PTS * 8 + 3 * PTS * 4 +
+         (size_t)(2 * kblocks + 4) * 4 + 16;
 }
 
 template <int PIECES, int COMPS>
 cudaError_t launch_fused(const DevTables& T, const CUtensorMap& tb, int64_t P, const double* coord, double cutoff,
                          int n_out, int n_tile, int n_tiles, int kblocks, const uint8_t* krec, int rec_bytes,
                          const int* perm, const double* scales, const RowBound& rb, double* out, int* err,
-                         int64_t cstride, cudaStream_t s) {
+                         int64_t cstride, const uint8_t* kskip, cudaStream_t s) {
   constexpr int PTS = BM / COMPS;
-  const size_t smem = fused_smem<PIECES, COMPS>(n_tile, rec_bytes);
+  const size_t smem = fused_smem<PIECES, COMPS>(n_tile, rec_bytes, kblocks);
   auto kern = fused_mo_kernel<PIECES, COMPS>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid((unsigned)((P + PTS - 1) / PTS), (unsigned)n_tiles);
   kern<<<grid, kThreadsF, smem, s>>>(T, tb, P, coord, cutoff, n_out, n_tile, kblocks, krec, rec_bytes, perm, scales,
-                                     rb, out, err, cstride);
+                                     rb, out, err, cstride, kskip);
   count_launch();
   return cudaGetLastError();
 }
@@ -213,8 +270,15 @@ cudaError_t launch_fused(const DevTables& T, const CUtensorMap& tb, int64_t P, c
 }  // namespace
 
 size_t tc_fused_smem(const TcPlan& plan, int comps, int rec_bytes) {
-  if (plan.pieces == 3) return comps == 5 ? fused_smem<3, 5>(plan.n_tile, rec_bytes) : fused_smem<3, 1>(plan.n_tile, rec_bytes);
-  return comps == 5 ? fused_smem<2, 5>(plan.n_tile, rec_bytes) : fused_smem<2, 1>(plan.n_tile, rec_bytes);
+  const int kb = (int)((plan.ao_num + BK - 1) / BK);
+  if (plan.pieces == 3)
+    return comps == 5 ? fused_smem<3, 5>(plan.n_tile, rec_bytes, kb) : fused_smem<3, 1>(plan.n_tile, rec_bytes, kb);
+  return comps == 5 ? fused_smem<2, 5>(plan.n_tile, rec_bytes, kb) : fused_smem<2, 1>(plan.n_tile, rec_bytes, kb);
+}
+
+size_t tc_kskip_bytes(int64_t ao_num, int64_t shell_num) {
+  const int kb = (int)((ao_num + BK - 1) / BK);
+  return (size_t)kskip_sph_offset(kb) + sizeof(double4) * (size_t)shell_num;
 }
 
 cudaError_t tc_encode_coef_map(const TcPlan& plan, const void* d_coef, CUtensorMap* map) {
@@ -232,7 +296,8 @@ cudaError_t tc_encode_coef_map(const TcPlan& plan, const void* d_coef, CUtensorM
 
 cudaError_t tc_launch_fused(const TcPlan& plan, int64_t point_num, int comps, const double* coord, double cutoff,
                             const CUtensorMap& tb, const void* krec, int rec_bytes, const int* perm, const void* d_coef,
-                            const RowBound& rb, double* out, int* err, cudaStream_t s, int64_t cstride) {
+                            const RowBound& rb, double* out, int* err, cudaStream_t s, int64_t cstride,
+                            const void* kskip) {
   if (point_num <= 0) return cudaSuccess;
   if (cstride < point_num) cstride = point_num;
   if (rec_bytes <= 0 || rec_bytes % 128 != 0) return cudaErrorInvalidValue;
@@ -241,20 +306,21 @@ cudaError_t tc_launch_fused(const TcPlan& plan, int64_t point_num, int comps, co
   const uint8_t* kr = (const uint8_t*)krec;
   const int M = (int)plan.mo_num;
   const double* sc = tc_scales(plan, d_coef);
+  const uint8_t* ks = (const uint8_t*)kskip;
   if (plan.pieces == 3)
     return comps == 5 ? launch_fused<3, 5>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
-                                           rec_bytes, perm, sc, rb, out, err, cstride, s)
+                                           rec_bytes, perm, sc, rb, out, err, cstride, ks, s)
                       : launch_fused<3, 1>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
-                                           rec_bytes, perm, sc, rb, out, err, cstride, s);
+                                           rec_bytes, perm, sc, rb, out, err, cstride, ks, s);
   return comps == 5 ? launch_fused<2, 5>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
-                                         rec_bytes, perm, sc, rb, out, err, cstride, s)
+                                         rec_bytes, perm, sc, rb, out, err, cstride, ks, s)
                     : launch_fused<2, 1>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
-                                         rec_bytes, perm, sc, rb, out, err, cstride, s);
+                                         rec_bytes, perm, sc, rb, out, err, cstride, ks, s);
 }
 
 cudaError_t tc_run_fused(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps, const double* coord,
                          double cutoff, const void* d_coef, const void* krec, int rec_bytes, const int* perm,
-                         const RowBound& rb, double* out, cudaStream_t s, int64_t cstride) {
+                         const RowBound& rb, double* out, cudaStream_t s, int64_t cstride, const void* kskip) {
   (void)T;
   if (point_num <= 0) return cudaSuccess;
   CUtensorMap tb;
@@ -262,7 +328,8 @@ cudaError_t tc_run_fused(const DevTables& T, const TcPlan& plan, int64_t point_n
   if (e != cudaSuccess) return e;
   int* err = fused_err_word();
   if (!err) return cudaErrorMemoryAllocation;
-  e = tc_launch_fused(plan, point_num, comps, coord, cutoff, tb, krec, rec_bytes, perm, d_coef, rb, out, err, s, cstride);
+  e = tc_launch_fused(plan, point_num, comps, coord, cutoff, tb, krec, rec_bytes, perm, d_coef, rb, out, err, s, cstride,
+                      kskip);
   if (e != cudaSuccess) return e;
   int h = 0;
   e = cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s);

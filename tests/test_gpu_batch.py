@@ -1,8 +1,9 @@
 """Batched MO VGL: many independent systems in one persistent launch.
 
-* every system's slice of the batched result equals the single-system mixed
-  evaluation of its own context (same arithmetic per point: the tiling and
-  point order do not enter a row's value);
+* every system's slice of the batched result agrees with the single-system
+  mixed evaluation of its own context to the mixed-form bound (the
+  single-system fused kernel contracts the AOs in its own K order, see
+  fused_tc.cu, so the two differ by rounding);
 * the per-system launch loop gives the same numbers;
 * every (producer warps, queue order) variant of the autotuner gives the same
   numbers, the tuner's choice is written to and read back from the tuning
@@ -89,7 +90,7 @@ def _check_equal_single(case, out):
             continue
         ref = _single(case, s)
         got = _slice(case, out, s)
-        assert np.abs(got - ref).max() <= 1e-13 * np.abs(ref).max(), s
+        assert max(comp_error(got, ref)) <= 1e-6, s
 
 
 def test_batch_matches_single_system(batch_case):

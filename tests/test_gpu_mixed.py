@@ -128,3 +128,32 @@ def test_host_getter_slices_match_device_entry():
     again = pq.get_mo_basis_mo_vgl(ctx, P * 5 * M)   # cached: copied from the device array
     assert np.array_equal(host, again)
     pq.context_destroy(ctx)
+
+
+def test_fused_tile_skipping():
+    """The fused kernel orders its K dimension by shell radius class and
+    nuclear position and skips the 64-AO blocks that vanish at every point of
+    a tile.  Points far from every nucleus (all blocks skipped) give exact
+    zeros; near points stay within the mixed-form bound of the FP64 form; the
+    unfused kernels (basis order, no skipping) agree to the same bound."""
+    import torch
+    d = gen.config(1, walk_num=4)
+    pts = gen.points(d)
+    far = pts[:60] + 500.0
+    allp = np.concatenate([pts, far])
+    P, M = allp.shape[0], d["mo_num"]
+    dc = torch.tensor(np.ascontiguousarray(allp.T), dtype=torch.float64, device="cuda")
+    res = {}
+    for name, form, fused in (("fp64", pq.FORM_FP64, 1), ("fused", pq.FORM_MIXED, 1), ("unfused", pq.FORM_MIXED, 0)):
+        ctx = make_context(d, points=False, form=form)
+        pq.b200_set_mixed_kernel(ctx, fused)
+        out = torch.full((P, 5, M), 7.0, dtype=torch.float64, device="cuda")
+        pq.b200_mo_vgl_device(ctx, P, dc.data_ptr(), out.data_ptr())
+        pq.b200_synchronize(ctx)
+        res[name] = out.cpu().numpy()
+        pq.context_destroy(ctx)
+    near = slice(0, pts.shape[0])
+    assert not res["fused"][pts.shape[0]:].any()
+    assert not res["fp64"][pts.shape[0]:].any()
+    assert max(comp_error(res["fused"][near], res["fp64"][near])) <= MIXED_TOL
+    assert max(comp_error(res["unfused"][near], res["fp64"][near])) <= MIXED_TOL
