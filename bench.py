@@ -417,6 +417,9 @@ def main():
     sampler = ClockSampler(local)
     sampler.start()
     launches0 = pq.b200_kernel_launch_count()
+    fused_path = form == pq.FORM_MIXED and not args.unfused
+    if fused_path:
+        pq.b200_get_kblock_stats(ctx, reset=True)
     times = []
     for _ in range(args.steps):
         flush.zero_()
@@ -429,6 +432,7 @@ def main():
         times.append(e0.elapsed_time(e1))
     torch.cuda.synchronize()
     launches = pq.b200_kernel_launch_count() - launches0
+    kb_eval, kb_total = pq.b200_get_kblock_stats(ctx) if fused_path else (0, 0)
     # dominant-kernel timing: the AO kernel alone (same stream, same events)
     ao_times = []
     if form == pq.FORM_FP64:
@@ -489,20 +493,24 @@ def main():
                                      "ms_per_launch": ms - ao_ms,
                                      "tflops": 2.0 * 5 * P * A * M / ((ms - ao_ms) * 1e-3) / 1e12}}
     else:
-        # fused kernel: 25 points x 5 components per 128-row MMA tile, MOs
-        # padded to 16, AOs to 64; 6 split-BF16 products per K step
+        # fused kernel: 25 points x 5 components per 128-row MMA tile, MOs in
+        # N tiles of n_tile columns, 64-AO K blocks (those that vanish over a
+        # tile are skipped: the kernel counts the blocks it evaluates);
+        # 6 split-BF16 products (3 for float16 x 2) per K step
         flops = 2.0 * 5 * P * A * M
-        tiles = -(-P // 25)
-        n_pad = -(-M // 16) * 16 if M <= 160 else M
-        k_pad = -(-A // 64) * 64
+        n_tiles = -(-M // 256)
+        n_tile = -(-(-(-M // n_tiles)) // 16) * 16
+        while n_tile > 160:
+            n_tiles += 1
+            n_tile = -(-(-(-M // n_tiles)) // 16) * 16
         nprod = 6 if args.pieces == 3 else 3
-        executed = 2.0 * tiles * 128 * n_pad * k_pad * nprod
+        executed = 2.0 * (kb_eval / args.steps) * 128 * n_tile * 64 * nprod
         t = traffic.get(("fused_mo_kernel", "mixed"))
         kname = ("fused_mo_kernel<3,5> (AO -> split-BF16 tcgen05 MO VGL" if args.pieces == 3 else
                  "fused_mo_kernel<2,5> (AO -> split-FP16 tcgen05 MO VGL") + "; step = 3 ordering kernels + this)"
         if args.unfused:
             # AO pieces to HBM, then 128-row tiles of the 5P x A pieces matrix x 6 products
-            executed = 2.0 * (-(-5 * P // 128) * 128) * n_pad * k_pad * 6
+            executed = 2.0 * (-(-5 * P // 128) * 128) * (n_tile * n_tiles) * (-(-A // 64) * 64) * 6
             kname = "ao_tile_kernel<3,5> + tc_gemm_kernel<3,2> (unfused mixed form; whole step)"
             t = None
         achieved = executed / (ms * 1e-3) / 1e12
@@ -513,6 +521,7 @@ def main():
                     "traffic_note": "ncu dram bytes of a 20,352-point launch scaled by points" if t else None,
                     "executed_tensor_flop_per_launch": executed,
                     "dense_equivalent_tflops": flops / (ms * 1e-3) / 1e12,
+                    "k_blocks_evaluated_fraction": (kb_eval / kb_total) if kb_total else None,
                     "output_bytes_per_launch": 40.0 * P * M}
 
     value = world * P / (ms * 1e-3)

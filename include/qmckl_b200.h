@@ -168,6 +168,14 @@ qmckl_exit_code qmckl_b200_batch_set_wait_limit(qmckl_b200_batch batch, const in
 qmckl_exit_code qmckl_b200_mo_vgl_device_noalloc(qmckl_context context, const int64_t point_num,
                                                  const double* d_coord, double* d_mo_vgl);
 
+/* Tile skipping of the fused mixed-form kernel: K blocks (64 AOs) it
+ * evaluated and K blocks of the dense contraction, summed over its launches
+ * (one count per CTA: tile of points x MO tile) since the context's first
+ * fused evaluation or the last reset (reset != 0 clears them after reading).
+ * Both 0 before any fused evaluation.  Synchronizes the context's stream. */
+qmckl_exit_code qmckl_b200_get_kblock_stats(qmckl_context context, int64_t* evaluated, int64_t* total,
+                                           const int32_t reset);
+
 /* Number of kernels this library launched since the process started. */
 int64_t qmckl_b200_kernel_launch_count(void);
 

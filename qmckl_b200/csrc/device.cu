@@ -339,7 +339,7 @@ struct DeviceState {
   // fused kernel: K order (AO at each K position; the coefficient pieces of
   // the fused plan follow it), tile-skipping tables, cutoff they were built for
   std::vector<int64_t> fused_perm;
-  DevBuf kskip;
+  DevBuf kskip, kstat;   // kstat: K blocks evaluated / dense, summed over the fused launches
   double krec_cutoff = -1.0;
 };
 
@@ -713,6 +713,11 @@ qmckl_exit_code prepare_fused(qmckl_context context, DeviceState* ds, bool* usab
     }
   }
   if (!fits(ds->rec_bytes)) return QMCKL_SUCCESS;
+  if (ds->kstat.p == nullptr) {
+    qmckl_exit_code rc = ensure(context, ds->kstat, 2 * sizeof(unsigned long long), fname);
+    if (rc != QMCKL_SUCCESS) return rc;
+    QB_CUDA(cudaMemsetAsync(ds->kstat.p, 0, 2 * sizeof(unsigned long long), ds->stream), fname);
+  }
   if (ds->tc_coef_version != ctx->mo_basis.coef_version || ds->tc_pieces != pieces || !ds->tc_coef.p) {
     // coefficient columns in the K order of the records
     std::vector<double> cp((size_t)(M * A));
@@ -806,7 +811,8 @@ qmckl_exit_code run_mo_mixed(qmckl_context context, DeviceState* ds, int64_t P, 
         double* o = out + a * comps * M;
         QB_CUDA(point_order(coord + a, n, lo, hi, keys, counts, perm, ds->stream, P), "qmckl_b200_mo_mixed");
         QB_CUDA(tc_run_fused(ds->T, ds->tc, n, comps, coord + a, cutoff_of(ctx), ds->tc_coef.p, ds->krec.p,
-                             ds->rec_bytes, perm, rb, o, ds->stream, P, ds->kskip.p),
+                             ds->rec_bytes, perm, rb, o, ds->stream, P, ds->kskip.p,
+                             (unsigned long long*)ds->kstat.p),
                 "qmckl_b200_mo_mixed");
         if (cr != nullptr)
           QB_CUDA(launch_cusp_mo(n, comps, coord + a, P, NN, (const double*)ds->nucl.p, cr, cprm, MM, o, ds->stream),
@@ -905,7 +911,7 @@ void dev_detach(Context* ctx) {
                     &ds->mo_vgl, &ds->mo_value, &ds->coef_t, &ds->tc_coef, &ds->tc_a, &ds->krec, &ds->order,
                     &ds->ao_hessian, &ds->coef_rows, &ds->adj_coord, &ds->adj_buf, &ds->adj_part, &ds->adj_nucl,
                     &ds->tc3_coef, &ds->env, &ds->nuc_ao, &ds->forces, &ds->adj_wp, &ds->adj_ct, &ds->adj_err,
-                    &ds->cusp, &ds->ao_masked, &ds->en_dist, &ds->mo_hessian, &ds->kskip})
+                    &ds->cusp, &ds->ao_masked, &ds->en_dist, &ds->mo_hessian, &ds->kskip, &ds->kstat})
     release(*b);
   if (ds->copy_stream) {
     cudaStreamSynchronize(ds->copy_stream);
@@ -1282,6 +1288,25 @@ using namespace qb;
 extern "C" {
 
 int64_t qmckl_b200_kernel_launch_count(void) { return g_launches.load(); }
+
+qmckl_exit_code qmckl_b200_get_kblock_stats(qmckl_context context, int64_t* evaluated, int64_t* total,
+                                           const int32_t reset) {
+  const char* fname = "qmckl_b200_get_kblock_stats";
+  if (qmckl_context_check(context) == QMCKL_NULL_CONTEXT) return QMCKL_INVALID_CONTEXT;
+  if (evaluated == nullptr) return qmckl_failwith(context, QMCKL_INVALID_ARG_2, fname, "NULL pointer");
+  if (total == nullptr) return qmckl_failwith(context, QMCKL_INVALID_ARG_3, fname, "NULL pointer");
+  *evaluated = *total = 0;
+  DeviceState* ds = state(context);
+  if (ds == nullptr || ds->kstat.p == nullptr) return QMCKL_SUCCESS;
+  if (ds->device >= 0) QB_CUDA(cudaSetDevice(ds->device), fname);
+  unsigned long long h[2] = {0, 0};
+  QB_CUDA(cudaMemcpyAsync(h, ds->kstat.p, sizeof h, cudaMemcpyDeviceToHost, ds->stream), fname);
+  if (reset) QB_CUDA(cudaMemsetAsync(ds->kstat.p, 0, sizeof h, ds->stream), fname);
+  QB_CUDA(cudaStreamSynchronize(ds->stream), fname);
+  *evaluated = (int64_t)h[0];
+  *total = (int64_t)h[1];
+  return QMCKL_SUCCESS;
+}
 
 qmckl_exit_code qmckl_b200_set_split_terms(qmckl_context context, const int32_t pieces) {
   if (qmckl_context_check(context) == QMCKL_NULL_CONTEXT) return QMCKL_INVALID_CONTEXT;

@@ -47,7 +47,7 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
                 const int kblocks, const uint8_t* __restrict__ krec, const int rec_bytes,
                 const int* __restrict__ perm, const double* __restrict__ scales, const RowBound rb,
                 double* __restrict__ out, int* __restrict__ err, const int64_t cstride,
-                const uint8_t* __restrict__ kskip) {
+                const uint8_t* __restrict__ kskip, unsigned long long* __restrict__ kstat) {
   constexpr int PTS = BM / COMPS;            // 25 points (VGL) or 128 (value)
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   // 1024-byte aligned base, kept as pointer arithmetic on the __shared__
@@ -130,6 +130,10 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
     if (n == 0) {   // all outputs zero: one (zero) block initialises the accumulators
       act[n++] = 0;
       lo = 0;
+    }
+    if (kstat != nullptr) {   // K blocks evaluated / in the dense contraction, summed over CTAs
+      atomicAdd(&kstat[0], (unsigned long long)n);
+      atomicAdd(&kstat[1], (unsigned long long)kblocks);
     }
     nact_p[0] = n;
     nact_p[1] = lo;   // -1: no block of the first half (accumulator 0 unused)
@@ -254,7 +258,7 @@ template <int PIECES, int COMPS>
 cudaError_t launch_fused(const DevTables& T, const CUtensorMap& tb, int64_t P, const double* coord, double cutoff,
                          int n_out, int n_tile, int n_tiles, int kblocks, const uint8_t* krec, int rec_bytes,
                          const int* perm, const double* scales, const RowBound& rb, double* out, int* err,
-                         int64_t cstride, const uint8_t* kskip, cudaStream_t s) {
+                         int64_t cstride, const uint8_t* kskip, unsigned long long* kstat, cudaStream_t s) {
   constexpr int PTS = BM / COMPS;
   const size_t smem = fused_smem<PIECES, COMPS>(n_tile, rec_bytes, kblocks);
   auto kern = fused_mo_kernel<PIECES, COMPS>;
@@ -262,7 +266,7 @@ cudaError_t launch_fused(const DevTables& T, const CUtensorMap& tb, int64_t P, c
   if (e != cudaSuccess) return e;
   dim3 grid((unsigned)((P + PTS - 1) / PTS), (unsigned)n_tiles);
   kern<<<grid, kThreadsF, smem, s>>>(T, tb, P, coord, cutoff, n_out, n_tile, kblocks, krec, rec_bytes, perm, scales,
-                                     rb, out, err, cstride, kskip);
+                                     rb, out, err, cstride, kskip, kstat);
   count_launch();
   return cudaGetLastError();
 }
@@ -297,7 +301,7 @@ cudaError_t tc_encode_coef_map(const TcPlan& plan, const void* d_coef, CUtensorM
 cudaError_t tc_launch_fused(const TcPlan& plan, int64_t point_num, int comps, const double* coord, double cutoff,
                             const CUtensorMap& tb, const void* krec, int rec_bytes, const int* perm, const void* d_coef,
                             const RowBound& rb, double* out, int* err, cudaStream_t s, int64_t cstride,
-                            const void* kskip) {
+                            const void* kskip, unsigned long long* kstat) {
   if (point_num <= 0) return cudaSuccess;
   if (cstride < point_num) cstride = point_num;
   if (rec_bytes <= 0 || rec_bytes % 128 != 0) return cudaErrorInvalidValue;
@@ -309,18 +313,19 @@ cudaError_t tc_launch_fused(const TcPlan& plan, int64_t point_num, int comps, co
   const uint8_t* ks = (const uint8_t*)kskip;
   if (plan.pieces == 3)
     return comps == 5 ? launch_fused<3, 5>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
-                                           rec_bytes, perm, sc, rb, out, err, cstride, ks, s)
+                                           rec_bytes, perm, sc, rb, out, err, cstride, ks, kstat, s)
                       : launch_fused<3, 1>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
-                                           rec_bytes, perm, sc, rb, out, err, cstride, ks, s);
+                                           rec_bytes, perm, sc, rb, out, err, cstride, ks, kstat, s);
   return comps == 5 ? launch_fused<2, 5>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
-                                         rec_bytes, perm, sc, rb, out, err, cstride, ks, s)
+                                         rec_bytes, perm, sc, rb, out, err, cstride, ks, kstat, s)
                     : launch_fused<2, 1>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
-                                         rec_bytes, perm, sc, rb, out, err, cstride, ks, s);
+                                         rec_bytes, perm, sc, rb, out, err, cstride, ks, kstat, s);
 }
 
 cudaError_t tc_run_fused(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps, const double* coord,
                          double cutoff, const void* d_coef, const void* krec, int rec_bytes, const int* perm,
-                         const RowBound& rb, double* out, cudaStream_t s, int64_t cstride, const void* kskip) {
+                         const RowBound& rb, double* out, cudaStream_t s, int64_t cstride, const void* kskip,
+                         unsigned long long* kstat) {
   (void)T;
   if (point_num <= 0) return cudaSuccess;
   CUtensorMap tb;
@@ -329,7 +334,7 @@ cudaError_t tc_run_fused(const DevTables& T, const TcPlan& plan, int64_t point_n
   int* err = fused_err_word();
   if (!err) return cudaErrorMemoryAllocation;
   e = tc_launch_fused(plan, point_num, comps, coord, cutoff, tb, krec, rec_bytes, perm, d_coef, rb, out, err, s, cstride,
-                      kskip);
+                      kskip, kstat);
   if (e != cudaSuccess) return e;
   int h = 0;
   e = cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s);

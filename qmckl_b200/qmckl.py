@@ -351,6 +351,13 @@ def mo_basis_rescale(ctx, factor):
     _call("qmckl_mo_basis_rescale", ctx, C.c_double(factor))
 
 
+def b200_get_kblock_stats(ctx, reset=False):
+    """(evaluated, total) K blocks of the fused kernel's launches since the last reset."""
+    ev, tot = C.c_int64(0), C.c_int64(0)
+    _call("qmckl_b200_get_kblock_stats", ctx, C.byref(ev), C.byref(tot), C.c_int32(1 if reset else 0))
+    return ev.value, tot.value
+
+
 def set_mo_basis_r_cusp(ctx, r_cusp):
     a, p, n = _arr(r_cusp, np.float64)
     _call("qmckl_set_mo_basis_r_cusp", ctx, p, n)

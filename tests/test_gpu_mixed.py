@@ -151,6 +151,13 @@ def test_fused_tile_skipping():
         pq.b200_mo_vgl_device(ctx, P, dc.data_ptr(), out.data_ptr())
         pq.b200_synchronize(ctx)
         res[name] = out.cpu().numpy()
+        if name == "fused":
+            ev, tot = pq.b200_get_kblock_stats(ctx, reset=True)
+            # one count per CTA: ceil(P / 25) tiles x 1 MO tile, 32 K blocks each; the
+            # far points' tiles evaluate one (zero) block
+            assert tot == -(-P // 25) * 32
+            assert 0 < ev < tot
+            assert pq.b200_get_kblock_stats(ctx) == (0, 0)
         pq.context_destroy(ctx)
     near = slice(0, pts.shape[0])
     assert not res["fused"][pts.shape[0]:].any()
