@@ -56,6 +56,15 @@ __device__ __forceinline__ void monomial_vgl(int a, int b, int c, R x, R y, R z,
   out[4] = R(a - 1) * pa2 * yz + R(b - 1) * pb2 * xz + R(c - 1) * pc2 * xy;
 }
 
+// x^n, x^(n-1) and x^(n-2) for 0 <= n <= 3 without branches; a missing power
+// is 1 (it is multiplied by n or n - 1 = 0).
+__device__ __forceinline__ void pows3(double x, int n, double& p0, double& p1, double& p2) {
+  const double f1 = n >= 1 ? x : 1.0, f2 = n >= 2 ? x : 1.0, f3 = n >= 3 ? x : 1.0;
+  p2 = f3;
+  p1 = f2 * f3;
+  p0 = f1 * p1;
+}
+
 struct WarpSmem {
   double rad[kBlockSlots][5];   // radial VGL of the block's shells
   double nuc[kBlockNuc][4];     // x, y, z displacement, r^2 (negative when screened out)
@@ -68,14 +77,14 @@ __device__ __forceinline__ void shell_radial(const DevTables& T, int slot, int n
                                              double out[5]) {
   double acc[5] = {0., 0., 0., 0., 0.};
   const int2 cr = T.slot_coef[slot];
-  const int p0 = T.nuc_prim_start[nucl];
+  (void)nucl;
   for (int j = cr.x; j < cr.y; ++j) {
-    const int ip = T.coef_prim[j];
-    const double a = T.expo[p0 + ip];
+    const double2 ac = T.coef_ac[j];
+    const double a = ac.x;
     const double ar2 = a * r2;
     if (ar2 > cutoff) break;   // primitives are sorted by exponent
     const double e = dp_exp ? exp(-ar2) : (double)expf(-(float)ar2);
-    const double cv = T.coef_val[j];
+    const double cv = ac.y;
     acc[0] += cv * e;
     if (COMPS == 5) {
       double f = a * e;
@@ -157,26 +166,34 @@ ao_f64_kernel(const DevTables T, const int64_t point_num, const double* __restri
       if (sm.nuc[nl][3] >= 0.0 && s1 != 0.0 && !cusp_masked(cusp_r, l, blk.x + nl, sm.nuc[nl][3], COMPS == 1)) {
         const double f = T.ao_factor[k];
         const double s2 = sm.rad[slot][1], s3 = sm.rad[slot][2], s4 = sm.rad[slot][3], s5 = sm.rad[slot][4];
-        if (l == 0) {
-          v[0] = s1 * f; v[1] = s2 * f; v[2] = s3 * f; v[3] = s4 * f; v[4] = s5 * f;
-        } else {
-          double P[5];
-          const double x = sm.nuc[nl][0], y = sm.nuc[nl][1], z = sm.nuc[nl][2];
-          if (l == 1) {
-            P[0] = (a ? x : (bb ? y : z)) + kShift;
-            P[1] = (double)a; P[2] = (double)bb; P[3] = (double)c; P[4] = 0.0;
-          } else {
-            monomial_vgl<double>(a, bb, c, x, y, z, P);
+        if (l <= 3) {
+          // one formula for every l <= 3 (the l = 0 and l = 1 cases of the
+          // reference are its special values): no divergence between lanes
+          double xa, xa1, xa2, yb, yb1, yb2, zc, zc1, zc2;
+          pows3(sm.nuc[nl][0], a, xa, xa1, xa2);
+          pows3(sm.nuc[nl][1], bb, yb, yb1, yb2);
+          pows3(sm.nuc[nl][2], c, zc, zc1, zc2);
+          const double da = (double)a, db = (double)bb, dc = (double)c;
+          const double yz = yb * zc, xz = xa * zc, xy = xa * yb;
+          const double P0 = xa * yz + (l >= 1 ? kShift : 0.0);
+          const double P1 = da * xa1 * yz, P2 = db * yb1 * xz, P3 = dc * zc1 * xy;
+          v[0] = P0 * s1 * f;
+          if (COMPS == 5) {
+            const double P4 = da * (da - 1.0) * xa2 * yz + db * (db - 1.0) * yb2 * xz + dc * (dc - 1.0) * zc2 * xy;
+            v[1] = (P1 * s1 + P0 * s2) * f;
+            v[2] = (P2 * s1 + P0 * s3) * f;
+            v[3] = (P3 * s1 + P0 * s4) * f;
+            v[4] = (P4 * s1 + P0 * s5 + 2.0 * (P1 * s2 + P2 * s3 + P3 * s4)) * f;
           }
+        } else {   // l >= 4
+          double P[5];
+          monomial_vgl<double>(a, bb, c, sm.nuc[nl][0], sm.nuc[nl][1], sm.nuc[nl][2], P);
           v[0] = P[0] * s1 * f;
           if (COMPS == 5) {
             v[1] = (P[1] * s1 + P[0] * s2) * f;
             v[2] = (P[2] * s1 + P[0] * s3) * f;
             v[3] = (P[3] * s1 + P[0] * s4) * f;
-            if (l == 1)
-              v[4] = (P[0] * s5 + 2.0 * (P[1] * s2 + P[2] * s3 + P[3] * s4)) * f;
-            else
-              v[4] = (P[4] * s1 + P[0] * s5 + 2.0 * (P[1] * s2 + P[2] * s3 + P[3] * s4)) * f;
+            v[4] = (P[4] * s1 + P[0] * s5 + 2.0 * (P[1] * s2 + P[2] * s3 + P[3] * s4)) * f;
           }
         }
       }
@@ -191,12 +208,13 @@ ao_f64_kernel(const DevTables T, const int64_t point_num, const double* __restri
           dst[2 * pstride] = pc[2];
         }
       } else {
-        row[k] = v[0];
+        // streaming stores: the array is written once and not read back here
+        __stcs(&row[k], v[0]);
         if (COMPS == 5) {
-          row[A + k] = v[1];
-          row[2 * A + k] = v[2];
-          row[3 * A + k] = v[3];
-          row[4 * A + k] = v[4];
+          __stcs(&row[A + k], v[1]);
+          __stcs(&row[2 * A + k], v[2]);
+          __stcs(&row[3 * A + k], v[3]);
+          __stcs(&row[4 * A + k], v[4]);
         }
       }
     }

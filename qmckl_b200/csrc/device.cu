@@ -497,6 +497,12 @@ qmckl_exit_code upload_tables(qmckl_context context, DeviceState* ds) {
   }
   const size_t o_aosh = put(ao_shell.data(), sizeof(int32_t) * A);
   const size_t o_shco = put(shell_coef.data(), sizeof(int2) * S);
+  // (exponent, coefficient) of every coefficient entry, for one load per primitive
+  std::vector<double2> coef_ac(d.coef_val.size());
+  for (int64_t sh = 0; sh < S; ++sh)
+    for (int j = d.shell_coef_start[sh]; j < d.shell_coef_start[sh + 1]; ++j)
+      coef_ac[j] = make_double2(d.expo_sorted[d.nuc_prim_start[shell_nuc[sh]] + d.coef_prim[j]], d.coef_val[j]);
+  const size_t o_cac = put(coef_ac.data(), sizeof(double2) * coef_ac.size());
   // AO tiles of the tiled kernels (ao_tile.cu)
   std::vector<int4> tiles;
   std::vector<int2> tile_nuc;
@@ -558,6 +564,7 @@ qmckl_exit_code upload_tables(qmckl_context context, DeviceState* ds) {
   T.shell_prims = (const int2*)(base + o_shpr);
   T.ao_shell = (const int32_t*)(base + o_aosh);
   T.shell_coef = (const int2*)(base + o_shco);
+  T.coef_ac = (const double2*)(base + o_cac);
   ds->tiles.ntiles = (int32_t)tiles.size();
   ds->tiles.tile = (const int4*)(base + o_tile);
   ds->tiles.tile_nuc = (const int2*)(base + o_tnuc);

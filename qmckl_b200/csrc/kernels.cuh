@@ -41,6 +41,7 @@ struct DevTables {
   // tables of the fused AO -> MO kernel (global shell numbering)
   const int32_t* ao_shell;        // [ao] shell of each AO
   const int2* shell_coef;         // [shell] (begin, end) into coef_prim / coef_val
+  const double2* coef_ac;         // [coefficient entry] (exponent, coefficient): coef_val with its exponent
 };
 
 // Global count of kernels launched by this library.
