@@ -58,6 +58,7 @@ struct alignas(64) BatchDesc {
   int64_t perm_off;    // offset of its point order in the permutation buffer
   int64_t P;
   const uint8_t* krec;
+  const uint8_t* kskip;   // tile-skipping tables of the K blocks (fused_tc.cu)
   const double* scales;   // scale block of the system's coefficient pieces
   RowBound rb;            // row bounds of the float16 operands
   double cutoff;
@@ -75,6 +76,8 @@ struct BatchCtl {                 // shared-memory control block of a CTA
   double pts[3 * kPts];
   int64_t pidx[kPts];
   int rexp[3 * kPts];
+  // followed in shared memory by the tile's K blocks, their flags and the
+  // counts (batch_smem): int act[kb_max], flag[kb_max], n, lo, hi, first
 };
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
@@ -157,7 +160,8 @@ __global__ void __launch_bounds__((PRODW + 2) * 32, 1)
 batch_mo_kernel(const BatchDesc* __restrict__ desc, const CUtensorMap* __restrict__ tmaps,
                 const int4* __restrict__ items, const int n_items, int* __restrict__ ctl_words,
                 const double* __restrict__ coord, double* __restrict__ out, int* __restrict__ perm,
-                const int n_tile_max, const int rec_max, const long long wait_limit, const int publish) {
+                const int n_tile_max, const int rec_max, const int kb_max, const long long wait_limit,
+                const int publish) {
   constexpr int COMPS = 5;
   constexpr int PIECES = kPieces;
   constexpr int CHUNK = BK / PRODW;
@@ -252,9 +256,52 @@ batch_mo_kernel(const BatchDesc* __restrict__ desc, const CUtensorMap* __restric
     const int kblocks = D.kblocks, n_tile = D.n_tile, rec_bytes = D.rec_bytes;
     const int n0 = ntile * n_tile;
     const int B_TILE = n_tile * BK * 2;
+    // K blocks that are not identically zero over the tile's points (as in
+    // the single-system fused kernel, fused_tc.cu)
+    int* act = (int*)(&C + 1);
+    int* kflag = act + kb_max;
+    int* kcnt = kflag + kb_max;
+    {
+      const int2* kb_sh = (const int2*)D.kskip;
+      const double4* sph = (const double4*)(D.kskip + kskip_sph_offset(kblocks));
+      for (int kb = warp; kb < kblocks; kb += NTHREADS / 32) {
+        bool live = false;
+        const int2 r = kb_sh[kb];
+        if (lane < kPts && p0 + lane < P) {
+          const double px = C.pts[lane], py = C.pts[kPts + lane], pz = C.pts[2 * kPts + lane];
+          for (int q = r.x; q < r.y && !live; ++q) {
+            const double4 c = sph[q];
+            const double x = px - c.x, y = py - c.y, z = pz - c.z;
+            live = x * x + y * y + z * z <= c.w;
+          }
+        }
+        live = __any_sync(0xffffffffu, live);
+        if (lane == 0) kflag[kb] = live ? 1 : 0;
+      }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      int n = 0, lo = -1, hi = -1;
+      for (int kb = 0; kb < kblocks; ++kb)
+        if (kflag[kb]) {
+          act[n++] = kb;
+          if (2 * kb >= kblocks) { if (hi < 0) hi = kb; }
+          else if (lo < 0) lo = kb;
+        }
+      if (n == 0) {
+        act[n++] = 0;
+        lo = 0;
+      }
+      kcnt[0] = n;
+      kcnt[1] = lo;
+      kcnt[2] = hi;
+      kcnt[3] = act[0];
+    }
+    __syncthreads();
+    const int nact = kcnt[0];
     if (warp < PRODW) {
-      for (int kb = 0; kb < kblocks; ++kb) {
-        const uint32_t g = kbase + (uint32_t)kb;
+      for (int it = 0; it < nact; ++it) {
+        const uint32_t g = kbase + (uint32_t)it;
         const int s = (int)(g & 1u);
         const uint32_t phase = (g >> 1) & 1u;
         bool ok = mbar_wait(&C.empty[s], phase ^ 1u, err, 21);
@@ -268,8 +315,9 @@ batch_mo_kernel(const BatchDesc* __restrict__ desc, const CUtensorMap* __restric
     } else if (warp == TMA_WARP) {
       if (lane == 0) {
         const CUtensorMap* map = tmaps + sys;
-        for (int kb = 0; kb < kblocks; ++kb) {
-          const uint32_t g = kbase + (uint32_t)kb;
+        for (int it = 0; it < nact; ++it) {
+          const int kb = act[it];
+          const uint32_t g = kbase + (uint32_t)it;
           const int s = (int)(g & 1u);
           const uint32_t phase = (g >> 1) & 1u;
           if (!mbar_wait(&C.empty[s], phase ^ 1u, err, 22)) break;
@@ -283,14 +331,14 @@ batch_mo_kernel(const BatchDesc* __restrict__ desc, const CUtensorMap* __restric
     } else {
       if (lane == 0) {
         const uint32_t idesc = mma_idesc<PIECES>(n_tile);
-        for (int kb = 0; kb < kblocks; ++kb) {
-          const uint32_t g = kbase + (uint32_t)kb;
+        for (int it = 0; it < nact; ++it) {
+          const uint32_t g = kbase + (uint32_t)it;
           const int s = (int)(g & 1u);
           const uint32_t phase = (g >> 1) & 1u;
           if (!mbar_wait(&C.full[s], phase, err, 23)) break;
           tc_fence_after();
           mma_kblock<PIECES>(smem_addr(smem + s * STAGE), (uint32_t)(PIECES * A_TILE), (uint32_t)B_TILE, tmem, n_tile,
-                             idesc, kb, kblocks);
+                             idesc, act[it], kblocks, kcnt[1], kcnt[2] < 0 ? kblocks : kcnt[2], kcnt[3]);
           umma_commit(&C.empty[s]);
         }
         umma_commit(&C.acc_full);
@@ -304,11 +352,11 @@ batch_mo_kernel(const BatchDesc* __restrict__ desc, const CUtensorMap* __restric
       ok = __all_sync(0xffffffffu, ok && *(volatile int*)err == 0);
       tc_fence_after();
       if (ok)
-        epilogue_warp<PIECES, COMPS>(tmem, n_tile, n0, D.n_out, kblocks >= 2, C.pidx, C.rexp, D.scales,
+        epilogue_warp<PIECES, COMPS>(tmem, n_tile, n0, D.n_out, kcnt[2] >= 0, C.pidx, C.rexp, D.scales,
                                      out + D.out_off, (double*)smem + warp * 32 * 16, warp, lane, warp >> 2,
-                                     PRODW / 4);
+                                     PRODW / 4, kcnt[1] >= 0);
     }
-    kbase += (uint32_t)kblocks;
+    kbase += (uint32_t)nact;
     ++ntiles;
   }
   tc_fence_before();
@@ -325,16 +373,17 @@ batch_mo_kernel(const BatchDesc* __restrict__ desc, const CUtensorMap* __restric
   }
 }
 
-size_t batch_smem(int n_tile_max, int rec_max) {
+size_t batch_smem(int n_tile_max, int rec_max, int kb_max) {
   return 1024 + (size_t)kStages * kPieces * (A_TILE + (size_t)n_tile_max * BK * 2) + (size_t)kStages * rec_max +
-         sizeof(BatchCtl);
+         sizeof(BatchCtl) + (size_t)(2 * kb_max + 4) * 4;
 }
 
 struct BatchSys {
   int64_t P = 0, A = 0, M = 0;
   TcPlan plan;
-  size_t coef_off = 0, krec_off = 0;
+  size_t coef_off = 0, krec_off = 0, kskip_off = 0;
   int rec_bytes = 0;
+  std::vector<int64_t> ao_perm;   // the AO at each K position of the records
   double cutoff = 0.0;
   double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
   int64_t coord_off = 0, out_off = 0, perm_off = 0;
@@ -365,8 +414,8 @@ struct Batch {
   bool own_stream = false;
   std::vector<BatchSys> sys;
   int64_t coord_total = 0, out_total = 0, perm_total = 0;
-  int n_tile_max = 0, rec_max = 0;
-  DBuf coef, krec, desc, tmaps, items, ctl, perm, keys, counts, loop_err, nucl, env;
+  int n_tile_max = 0, rec_max = 0, kb_max = 0;
+  DBuf coef, krec, kskip, desc, tmaps, items, ctl, perm, keys, counts, loop_err, nucl, env;
   int n_items = 0;
   // tuning
   int prod_warps = 16;
@@ -444,7 +493,7 @@ cudaError_t build_items(Batch* B) {
 }
 
 cudaError_t set_kernel_attrs(Batch* B) {
-  const size_t smem = batch_smem(B->n_tile_max, B->rec_max);
+  const size_t smem = batch_smem(B->n_tile_max, B->rec_max, B->kb_max);
   cudaError_t e = cudaFuncSetAttribute(batch_mo_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(batch_mo_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -452,7 +501,7 @@ cudaError_t set_kernel_attrs(Batch* B) {
 }
 
 cudaError_t enqueue(Batch* B, const double* coord, double* out) {
-  const size_t smem = batch_smem(B->n_tile_max, B->rec_max);
+  const size_t smem = batch_smem(B->n_tile_max, B->rec_max, B->kb_max);
   cudaError_t e = cudaMemsetAsync(B->ctl.p, 0, sizeof(int) * (2 + B->sys.size()), B->stream);
   if (e != cudaSuccess) return e;
   int sms = 148;
@@ -461,11 +510,13 @@ cudaError_t enqueue(Batch* B, const double* coord, double* out) {
   if (B->prod_warps == 8)
     batch_mo_kernel<8><<<grid, 10 * 32, smem, B->stream>>>(
         (const BatchDesc*)B->desc.p, (const CUtensorMap*)B->tmaps.p, (const int4*)B->items.p, B->n_items,
-        (int*)B->ctl.p, coord, out, (int*)B->perm.p, B->n_tile_max, B->rec_max, B->wait_limit, B->publish);
+        (int*)B->ctl.p, coord, out, (int*)B->perm.p, B->n_tile_max, B->rec_max, B->kb_max, B->wait_limit,
+        B->publish);
   else
     batch_mo_kernel<16><<<grid, 18 * 32, smem, B->stream>>>(
         (const BatchDesc*)B->desc.p, (const CUtensorMap*)B->tmaps.p, (const int4*)B->items.p, B->n_items,
-        (int*)B->ctl.p, coord, out, (int*)B->perm.p, B->n_tile_max, B->rec_max, B->wait_limit, B->publish);
+        (int*)B->ctl.p, coord, out, (int*)B->perm.p, B->n_tile_max, B->rec_max, B->kb_max, B->wait_limit,
+        B->publish);
   return cudaGetLastError();
 }
 
@@ -575,13 +626,24 @@ qmckl_exit_code qmckl_b200_batch_create(const qmckl_context* contexts, const int
     return fail(c0, fname, msg);
   };
   B->sys.resize((size_t)num);
-  size_t coef_total = 0, krec_total = 0, nucl_total = 0, env_total = 0;
-  std::vector<std::vector<uint8_t>> recs((size_t)num);
+  size_t coef_total = 0, krec_total = 0, nucl_total = 0, env_total = 0, kskip_total = 0;
+  std::vector<std::vector<uint8_t>> recs((size_t)num), kskips((size_t)num);
   std::vector<std::vector<float>> envs((size_t)num);
   std::vector<float> env_r0((size_t)num), env_il((size_t)num);
   std::vector<size_t> nucl_off((size_t)num), env_off((size_t)num);
   uint64_t sig = 1469598103934665603ull;
   sig = fnv(sig, num);
+  // the kernel's shared memory follows the largest MO tile and K-block count
+  // of the batch: known before the records are built, so that each system's
+  // records can take what is left
+  for (int64_t s = 0; s < num; ++s) {
+    const Context* ctx = ctx_of(contexts[s]);
+    const TcPlan pl = tc_plan(ctx->ao_basis.ao_num, ctx->mo_basis.mo_num, kPieces);
+    B->n_tile_max = std::max(B->n_tile_max, pl.n_tile);
+    B->kb_max = std::max(B->kb_max, (int)((ctx->ao_basis.ao_num + BK - 1) / BK));
+  }
+  size_t max_rec = 128;
+  while (batch_smem(B->n_tile_max, (int)max_rec + 128, B->kb_max) <= 232448) max_rec += 128;
   for (int64_t s = 0; s < num; ++s) {
     const Context* ctx = ctx_of(contexts[s]);
     BatchSys& S = B->sys[s];
@@ -590,7 +652,8 @@ qmckl_exit_code qmckl_b200_batch_create(const qmckl_context* contexts, const int
     S.M = ctx->mo_basis.mo_num;
     S.plan = tc_plan(S.A, S.M, kPieces);
     S.cutoff = std::log((double)(((uint64_t)1) << (ctx->precision - 1)));
-    if (!build_krec_records(ctx, recs[s], S.rec_bytes)) return bail("AOs are not numbered shell by shell");
+    if (!build_fused_records(ctx, S.cutoff, max_rec, recs[s], S.rec_bytes, kskips[s], S.ao_perm))
+      return bail("AOs are not numbered shell by shell");
     build_envelopes(ctx, envs[s], env_r0[s], env_il[s]);
     nucl_off[s] = nucl_total;
     nucl_total += 3 * (size_t)ctx->nucleus.num;
@@ -609,6 +672,8 @@ qmckl_exit_code qmckl_b200_batch_create(const qmckl_context* contexts, const int
     coef_total += (S.plan.coef_bytes + 1023) / 1024 * 1024;
     S.krec_off = krec_total;
     krec_total += recs[s].size();
+    S.kskip_off = kskip_total;
+    kskip_total += (kskips[s].size() + 255) / 256 * 256;
     S.coord_off = B->coord_total;
     B->coord_total += 3 * S.P;
     S.out_off = B->out_total;
@@ -620,8 +685,9 @@ qmckl_exit_code qmckl_b200_batch_create(const qmckl_context* contexts, const int
     sig = fnv(fnv(fnv(sig, S.P), S.A), S.M);
   }
   B->signature = sig;
-  if (batch_smem(B->n_tile_max, B->rec_max) > 232448) return bail("basis too large for the batched kernel");
+  if (batch_smem(B->n_tile_max, B->rec_max, B->kb_max) > 232448) return bail("basis too large for the batched kernel");
   if (dalloc(B->coef, coef_total) != cudaSuccess || dalloc(B->krec, krec_total) != cudaSuccess ||
+      dalloc(B->kskip, std::max<size_t>(kskip_total, 256)) != cudaSuccess ||
       dalloc(B->desc, sizeof(BatchDesc) * num) != cudaSuccess ||
       dalloc(B->tmaps, sizeof(CUtensorMap) * num) != cudaSuccess ||
       dalloc(B->ctl, sizeof(int) * (2 + num)) != cudaSuccess ||
@@ -640,8 +706,17 @@ qmckl_exit_code qmckl_b200_batch_create(const qmckl_context* contexts, const int
     const Context* ctx = ctx_of(contexts[s]);
     BatchSys& S = B->sys[s];
     void* dcoef = (char*)B->coef.p + S.coef_off;
-    if (tc_prepare_coef(S.plan, ctx->mo_basis.coefficient.data(), dcoef, B->stream) != cudaSuccess)
-      return bail("coefficient upload failed");
+    {
+      // coefficient columns in the K order of the records
+      std::vector<double> cp((size_t)(S.M * S.A));
+      const std::vector<double>& c = ctx->mo_basis.coefficient;
+      for (int64_t i = 0; i < S.M; ++i)
+        for (int64_t k = 0; k < S.A; ++k) cp[i * S.A + k] = c[i * S.A + S.ao_perm[k]];
+      if (tc_prepare_coef(S.plan, cp.data(), dcoef, B->stream) != cudaSuccess) return bail("coefficient upload failed");
+    }
+    if (cudaMemcpyAsync((char*)B->kskip.p + S.kskip_off, kskips[s].data(), kskips[s].size(), cudaMemcpyHostToDevice,
+                        B->stream) != cudaSuccess)
+      return bail("record upload failed");
     double* dn = (double*)B->nucl.p + nucl_off[s];
     float* de = (float*)B->env.p + env_off[s];
     if (cudaMemcpyAsync(dn, ctx->nucleus.coord.data(), sizeof(double) * 3 * ctx->nucleus.num, cudaMemcpyHostToDevice,
@@ -662,6 +737,7 @@ qmckl_exit_code qmckl_b200_batch_create(const qmckl_context* contexts, const int
     D.perm_off = S.perm_off;
     D.P = S.P;
     D.krec = (const uint8_t*)B->krec.p + S.krec_off;
+    D.kskip = (const uint8_t*)B->kskip.p + S.kskip_off;
     D.scales = tc_scales(S.plan, dcoef);
     D.rb = RowBound{dn, de, (int)ctx->nucleus.num, env_r0[s], env_il[s]};
     S.rb = D.rb;
@@ -695,7 +771,7 @@ qmckl_exit_code qmckl_b200_batch_destroy(qmckl_b200_batch batch) {
   cudaSetDevice(B->device);
   if (B->stream) cudaStreamSynchronize(B->stream);
   drop_graph(B);
-  for (DBuf* b : {&B->coef, &B->krec, &B->desc, &B->tmaps, &B->items, &B->ctl, &B->perm, &B->keys, &B->counts,
+  for (DBuf* b : {&B->coef, &B->krec, &B->kskip, &B->desc, &B->tmaps, &B->items, &B->ctl, &B->perm, &B->keys, &B->counts,
                   &B->loop_err, &B->nucl, &B->env})
     if (b->p) cudaFree(b->p);
   if (B->h_err) cudaFreeHost(B->h_err);
@@ -815,7 +891,7 @@ qmckl_exit_code qmckl_b200_batch_mo_vgl_loop_device(qmckl_b200_batch batch, cons
     if (e == cudaSuccess)
       e = tc_launch_fused(S.plan, S.P, 5, c, S.cutoff, S.map, (const char*)B->krec.p + S.krec_off, S.rec_bytes, pm,
                           (const char*)B->coef.p + S.coef_off, S.rb, d_mo_vgl + S.out_off, (int*)B->loop_err.p,
-                          B->stream);
+                          B->stream, -1, (const char*)B->kskip.p + S.kskip_off);
   }
   if (e == cudaSuccess) e = cudaMemcpyAsync(B->h_err, B->loop_err.p, sizeof(int), cudaMemcpyDeviceToHost, B->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(B->stream);

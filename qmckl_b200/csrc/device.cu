@@ -217,6 +217,28 @@ std::vector<int32_t> fused_shell_order(const Context* ctx, double cutoff) {
   return order;
 }
 
+// Records and tile-skipping tables of the fused kernels in the K order of
+// fused_shell_order, or in the basis order when the reordered records would
+// exceed max_rec_bytes (the shared memory they get); kskip is laid out as
+// the kernels read it (int2 per K block, double4 per shell from
+// tc_kskip_bytes - 32 * shell_num on) and ao_perm[k] is the AO at K
+// position k.  False when the AO numbering allows no records.
+bool build_fused_records(const Context* ctx, double cutoff, size_t max_rec_bytes, std::vector<uint8_t>& recs,
+                         int& rec_bytes, std::vector<uint8_t>& kskip, std::vector<int64_t>& ao_perm) {
+  const int64_t A = ctx->ao_basis.ao_num, S = ctx->ao_basis.shell_num;
+  std::vector<int2> kb_sh;
+  std::vector<double4> sph;
+  const std::vector<int32_t> order = fused_shell_order(ctx, cutoff);
+  bool ok = build_krec_records(ctx, recs, rec_bytes, &order, &ao_perm, &kb_sh, &sph, cutoff) &&
+            (size_t)rec_bytes <= max_rec_bytes;
+  if (!ok && !build_krec_records(ctx, recs, rec_bytes, nullptr, &ao_perm, &kb_sh, &sph, cutoff)) return false;
+  const size_t kbytes = tc_kskip_bytes(A, S);
+  kskip.assign(kbytes, 0);
+  std::memcpy(kskip.data(), kb_sh.data(), sizeof(int2) * kb_sh.size());
+  std::memcpy(kskip.data() + (kbytes - sizeof(double4) * (size_t)S), sph.data(), sizeof(double4) * sph.size());
+  return true;
+}
+
 // Row-bound envelopes of the 2-piece float16 operands (fused_common.cuh
 // RowBound) for the basis of a context: env[nucl][3][kEnvCells], and the
 // radial cells (r0, 1 / log2 of the cell ratio) shared by all nuclei.
@@ -679,7 +701,7 @@ qmckl_exit_code prepare_fused(qmckl_context context, DeviceState* ds, bool* usab
   const char* fname = "qmckl_b200_mo_mixed";
   Context* ctx = ctx_of(context);
   *usable = false;
-  const int64_t A = ctx->ao_basis.ao_num, M = ctx->mo_basis.mo_num, S = ctx->ao_basis.shell_num;
+  const int64_t A = ctx->ao_basis.ao_num, M = ctx->mo_basis.mo_num;
   const int pieces = ds->split_pieces;
   const double cutoff = cutoff_of(ctx);
   const TcPlan plan = tc_plan(A, M, pieces);
@@ -691,22 +713,18 @@ qmckl_exit_code prepare_fused(qmckl_context context, DeviceState* ds, bool* usab
                      ds->krec_nucl_version == ctx->nucleus.coord_version &&
                      ds->krec_cusp_version == ctx->mo_basis.cusp_version && ds->krec_cutoff == cutoff;
   if (!fresh) {
-    std::vector<uint8_t> h;
+    std::vector<uint8_t> h, ks;
     std::vector<int64_t> perm;
-    std::vector<int2> kb_sh;
-    std::vector<double4> sph;
     int rec = 0;
-    const std::vector<int32_t> order = fused_shell_order(ctx, cutoff);
-    bool ok = build_krec_records(ctx, h, rec, &order, &perm, &kb_sh, &sph, cutoff) && fits(rec);
-    if (!ok && !build_krec_records(ctx, h, rec, nullptr, &perm, &kb_sh, &sph, cutoff)) return QMCKL_SUCCESS;
+    // the largest record that keeps the VGL kernel within its shared memory
+    size_t max_rec = 128;
+    while (fits((int)(max_rec + 128))) max_rec += 128;
+    if (!build_fused_records(ctx, cutoff, max_rec, h, rec, ks, perm)) return QMCKL_SUCCESS;
     qmckl_exit_code rc = ensure(context, ds->krec, h.size(), fname);
     if (rc != QMCKL_SUCCESS) return rc;
-    const size_t kbytes = tc_kskip_bytes(A, S);
+    const size_t kbytes = ks.size();
     rc = ensure(context, ds->kskip, kbytes, fname);
     if (rc != QMCKL_SUCCESS) return rc;
-    std::vector<uint8_t> ks(kbytes, 0);
-    std::memcpy(ks.data(), kb_sh.data(), sizeof(int2) * kb_sh.size());
-    std::memcpy(ks.data() + (kbytes - sizeof(double4) * (size_t)S), sph.data(), sizeof(double4) * sph.size());
     QB_CUDA(cudaMemcpy(ds->krec.p, h.data(), h.size(), cudaMemcpyHostToDevice), fname);
     QB_CUDA(cudaMemcpy(ds->kskip.p, ks.data(), kbytes, cudaMemcpyHostToDevice), fname);
     ds->rec_bytes = rec;

@@ -47,6 +47,13 @@ struct KRecShell {
   float cusp_r2;
   int32_t pad;
 };
+// Tile-skipping tables of the K blocks (built by build_fused_records in
+// device.cu): int2 kb_sh[kblocks], the range of shell spheres of each K
+// block, then, from byte kskip_sph_offset(kblocks) on, double4 sph[] (the
+// shell's nucleus and the squared radius beyond which its AOs vanish in the
+// producers).
+__host__ __device__ constexpr int kskip_sph_offset(int kblocks) { return (kblocks * 8 + 31) / 32 * 32; }
+
 constexpr int kRecAoOff = 16;
 constexpr int kRecShellOff = 16 + 64 * 8;
 

@@ -32,13 +32,10 @@ constexpr int kMmaWarp = kProdWarps + 1;
 constexpr int kThreadsF = (kProdWarps + 2) * 32;
 constexpr int STAGES = 2;
 
-// Tile skipping: kskip (optional) holds int2 kb_sh[kblocks] (the range of
-// shell spheres of each K block) and, from byte kskip_sph_offset(kblocks) on,
-// double4 sph[] (nucleus of the shell, squared radius beyond which its AOs
-// vanish in the producers; see shell_r2max in device.cu).  A K block whose
-// shells are all beyond their radius at every point of the tile contributes
-// exact zeros and is left out of the producer, TMA and MMA loops.
-__host__ __device__ constexpr int kskip_sph_offset(int kblocks) { return (kblocks * 8 + 31) / 32 * 32; }
+// Tile skipping: kskip (optional; layout in fused_common.cuh) lists, per K
+// block, the screening spheres of its shells.  A K block whose shells are
+// all beyond their radius at every point of the tile contributes exact zeros
+// and is left out of the producer, TMA and MMA loops.
 
 template <int PIECES, int COMPS>
 __global__ void __launch_bounds__(kThreadsF, 1)

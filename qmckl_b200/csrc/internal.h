@@ -147,6 +147,11 @@ struct PreparedMixed;
 qmckl_exit_code dev_prepared_mixed(qmckl_context context, PreparedMixed* out);
 // K-block records of the fused kernels for the basis and nuclei of a context (device.cu)
 bool build_krec_records(const Context* ctx, std::vector<uint8_t>& records, int& rec_bytes);
+// The same records in the fused kernels' own K order, with the K blocks'
+// tile-skipping tables and the AO at each K position (device.cu); the basis
+// order when the reordered records would exceed max_rec_bytes.
+bool build_fused_records(const Context* ctx, double cutoff, size_t max_rec_bytes, std::vector<uint8_t>& recs,
+                         int& rec_bytes, std::vector<uint8_t>& kskip, std::vector<int64_t>& ao_perm);
 // Row-bound envelopes of the mixed form's 2-piece float16 operands (device.cu)
 void build_envelopes(const Context* ctx, std::vector<float>& env, float& r0, float& inv_log2q);
 
