@@ -126,6 +126,10 @@ qmckl_exit_code qmckl_get_electron_down_num(const qmckl_context context, int64_t
 qmckl_exit_code qmckl_get_electron_walk_num(const qmckl_context context, int64_t* const walk_num);
 qmckl_exit_code qmckl_get_electron_coord(const qmckl_context context, const char transp,
                                          double* const coord, const int64_t size_max);
+/* TREXIO input (org/qmckl_trexio.org:1106-1188); this build has no TREXIO
+ * and returns QMCKL_FAILURE "QMCkl was compiled without TREXIO", as the
+ * reference does when built without it. */
+qmckl_exit_code qmckl_trexio_read(const qmckl_context context, const char* file_name, const int64_t size_max);
 /* point-nucleus distances [point][nucl] (org/qmckl_electron.org:1205-1262) */
 qmckl_exit_code qmckl_get_electron_en_distance(qmckl_context context, double* const distance,
                                                const int64_t size_max);

@@ -358,6 +358,13 @@ def b200_get_kblock_stats(ctx, reset=False):
     return ev.value, tot.value
 
 
+def trexio_read(ctx, file_name):
+    """qmckl_trexio_read: this build has no TREXIO and raises RuntimeError (the
+    reference's behaviour when built without it)."""
+    b = file_name.encode()
+    _call("qmckl_trexio_read", ctx, C.c_char_p(b), C.c_int64(len(b)))
+
+
 def set_mo_basis_r_cusp(ctx, r_cusp):
     a, p, n = _arr(r_cusp, np.float64)
     _call("qmckl_set_mo_basis_r_cusp", ctx, p, n)

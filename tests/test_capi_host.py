@@ -161,3 +161,12 @@ def test_compute_without_gpu_fails_loudly(chbrclf):
     with pytest.raises(RuntimeError, match="no CUDA device"):
         pq.get_mo_basis_mo_vgl(ctx, 136 * 5 * 224)
     pq.context_destroy(ctx)
+
+
+def test_trexio_read_reports_no_trexio():
+    """qmckl_trexio_read exists and fails as the reference does when built
+    without TREXIO (org/qmckl_trexio.org:1182-1186)."""
+    ctx = pq.context_create()
+    with pytest.raises(RuntimeError, match="compiled without TREXIO"):
+        pq.trexio_read(ctx, "fake.h5")
+    pq.context_destroy(ctx)

@@ -164,3 +164,22 @@ def test_fused_tile_skipping():
     assert not res["fp64"][pts.shape[0]:].any()
     assert max(comp_error(res["fused"][near], res["fp64"][near])) <= MIXED_TOL
     assert max(comp_error(res["unfused"][near], res["fp64"][near])) <= MIXED_TOL
+
+
+def test_fused_follows_precision_changes():
+    """The fused kernel's K order and tile-skipping radii depend on the
+    screening cutoff (ln 2^(p-1)): after the precision changes the mixed form
+    agrees with the oracle at the new precision."""
+    d = gen.config(0, walk_num=4)
+    pts = gen.points(d)
+    P, M = pts.shape[0], d["mo_num"]
+    basis = O.Basis(d)
+    ctx = make_context(d, form=pq.FORM_MIXED)
+    first = pq.get_mo_basis_mo_vgl(ctx, P * 5 * M).reshape(P, 5, M)
+    ref53 = O.mo_vgl(d["mo_coef"], O.ao_vgl(basis, pts, d["nucl_coord"], precision=53))
+    assert max(comp_error(first, ref53)) <= MIXED_TOL
+    pq.set_numprec_precision(ctx, 30)
+    second = pq.get_mo_basis_mo_vgl(ctx, P * 5 * M).reshape(P, 5, M)
+    ref30 = O.mo_vgl(d["mo_coef"], O.ao_vgl(basis, pts, d["nucl_coord"], precision=30))
+    assert max(comp_error(second, ref30)) <= MIXED_TOL
+    pq.context_destroy(ctx)
