@@ -49,6 +49,18 @@ struct DerivSmem {
 // x^a and its first three derivatives (Leibniz, one factor x at a time)
 template <typename F>
 __device__ __forceinline__ void pow_derivs(F x, int a, F (&q)[4]) {
+  if (a <= 3) {
+    // without branches (lanes of a warp hold different exponents): with
+    // f_i = x for i <= a, 1 otherwise, x^a = f1 f2 f3, and the derivatives
+    // a x^(a-1), a (a-1) x^(a-2), a (a-1) (a-2) vanish where they must
+    const F f1 = a >= 1 ? x : F(1), f2 = a >= 2 ? x : F(1), f3 = a >= 3 ? x : F(1);
+    const F fa = F(a);
+    q[2] = fa * (fa - F(1)) * f3;
+    q[1] = fa * (f2 * f3);
+    q[0] = f1 * (f2 * f3);
+    q[3] = fa * (fa - F(1)) * (fa - F(2));
+    return;
+  }
   q[0] = F(1); q[1] = F(0); q[2] = F(0); q[3] = F(0);
   for (int i = 0; i < a; ++i) {
     q[3] = q[3] * x + F(3) * q[2];
@@ -171,15 +183,14 @@ deriv_kernel(const DevTables T, const int64_t point_num, const double* __restric
     for (int i = threadIdx.x; i < 3 * T.nucl_num; i += blockDim.x) sacc[i] = 0.0;
     __syncthreads();
   }
-  const int64_t items = point_num * (int64_t)T.nblock;
   const int64_t stride = (int64_t)gridDim.x * kWarpsD;
-  for (int64_t it = (int64_t)blockIdx.x * kWarpsD + warp; it < items; it += stride) {
-    const int64_t p = it / T.nblock;
-    const int b = (int)(it - p * T.nblock);
+  // one warp per point, through its nucleus blocks (as the FP64 AO kernel)
+  for (int64_t p = (int64_t)blockIdx.x * kWarpsD + warp; p < point_num; p += stride) {
+   double pg[3] = {0., 0., 0.};
+   for (int b = 0; b < T.nblock; ++b) {
     const int4 blk = T.block[b];
     const int2 slots = T.block_slots[b];
     stage_deriv<MIXED>(T, sm, blk, slots, coord[p], coord[p + cstride], coord[p + 2 * cstride], cutoff, lane);
-    double pg[3] = {0., 0., 0.};
     for (int k0 = blk.z; k0 < blk.w; k0 += 32) {
       const int k = k0 + lane;
       const bool valid = k < blk.w;
@@ -247,6 +258,8 @@ deriv_kernel(const DevTables T, const int64_t point_num, const double* __restric
         }
       }
     }
+    __syncwarp();
+   }
     if (MODE == MODE_ADJOINT && grad_coord != nullptr) {
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
@@ -274,8 +287,7 @@ cudaError_t launch_deriv(const DevTables& T, int64_t point_num, const double* co
                          bool mixed, double* out, const void* G, double* grad_nucl, double* grad_coord,
                          int64_t gstride, cudaStream_t s, const double* cusp_r = nullptr) {
   if (point_num <= 0) return cudaSuccess;
-  const int64_t items = point_num * (int64_t)T.nblock;
-  const int grid = (int)std::min<int64_t>((items + kWarpsD - 1) / kWarpsD, 148 * 8);
+  const int grid = (int)std::min<int64_t>((point_num + kWarpsD - 1) / kWarpsD, 148 * 8);   // warps = points
   size_t dyn = 0;
   bool use_smem = false;
   if (MODE == MODE_ADJOINT) {
