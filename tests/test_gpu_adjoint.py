@@ -262,3 +262,24 @@ def test_autograd_function(adjoint_case):
             assert abs(fd - g) <= 1e-5 * float(coord.grad.abs().max())
     torch_ops.forget(ctx)
     pq.context_destroy(ctx)
+
+
+def test_adjoint_mixed_two_mo_tiles():
+    """250 MOs: two MO tiles in both tensor-core contractions of the mixed
+    adjoint (dL/dC: tiles of 192 MOs; G = W C^T: K = 250 in 4 K blocks),
+    against the oracle on 60 points of the config-1 molecule."""
+    torch = _torch()
+    d = dict(gen.config(1, walk_num=1))
+    rng = np.random.default_rng(17)
+    q, _ = np.linalg.qr(rng.standard_normal((d["ao_num"], 250)))
+    d["mo_coef"] = np.ascontiguousarray(q.T)
+    d["mo_num"] = 250
+    d["elec_coord"] = d["elec_coord"][:, :60]
+    pts = gen.points(d)
+    w = rng.standard_normal((pts.shape[0], 5, 250))
+    ctx = make_context(d, points=False, form=pq.FORM_MIXED)
+    got = _adjoint(ctx, d, w, torch)
+    pq.context_destroy(ctx)
+    ref = O.mo_vgl_adjoint(O.Basis(d), pts, d["nucl_coord"], d["mo_coef"], w)
+    for g, r in zip(got, ref):
+        assert np.abs(g - r).max() <= 1e-6 * np.abs(r).max()
