@@ -53,8 +53,12 @@ constexpr int kThreads = 32 * (kEpiWarps + 2);
 
 // ------------------------------------------------------------ GEMM kernel
 
-template <int PIECES, int STAGES, typename OutT = double>
-__global__ void __launch_bounds__(kThreads, 1)
+// TWO_ACC: one accumulator for the leading product and one for the
+// corrections (short K: the split of the leading product over two halves of
+// K is not needed), so that a 128-column tile needs 256 TMEM columns and two
+// CTAs share an SM.
+template <int PIECES, int STAGES, typename OutT = double, bool TWO_ACC = false>
+__global__ void __launch_bounds__(kThreads, TWO_ACC ? 2 : 1)
 tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                const int64_t M, const int n_out, const int n_tile, const int kblocks, const int comps,
                const double* __restrict__ scales, OutT* __restrict__ out, const int64_t ldo,
@@ -78,8 +82,9 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
   const int n0 = blockIdx.y * n_tile;
   // three accumulators of n_tile columns: A1*C1 (first half of K), A1*C1
   // (second half), corrections
+  constexpr int NACC = TWO_ACC ? 2 : 3;
   uint32_t tmem_cols = 32;
-  while ((int)tmem_cols < 3 * n_tile) tmem_cols <<= 1;
+  while ((int)tmem_cols < NACC * n_tile) tmem_cols <<= 1;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
@@ -139,8 +144,8 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
             const uint32_t a_addr = base + ia * A_TILE + kk * UMMA_K * 2;
             const uint32_t b_addr = base + PIECES * A_TILE + ib * B_TILE + kk * UMMA_K * 2;
             const bool lead = (t == NPROD - 1);                 // A1*C1
-            const bool second = lead && (2 * kb >= kblocks);
-            const uint32_t d = tmem + (uint32_t)((lead ? (second ? 1 : 0) : 2) * n_tile);
+            const bool second = !TWO_ACC && lead && (2 * kb >= kblocks);
+            const uint32_t d = tmem + (uint32_t)((lead ? (second ? 1 : 0) : NACC - 1) * n_tile);
             const bool first_use = lead ? (second ? (kb == (kblocks + 1) / 2 && kk == 0) : (kb == 0 && kk == 0))
                                         : (kb == 0 && kk == 0 && t == 0);
             umma_bf16(d, smem_desc(a_addr), smem_desc(b_addr), idesc, first_use ? 0u : 1u);
@@ -158,13 +163,13 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     if (ok) {
       double* stage = (double*)smem + warp * 32 * 16;     // [32 rows][16 cols] per warp; stages are idle now
       const int row_base = warp * 32;
-      const bool has_second = kblocks >= 2;
+      const bool has_second = !TWO_ACC && kblocks >= 2;
       for (int c0 = 0; c0 < n_tile; c0 += 16) {
         uint32_t r0[16], r1[16], r2[16];
         const uint32_t ta = tmem + ((uint32_t)row_base << 16) + (uint32_t)c0;
         tmem_ld16(ta, r0);
-        tmem_ld16(ta + (uint32_t)n_tile, r1);
-        tmem_ld16(ta + (uint32_t)(2 * n_tile), r2);
+        if (has_second) tmem_ld16(ta + (uint32_t)n_tile, r1);
+        tmem_ld16(ta + (uint32_t)((NACC - 1) * n_tile), r2);
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           double v = (double)__uint_as_float(r0[j]) + (double)__uint_as_float(r2[j]);
@@ -549,13 +554,13 @@ int* err_word() {
   return words[dev];
 }
 
-template <int PIECES, int STAGES, typename OutT = double>
+template <int PIECES, int STAGES, typename OutT = double, bool TWO_ACC = false>
 cudaError_t launch_gemm(const CUtensorMap& ta, const CUtensorMap& tb, int64_t M, int n_out, int n_tile, int n_tiles,
                         int kblocks, int comps, const double* scales, OutT* out, int64_t ldo, int* err,
                         cudaStream_t s) {
   const size_t stage = (size_t)PIECES * (BM * BK * 2 + (size_t)n_tile * BK * 2);
   const size_t smem = 1024 + STAGES * stage + (2 * STAGES + 1) * 8 + 16;
-  auto kern = tc_gemm_kernel<PIECES, STAGES, OutT>;
+  auto kern = tc_gemm_kernel<PIECES, STAGES, OutT, TWO_ACC>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   dim3 grid((unsigned)((M + BM - 1) / BM), (unsigned)n_tiles);
@@ -824,13 +829,16 @@ cudaError_t tc_gemm_nt(const void* x, int64_t ldx, int64_t x_pstride, int64_t ro
                        int64_t ldy, int64_t y_pstride, int64_t n, float* out, int64_t ldo, int* err, cudaStream_t s) {
   if (rows <= 0 || n <= 0) return cudaSuccess;
   if (ldx % 8 != 0 || ldy % 8 != 0 || x_pstride % 8 != 0 || y_pstride % 8 != 0) return cudaErrorInvalidValue;
-  const TcPlan tiles = tc_plan(k, n, 3);   // N tiling of the forward contraction
+  // 128-column MO tiles, one stage, two accumulators: ~99 KB of shared
+  // memory and 256 TMEM columns, two CTAs per SM (one's epilogue overlaps
+  // the other's loads and MMAs); K (the MO count) is short
+  const int n_tile = 128;
+  const int n_tiles = (int)((n + n_tile - 1) / n_tile);
   CUtensorMap tx, ty;
   if (!make_map(&tx, x, k, rows, ldx, 3, x_pstride, BM)) return cudaErrorInvalidValue;
-  if (!make_map(&ty, y, k, n, ldy, 3, y_pstride, tiles.n_tile)) return cudaErrorInvalidValue;
+  if (!make_map(&ty, y, k, n, ldy, 3, y_pstride, n_tile)) return cudaErrorInvalidValue;
   const int kblocks = (int)((k + BK - 1) / BK);
-  return launch_gemm<3, 2, float>(tx, ty, rows, (int)n, tiles.n_tile, tiles.n_tiles, kblocks, 1, nullptr, out, ldo,
-                                  err, s);
+  return launch_gemm<3, 1, float, true>(tx, ty, rows, (int)n, n_tile, n_tiles, kblocks, 1, nullptr, out, ldo, err, s);
 }
 
 }  // namespace qb
