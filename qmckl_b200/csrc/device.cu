@@ -432,31 +432,43 @@ qmckl_exit_code upload_tables(qmckl_context context, DeviceState* ds) {
       return qmckl_failwith(context, QMCKL_FAILURE, "qmckl_b200_upload_basis",
                             "more than 64 shells on one nucleus is not supported");
   }
+  // The lanes of a warp stage a block's shells 32 at a time, each pass
+  // lasting as long as its longest primitive list; slots are therefore
+  // numbered by descending primitive count (ties in shell order), so that
+  // the long contracted shells share a pass (config-1 molecule: 89 instead
+  // of 131 primitive steps per point).  Results do not depend on the order.
+  std::vector<std::pair<int64_t, int64_t>> blk_shells;   // (shell, nucleus)
   int64_t n = 0;
   while (n < N) {
     const int nb = (int)n;
-    int slots = 0;
     const int slot_begin = (int)slot_nuc.size();
     int64_t ao_begin = -1, ao_end = -1;
-    while (n < N && (n - nb) < kBlockNuc && slots + B.nucleus_shell_num[n] <= kBlockSlots) {
-      for (int64_t s = B.nucleus_index[n]; s < B.nucleus_index[n] + B.nucleus_shell_num[n]; ++s) {
-        const int slot = (int)slot_nuc.size() - slot_begin;
-        slot_nuc.push_back((int32_t)n);
-        slot_coef.push_back(make_int2(d.shell_coef_start[s], d.shell_coef_start[s + 1]));
-        const int l = B.shell_ang_mom[s];
-        const int64_t k0 = d.ao_index[s];
-        int64_t k = k0;
-        for (int a = l; a >= 0; --a)
-          for (int b = l - a; b >= 0; --b) {
-            const int c = l - a - b;
-            ao_code[k] = a | (b << 4) | (c << 8) | (l << 12) | (slot << 16) | ((int)(n - nb) << 24);
-            ++k;
-          }
-        if (ao_begin < 0 || k0 < ao_begin) ao_begin = k0;
-        if (k > ao_end) ao_end = k;
-        ++slots;
-      }
+    blk_shells.clear();
+    while (n < N && (n - nb) < kBlockNuc && (int64_t)blk_shells.size() + B.nucleus_shell_num[n] <= kBlockSlots) {
+      for (int64_t s = B.nucleus_index[n]; s < B.nucleus_index[n] + B.nucleus_shell_num[n]; ++s)
+        blk_shells.emplace_back(s, n);
       ++n;
+    }
+    std::stable_sort(blk_shells.begin(), blk_shells.end(), [&](const auto& u, const auto& v) {
+      return d.shell_coef_start[u.first + 1] - d.shell_coef_start[u.first] >
+             d.shell_coef_start[v.first + 1] - d.shell_coef_start[v.first];
+    });
+    for (size_t i = 0; i < blk_shells.size(); ++i) {
+      const int64_t s = blk_shells[i].first, sn = blk_shells[i].second;
+      const int slot = (int)i;
+      slot_nuc.push_back((int32_t)sn);
+      slot_coef.push_back(make_int2(d.shell_coef_start[s], d.shell_coef_start[s + 1]));
+      const int l = B.shell_ang_mom[s];
+      const int64_t k0 = d.ao_index[s];
+      int64_t k = k0;
+      for (int a = l; a >= 0; --a)
+        for (int b = l - a; b >= 0; --b) {
+          const int c = l - a - b;
+          ao_code[k] = a | (b << 4) | (c << 8) | (l << 12) | (slot << 16) | ((int)(sn - nb) << 24);
+          ++k;
+        }
+      if (ao_begin < 0 || k0 < ao_begin) ao_begin = k0;
+      if (k > ao_end) ao_end = k;
     }
     if (ao_begin < 0) { ao_begin = 0; ao_end = 0; }
     blocks.push_back(make_int4(nb, (int)n, (int)ao_begin, (int)ao_end));
