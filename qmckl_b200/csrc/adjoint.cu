@@ -44,6 +44,7 @@ constexpr int MODE_HESSIAN = 0, MODE_ADJOINT = 1;
 struct DerivSmem {
   double rad[kBlockSlots][4];   // R, R1, R2, R3 of the block's shells
   double nuc[kBlockNuc][4];     // displacement, r^2 (negative when screened out)
+  uint8_t act[kBlockSlots];     // the shells whose nucleus is in range
 };
 
 // x^a and its first three derivatives (Leibniz, one factor x at a time)
@@ -88,11 +89,15 @@ __device__ __forceinline__ void stage_deriv(const DevTables& T, DerivSmem& sm, c
     sm.nuc[lane][3] = in ? r2 : -1.0;
   }
   __syncwarp();
-  for (int s = slots.x + lane; s < slots.y; s += 32) {
+  // shells of screened-out nuclei are not staged (the AO loop tests the nucleus first)
+  const int nlive = pack_live_slots(T.slot_nuc, blk.x, slots, sm.nuc, sm.act, lane);
+  for (int i = lane; i < nlive; i += 32) {
+    const int ls = sm.act[i];
+    const int s = slots.x + ls;
     const int nucl = T.slot_nuc[s];
     const double r2 = sm.nuc[nucl - blk.x][3];
     double acc[4] = {0., 0., 0., 0.};
-    if (r2 >= 0.0) {
+    {
       const int2 cr = T.slot_coef[s];
       const int p0 = T.nuc_prim_start[nucl];
       for (int j = cr.x; j < cr.y; ++j) {
@@ -107,7 +112,6 @@ __device__ __forceinline__ void stage_deriv(const DevTables& T, DerivSmem& sm, c
         acc[3] -= a * a * a * ce;
       }
     }
-    const int ls = s - slots.x;
 #pragma unroll
     for (int c = 0; c < 4; ++c) sm.rad[ls][c] = acc[c];
   }

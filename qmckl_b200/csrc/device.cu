@@ -821,12 +821,15 @@ qmckl_exit_code run_mo_mixed(qmckl_context context, DeviceState* ds, int64_t P, 
     if (ok && tc_fused_smem(ds->tc, comps, ds->rec_bytes) <= 232448) {
       // spatial order of the points, then the fused AO -> MO kernel (the AO
       // pieces never leave shared memory)
-      const size_t obytes = sizeof(int) * 2 * (size_t)P + sizeof(unsigned int) * (kSortCells + 1);
+      // scratch: keys[P], perm[P], cell counts, then the tile plan (256-byte aligned)
+      const size_t sort_bytes = (sizeof(int) * 2 * (size_t)P + sizeof(unsigned int) * (kSortCells + 1) + 255) / 256 * 256;
+      const size_t obytes = sort_bytes + tc_tile_plan_bytes(ds->tc, P, comps);
       qmckl_exit_code rc = ensure(context, ds->order, obytes, "qmckl_b200_mo_mixed");
       if (rc != QMCKL_SUCCESS) return rc;
       int* keys = (int*)ds->order.p;
       int* perm = keys + P;
       unsigned int* counts = (unsigned int*)(perm + P);
+      void* tplan = (uint8_t*)ds->order.p + sort_bytes;
       double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
       const int64_t N = ctx->nucleus.num;
       for (int64_t n = 0; n < N; ++n)
@@ -849,7 +852,7 @@ qmckl_exit_code run_mo_mixed(qmckl_context context, DeviceState* ds, int64_t P, 
         QB_CUDA(point_order(coord + a, n, lo, hi, keys, counts, perm, ds->stream, P), "qmckl_b200_mo_mixed");
         QB_CUDA(tc_run_fused(ds->T, ds->tc, n, comps, coord + a, cutoff_of(ctx), ds->tc_coef.p, ds->krec.p,
                              ds->rec_bytes, perm, rb, o, ds->stream, P, ds->kskip.p,
-                             (unsigned long long*)ds->kstat.p),
+                             (unsigned long long*)ds->kstat.p, tplan),
                 "qmckl_b200_mo_mixed");
         if (cr != nullptr)
           QB_CUDA(launch_cusp_mo(n, comps, coord + a, P, NN, (const double*)ds->nucl.p, cr, cprm, MM, o, ds->stream),

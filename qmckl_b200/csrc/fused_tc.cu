@@ -44,7 +44,8 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
                 const int kblocks, const uint8_t* __restrict__ krec, const int rec_bytes,
                 const int* __restrict__ perm, const double* __restrict__ scales, const RowBound rb,
                 double* __restrict__ out, int* __restrict__ err, const int64_t cstride,
-                const uint8_t* __restrict__ kskip, unsigned long long* __restrict__ kstat) {
+                const uint8_t* __restrict__ kskip, unsigned long long* __restrict__ kstat,
+                const double* __restrict__ tpts, const int* __restrict__ tinfo) {
   constexpr int PTS = BM / COMPS;            // 25 points (VGL) or 128 (value)
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   // 1024-byte aligned base, kept as pointer arithmetic on the __shared__
@@ -84,14 +85,22 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
   for (int t = tid; t < 3 * PTS; t += kThreadsF) {
     const int d = t / PTS, i = t - d * PTS;
     const int64_t q = (p0 + i < P) ? (perm ? (int64_t)perm[p0 + i] : p0 + i) : -1;
-    pts[t] = q >= 0 ? coord[q + d * cstride] : 0.0;
+    // with a tile plan the coordinates come gathered in tile order
+    pts[t] = tpts != nullptr ? tpts[(size_t)blockIdx.x * 3 * PTS + t] : (q >= 0 ? coord[q + d * cstride] : 0.0);
     if (d == 0) pidx[i] = q;
     rexp[t] = PIECES == 2 ? kExpMin : 0;
+  }
+  if (tinfo != nullptr) {   // the tile's K-block list, made by tile_plan_kernel
+    const int* ti = tinfo + (size_t)blockIdx.x * (kblocks + 4);
+    for (int t = tid; t < kblocks + 4; t += kThreadsF) {
+      if (t < 4) nact_p[t] = ti[t];
+      else act[t - 4] = ti[t];
+    }
   }
   __syncthreads();
   if (PIECES == 2) row_exponents<PTS>(rb, pts, pidx, rexp, tid, kThreadsF);
   // K blocks that are not identically zero over the tile's points
-  {
+  if (tinfo == nullptr) {
     const int2* kb_sh = (const int2*)kskip;
     const double4* sph = (const double4*)(kskip + kskip_sph_offset(kblocks));
     for (int kb = warp; kb < kblocks; kb += kThreadsF / 32) {
@@ -115,7 +124,7 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
     }
   }
   __syncthreads();
-  if (tid == 0) {
+  if (tid == 0 && tinfo == nullptr) {
     int n = 0;
     int lo = -1, hi = -1;
     for (int kb = 0; kb < kblocks; ++kb)
@@ -218,6 +227,87 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
   }
 }
 
+// Tile plan: per tile of PTS points (in the order perm), the coordinates
+// gathered in tile order (tpts[tile][3][PTS]) and the K blocks that do not
+// vanish over the tile (tinfo[tile][kblocks + 4]: count, first block of each
+// half of K, first block, then the list, padded with 0), exactly as the fused
+// kernel's own prologue finds them.  One CTA per tile: the warps take K
+// blocks, the lanes the block's screening spheres, each tested against the
+// tile's points in shared memory (no chains of dependent loads).
+template <int PTS>
+__global__ void __launch_bounds__(256)
+tile_plan_kernel(const int64_t P, const double* __restrict__ coord, const int64_t cstride, const int* __restrict__ perm,
+                 const int kblocks, const uint8_t* __restrict__ kskip, double* __restrict__ tpts,
+                 int* __restrict__ tinfo, unsigned long long* __restrict__ kstat, const int n_tiles) {
+  __shared__ double spts[3 * PTS];
+  extern __shared__ int sflag[];   // [kblocks]
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int64_t tile = blockIdx.x;
+  const int64_t p0 = tile * PTS;
+  const int np = (int)(P - p0 < PTS ? P - p0 : PTS);
+  for (int t = tid; t < 3 * PTS; t += blockDim.x) {
+    const int d = t / PTS, i = t - d * PTS;
+    const int64_t q = i < np ? (perm ? (int64_t)perm[p0 + i] : p0 + i) : -1;
+    const double v = q >= 0 ? coord[q + d * cstride] : 0.0;
+    spts[t] = v;
+    tpts[tile * 3 * PTS + t] = v;
+  }
+  __syncthreads();
+  const int2* kb_sh = (const int2*)kskip;
+  const double4* sph = kskip ? (const double4*)(kskip + kskip_sph_offset(kblocks)) : nullptr;
+  for (int kb = warp; kb < kblocks; kb += (int)(blockDim.x >> 5)) {
+    bool live = kskip == nullptr;
+    if (!live) {
+      const int2 r = kb_sh[kb];
+      for (int q0 = r.x; q0 < r.y && !live; q0 += 32) {
+        bool l = false;
+        if (q0 + lane < r.y) {
+          const double4 c = sph[q0 + lane];
+          for (int i = 0; i < np && !l; ++i) {
+            const double x = spts[i] - c.x, y = spts[PTS + i] - c.y, z = spts[2 * PTS + i] - c.z;
+            l = x * x + y * y + z * z <= c.w;
+          }
+        }
+        live = __any_sync(0xffffffffu, l);
+      }
+    }
+    if (lane == 0) sflag[kb] = live ? 1 : 0;
+  }
+  __syncthreads();
+  if (warp != 0) return;
+  int* ti = tinfo + tile * (kblocks + 4);
+  int n = 0, lo = -1, hi = -1, first = -1;
+  for (int kb0 = 0; kb0 < kblocks; kb0 += 32) {
+    const int kb = kb0 + lane;
+    const bool f = kb < kblocks && sflag[kb] != 0;
+    const unsigned int m = __ballot_sync(0xffffffffu, f);
+    const unsigned int mlo = __ballot_sync(0xffffffffu, f && 2 * kb < kblocks);
+    const unsigned int mhi = __ballot_sync(0xffffffffu, f && 2 * kb >= kblocks);
+    if (f) ti[4 + n + __popc(m & ((1u << lane) - 1u))] = kb;
+    if (first < 0 && m != 0u) first = kb0 + __ffs(m) - 1;
+    if (lo < 0 && mlo != 0u) lo = kb0 + __ffs(mlo) - 1;
+    if (hi < 0 && mhi != 0u) hi = kb0 + __ffs(mhi) - 1;
+    n += __popc(m);
+  }
+  if (n == 0) {   // all outputs zero: one (zero) block initialises the accumulators
+    if (lane == 0) ti[4] = 0;
+    n = 1;
+    lo = 0;
+    first = 0;
+  }
+  for (int t = n + lane; t < kblocks; t += 32) ti[4 + t] = 0;
+  if (lane == 0) {
+    ti[0] = n;
+    ti[1] = lo;
+    ti[2] = hi;
+    ti[3] = first;
+    if (kstat != nullptr) {   // counted per CTA of the fused kernel: once per MO tile
+      atomicAdd(&kstat[0], (unsigned long long)n * n_tiles);
+      atomicAdd(&kstat[1], (unsigned long long)kblocks * n_tiles);
+    }
+  }
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (!fn) {
@@ -243,6 +333,8 @@ int* fused_err_word() {
   return words[dev];
 }
 
+size_t tile_plan_pts_bytes(int64_t tiles, int pts) { return ((size_t)tiles * 3 * pts * sizeof(double) + 255) / 256 * 256; }
+
 template <int PIECES, int COMPS>
 size_t fused_smem(int n_tile, int rec_bytes, int kblocks) {
   constexpr int PTS = BM / COMPS;
@@ -255,15 +347,27 @@ template <int PIECES, int COMPS>
 cudaError_t launch_fused(const DevTables& T, const CUtensorMap& tb, int64_t P, const double* coord, double cutoff,
                          int n_out, int n_tile, int n_tiles, int kblocks, const uint8_t* krec, int rec_bytes,
                          const int* perm, const double* scales, const RowBound& rb, double* out, int* err,
-                         int64_t cstride, const uint8_t* kskip, unsigned long long* kstat, cudaStream_t s) {
+                         int64_t cstride, const uint8_t* kskip, unsigned long long* kstat, void* tplan,
+                         cudaStream_t s) {
   constexpr int PTS = BM / COMPS;
   const size_t smem = fused_smem<PIECES, COMPS>(n_tile, rec_bytes, kblocks);
   auto kern = fused_mo_kernel<PIECES, COMPS>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  dim3 grid((unsigned)((P + PTS - 1) / PTS), (unsigned)n_tiles);
+  const int64_t tiles = (P + PTS - 1) / PTS;
+  double* tpts = nullptr;
+  int* tinfo = nullptr;
+  if (tplan != nullptr) {
+    tpts = (double*)tplan;
+    tinfo = (int*)((uint8_t*)tplan + tile_plan_pts_bytes(tiles, PTS));
+    tile_plan_kernel<PTS><<<(unsigned)tiles, 256, sizeof(int) * (size_t)kblocks, s>>>(
+        P, coord, cstride, perm, kblocks, kskip, tpts, tinfo, kstat, n_tiles);
+    count_launch();
+    kstat = nullptr;   // counted by the plan
+  }
+  dim3 grid((unsigned)tiles, (unsigned)n_tiles);
   kern<<<grid, kThreadsF, smem, s>>>(T, tb, P, coord, cutoff, n_out, n_tile, kblocks, krec, rec_bytes, perm, scales,
-                                     rb, out, err, cstride, kskip, kstat);
+                                     rb, out, err, cstride, kskip, kstat, tpts, tinfo);
   count_launch();
   return cudaGetLastError();
 }
@@ -275,6 +379,13 @@ size_t tc_fused_smem(const TcPlan& plan, int comps, int rec_bytes) {
   if (plan.pieces == 3)
     return comps == 5 ? fused_smem<3, 5>(plan.n_tile, rec_bytes, kb) : fused_smem<3, 1>(plan.n_tile, rec_bytes, kb);
   return comps == 5 ? fused_smem<2, 5>(plan.n_tile, rec_bytes, kb) : fused_smem<2, 1>(plan.n_tile, rec_bytes, kb);
+}
+
+size_t tc_tile_plan_bytes(const TcPlan& plan, int64_t point_num, int comps) {
+  const int pts = BM / comps;
+  const int64_t tiles = (point_num + pts - 1) / pts;
+  const int kb = (int)((plan.ao_num + BK - 1) / BK);
+  return tile_plan_pts_bytes(tiles, pts) + sizeof(int) * (size_t)tiles * (kb + 4);
 }
 
 size_t tc_kskip_bytes(int64_t ao_num, int64_t shell_num) {
@@ -298,7 +409,7 @@ cudaError_t tc_encode_coef_map(const TcPlan& plan, const void* d_coef, CUtensorM
 cudaError_t tc_launch_fused(const TcPlan& plan, int64_t point_num, int comps, const double* coord, double cutoff,
                             const CUtensorMap& tb, const void* krec, int rec_bytes, const int* perm, const void* d_coef,
                             const RowBound& rb, double* out, int* err, cudaStream_t s, int64_t cstride,
-                            const void* kskip, unsigned long long* kstat) {
+                            const void* kskip, unsigned long long* kstat, void* tplan) {
   if (point_num <= 0) return cudaSuccess;
   if (cstride < point_num) cstride = point_num;
   if (rec_bytes <= 0 || rec_bytes % 128 != 0) return cudaErrorInvalidValue;
@@ -310,19 +421,19 @@ cudaError_t tc_launch_fused(const TcPlan& plan, int64_t point_num, int comps, co
   const uint8_t* ks = (const uint8_t*)kskip;
   if (plan.pieces == 3)
     return comps == 5 ? launch_fused<3, 5>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
-                                           rec_bytes, perm, sc, rb, out, err, cstride, ks, kstat, s)
+                                           rec_bytes, perm, sc, rb, out, err, cstride, ks, kstat, tplan, s)
                       : launch_fused<3, 1>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
-                                           rec_bytes, perm, sc, rb, out, err, cstride, ks, kstat, s);
+                                           rec_bytes, perm, sc, rb, out, err, cstride, ks, kstat, tplan, s);
   return comps == 5 ? launch_fused<2, 5>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
-                                         rec_bytes, perm, sc, rb, out, err, cstride, ks, kstat, s)
+                                         rec_bytes, perm, sc, rb, out, err, cstride, ks, kstat, tplan, s)
                     : launch_fused<2, 1>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
-                                         rec_bytes, perm, sc, rb, out, err, cstride, ks, kstat, s);
+                                         rec_bytes, perm, sc, rb, out, err, cstride, ks, kstat, tplan, s);
 }
 
 cudaError_t tc_run_fused(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps, const double* coord,
                          double cutoff, const void* d_coef, const void* krec, int rec_bytes, const int* perm,
                          const RowBound& rb, double* out, cudaStream_t s, int64_t cstride, const void* kskip,
-                         unsigned long long* kstat) {
+                         unsigned long long* kstat, void* tplan) {
   (void)T;
   if (point_num <= 0) return cudaSuccess;
   CUtensorMap tb;
@@ -331,7 +442,7 @@ cudaError_t tc_run_fused(const DevTables& T, const TcPlan& plan, int64_t point_n
   int* err = fused_err_word();
   if (!err) return cudaErrorMemoryAllocation;
   e = tc_launch_fused(plan, point_num, comps, coord, cutoff, tb, krec, rec_bytes, perm, d_coef, rb, out, err, s, cstride,
-                      kskip, kstat);
+                      kskip, kstat, tplan);
   if (e != cudaSuccess) return e;
   int h = 0;
   e = cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s);

@@ -57,6 +57,24 @@ __device__ __forceinline__ bool cusp_masked(const double* cusp_r, int l, int nuc
   return strict ? (r < R) : (r <= R);
 }
 
+// Whole warp: the positions (relative to slots.x) of a nucleus block's shells
+// whose nucleus is in range of the point (nuc[.][3] >= 0), packed in slot
+// order into act; returns their count.  The radial staging then runs over
+// the live shells only, in as few 32-lane passes as they need.
+__device__ __forceinline__ int pack_live_slots(const int32_t* __restrict__ slot_nuc, int blk_first, int2 slots,
+                                               const double (*nuc)[4], uint8_t* act, int lane) {
+  int n = 0;
+  for (int s0 = slots.x; s0 < slots.y; s0 += 32) {
+    const int s = s0 + lane;
+    const bool live = s < slots.y && nuc[slot_nuc[s] - blk_first][3] >= 0.0;
+    const unsigned int m = __ballot_sync(0xffffffffu, live);
+    if (live) act[n + __popc(m & ((1u << lane) - 1u))] = (uint8_t)(s - slots.x);
+    n += __popc(m);
+  }
+  __syncwarp();
+  return n;
+}
+
 // AO kernels (ao_kernels.cu).  coord is [3][point_num].  All return
 // cudaGetLastError() after the launch.
 // cusp_r (optional, [nucl]): the AOs that the cusp adjustment leaves out of

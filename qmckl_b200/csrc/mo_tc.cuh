@@ -66,12 +66,16 @@ cudaError_t tc_run(const DevTables& T, const TcPlan& plan, int64_t point_num, in
 // rb: the per-row scale bounds of 2-piece float16 operands (fused_common.cuh).
 // kskip (optional): the tile-skipping tables of the K blocks (fused_tc.cu),
 // tc_kskip_bytes long; kstat (optional): two device counters to which every
-// CTA adds its evaluated K blocks and the dense count.
+// tile adds its evaluated K blocks and the dense count.  tplan (optional,
+// tc_tile_plan_bytes of scratch): a small kernel first gathers each tile's
+// coordinates and finds its K blocks, so that the fused kernel's CTAs start
+// on their pipeline at once (the same blocks, the same results).
 cudaError_t tc_run_fused(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps, const double* coord,
                          double cutoff, const void* d_coef, const void* krec, int rec_bytes, const int* perm,
                          const fz::RowBound& rb, double* out, cudaStream_t s, int64_t cstride = -1,
-                         const void* kskip = nullptr, unsigned long long* kstat = nullptr);
+                         const void* kskip = nullptr, unsigned long long* kstat = nullptr, void* tplan = nullptr);
 size_t tc_kskip_bytes(int64_t ao_num, int64_t shell_num);
+size_t tc_tile_plan_bytes(const TcPlan& plan, int64_t point_num, int comps);
 // TMA map of a plan's coefficient pieces (box: 64 AOs x n_tile MOs x 1 piece,
 // 128B swizzle) and a launch of the fused kernel that does not wait for it
 // (err: device error word, left for the caller to check).
@@ -79,7 +83,7 @@ cudaError_t tc_encode_coef_map(const TcPlan& plan, const void* d_coef, CUtensorM
 cudaError_t tc_launch_fused(const TcPlan& plan, int64_t point_num, int comps, const double* coord, double cutoff,
                             const CUtensorMap& map, const void* krec, int rec_bytes, const int* perm, const void* d_coef,
                             const fz::RowBound& rb, double* out, int* err, cudaStream_t s, int64_t cstride = -1,
-                            const void* kskip = nullptr, unsigned long long* kstat = nullptr);
+                            const void* kskip = nullptr, unsigned long long* kstat = nullptr, void* tplan = nullptr);
 // Spatial order of points (32^3 cells over [box_lo, box_hi], Morton order) by
 // a counting sort: perm[P]; keys[P] and counts[kSortCells + 1] are scratch.
 // cstride: distance between the x, y and z blocks of coord (default
