@@ -370,6 +370,48 @@ __device__ __forceinline__ void epilogue_warp(uint32_t tmem, int n_tile, int n0,
   }
 }
 
+// Epilogue into shared memory: TMEM lane quadrant warp % 4, a share of the
+// 16-column chunks, as epilogue_warp; row r (= point * COMPS + component) of
+// the tile goes to stg + r * ldst in the same arithmetic.  ldst = n_tile + 2
+// puts the 16-byte stores of a warp's 32 rows on 8 distinct bank groups.  The
+// caller copies each row to its place in global memory with one bulk copy.
+template <int PIECES, int COMPS>
+__device__ __forceinline__ void epilogue_stage_warp(uint32_t tmem, int n_tile, int n0, int n_out, bool has_second,
+                                                    const int* rexp, const double* scales, double* stg, int ldst,
+                                                    int warp, int lane, int chunk0, int chunk_step, bool has_first) {
+  constexpr int PTS = BM / COMPS;
+  const int row_base = (warp & 3) * 32;
+  const int r = row_base + lane;
+  const bool row_ok = r < PTS * COMPS;
+  const double rs = (PIECES == 2 && row_ok) ? pow2d(rexp[comp_group<COMPS>(r % COMPS) * PTS + r / COMPS]) : 1.0;
+  for (int c0 = 16 * chunk0; c0 < n_tile; c0 += 16 * chunk_step) {
+    uint32_t r0[16], r1[16], r2[16];
+    const uint32_t ta = tmem + ((uint32_t)row_base << 16) + (uint32_t)c0;
+    tmem_ld16(ta, r0);
+    tmem_ld16(ta + (uint32_t)n_tile, r1);
+    tmem_ld16(ta + (uint32_t)(2 * n_tile), r2);
+    if (row_ok) {
+      double* dst = stg + (size_t)r * ldst + c0;
+#pragma unroll
+      for (int j = 0; j < 16; j += 2) {
+        double v[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          double x = has_first ? (double)__uint_as_float(r0[j + h]) + (double)__uint_as_float(r2[j + h])
+                               : (double)__uint_as_float(r2[j + h]);
+          if (has_second) x += (double)__uint_as_float(r1[j + h]);
+          if (PIECES == 2) {
+            const int col = n0 + c0 + j + h;
+            x *= (col < n_out ? scales[kScaleCols + col] : 1.0) * rs;
+          }
+          v[h] = x;
+        }
+        *reinterpret_cast<double2*>(dst + j) = make_double2(v[0], v[1]);
+      }
+    }
+  }
+}
+
 // Zero the rows PTS*COMPS .. 127 of every A tile (they stay zero).
 template <int PIECES, int COMPS, int STAGES>
 __device__ __forceinline__ void zero_pad_rows(uint8_t* smem, int stage_bytes, int tid, int nthreads) {
