@@ -261,42 +261,10 @@ batch_mo_kernel(const BatchDesc* __restrict__ desc, const CUtensorMap* __restric
     int* act = (int*)(&C + 1);
     int* kflag = act + kb_max;
     int* kcnt = kflag + kb_max;
-    {
-      const int2* kb_sh = (const int2*)D.kskip;
-      const double4* sph = (const double4*)(D.kskip + kskip_sph_offset(kblocks));
-      for (int kb = warp; kb < kblocks; kb += NTHREADS / 32) {
-        bool live = false;
-        const int2 r = kb_sh[kb];
-        if (lane < kPts && p0 + lane < P) {
-          const double px = C.pts[lane], py = C.pts[kPts + lane], pz = C.pts[2 * kPts + lane];
-          for (int q = r.x; q < r.y && !live; ++q) {
-            const double4 c = sph[q];
-            const double x = px - c.x, y = py - c.y, z = pz - c.z;
-            live = x * x + y * y + z * z <= c.w;
-          }
-        }
-        live = __any_sync(0xffffffffu, live);
-        if (lane == 0) kflag[kb] = live ? 1 : 0;
-      }
-    }
+    tile_kblock_flags<kPts>(D.kskip, kblocks, C.pts, (int)(P - p0 < kPts ? P - p0 : kPts), kflag, warp, lane,
+                            NTHREADS / 32);
     __syncthreads();
-    if (tid == 0) {
-      int n = 0, lo = -1, hi = -1;
-      for (int kb = 0; kb < kblocks; ++kb)
-        if (kflag[kb]) {
-          act[n++] = kb;
-          if (2 * kb >= kblocks) { if (hi < 0) hi = kb; }
-          else if (lo < 0) lo = kb;
-        }
-      if (n == 0) {
-        act[n++] = 0;
-        lo = 0;
-      }
-      kcnt[0] = n;
-      kcnt[1] = lo;
-      kcnt[2] = hi;
-      kcnt[3] = act[0];
-    }
+    if (warp == 0) tile_kblock_list(kflag, kblocks, act, kcnt, lane);
     __syncthreads();
     const int nact = kcnt[0];
     if (warp < PRODW) {
@@ -345,16 +313,42 @@ batch_mo_kernel(const BatchDesc* __restrict__ desc, const CUtensorMap* __restric
       }
     }
     if (warp < PRODW) {
-      // epilogue: every producer warp, TMEM lane quadrant warp % 4 (its
-      // staging scratch overlaps the zero rows of the first A tile; those
-      // rows only feed accumulator rows that are never stored)
+      // epilogue: every producer warp, TMEM lane quadrant warp % 4.  The
+      // stage memory is idle until the next item: the tile's rows are staged
+      // there and each leaves in one bulk copy when they fit and are 16-byte
+      // aligned in global memory, else each warp writes its rows through a
+      // small staging buffer.  Either staging overwrites the zero rows of
+      // the A tiles; those rows only feed accumulator rows that are never
+      // stored.
       bool ok = mbar_wait(&C.acc_full, ntiles & 1u, err, 24);
       ok = __all_sync(0xffffffffu, ok && *(volatile int*)err == 0);
       tc_fence_after();
-      if (ok)
-        epilogue_warp<PIECES, COMPS>(tmem, n_tile, n0, D.n_out, kcnt[2] >= 0, C.pidx, C.rexp, D.scales,
-                                     out + D.out_off, (double*)smem + warp * 32 * 16, warp, lane, warp >> 2,
-                                     PRODW / 4, kcnt[1] >= 0);
+      double* o = out + D.out_off;
+      const int ldst = n_tile + 2;
+      const bool bulk = (size_t)BM * ldst * sizeof(double) <= (size_t)kStages * STAGE && (D.n_out & 1) == 0 &&
+                        (reinterpret_cast<uintptr_t>(o) & 15) == 0;
+      if (bulk) {
+        double* stg = (double*)smem;
+        if (ok)
+          epilogue_stage_warp<PIECES, COMPS>(tmem, n_tile, n0, D.n_out, kcnt[2] >= 0, C.rexp, D.scales, stg, ldst,
+                                             warp, lane, warp >> 2, PRODW / 4, kcnt[1] >= 0);
+        fence_async_smem();
+        named_bar_sync(1, NPROD);   // all producer warps arrive, whatever their `ok`
+        if (ok) {
+          const int ncols = min(n_tile, D.n_out - n0);
+          for (int r = tid; r < kPts * COMPS; r += NPROD) {
+            const int64_t pq = C.pidx[r / COMPS];
+            if (pq >= 0)
+              bulk_store(o + (pq * COMPS + r % COMPS) * D.n_out + n0, stg + (size_t)r * ldst, (uint32_t)ncols * 8u);
+          }
+          bulk_commit();
+          bulk_wait_read();
+        }
+      } else if (ok) {
+        epilogue_warp<PIECES, COMPS>(tmem, n_tile, n0, D.n_out, kcnt[2] >= 0, C.pidx, C.rexp, D.scales, o,
+                                     (double*)smem + warp * 32 * 16, warp, lane, warp >> 2, PRODW / 4,
+                                     kcnt[1] >= 0);
+      }
     }
     kbase += (uint32_t)nact;
     ++ntiles;

@@ -201,6 +201,69 @@ __device__ __forceinline__ void ao_product(int code, float f, const float (&s)[5
 // p_first: index of the tile's first point among the P points (rows past P
 // are written as zeros).  Pairs of AOs that are zero at every point of the
 // warp skip the split arithmetic.
+// Tile skipping.  flags[kb] = 1 when some shell of K block kb reaches one of
+// the tile's np points (pts: [3][PTS]), by the kskip tables (null: every
+// block).  Warp w of nwarps takes blocks w, w + nwarps, ...; its lanes take
+// the block's screening spheres, each tested against the points in shared
+// memory (one load per lane, no chain of dependent loads).
+template <int PTS>
+__device__ __forceinline__ void tile_kblock_flags(const uint8_t* kskip, int kblocks, const double* pts, int np,
+                                                  int* flags, int warp, int lane, int nwarps) {
+  const int2* kb_sh = (const int2*)kskip;
+  const double4* sph = kskip ? (const double4*)(kskip + kskip_sph_offset(kblocks)) : nullptr;
+  for (int kb = warp; kb < kblocks; kb += nwarps) {
+    bool live = kskip == nullptr;
+    if (!live) {
+      const int2 r = kb_sh[kb];
+      for (int q0 = r.x; q0 < r.y && !live; q0 += 32) {
+        bool l = false;
+        if (q0 + lane < r.y) {
+          const double4 c = sph[q0 + lane];
+          for (int i = 0; i < np && !l; ++i) {
+            const double x = pts[i] - c.x, y = pts[PTS + i] - c.y, z = pts[2 * PTS + i] - c.z;
+            l = x * x + y * y + z * z <= c.w;
+          }
+        }
+        live = __any_sync(0xffffffffu, l);
+      }
+    }
+    if (lane == 0) flags[kb] = live ? 1 : 0;
+  }
+}
+
+// One warp: the flagged K blocks in order into act[], and cnt[0..3] = their
+// count, the first block of each half of K (-1: none) and the first block.
+// With no block alive, one (zero) block 0 initialises the accumulators.
+// Returns the count.
+__device__ __forceinline__ int tile_kblock_list(const int* flags, int kblocks, int* act, int* cnt, int lane) {
+  int n = 0, lo = -1, hi = -1, first = -1;
+  for (int kb0 = 0; kb0 < kblocks; kb0 += 32) {
+    const int kb = kb0 + lane;
+    const bool f = kb < kblocks && flags[kb] != 0;
+    const unsigned int m = __ballot_sync(0xffffffffu, f);
+    const unsigned int mlo = __ballot_sync(0xffffffffu, f && 2 * kb < kblocks);
+    const unsigned int mhi = __ballot_sync(0xffffffffu, f && 2 * kb >= kblocks);
+    if (f) act[n + __popc(m & ((1u << lane) - 1u))] = kb;
+    if (first < 0 && m != 0u) first = kb0 + __ffs(m) - 1;
+    if (lo < 0 && mlo != 0u) lo = kb0 + __ffs(mlo) - 1;
+    if (hi < 0 && mhi != 0u) hi = kb0 + __ffs(mhi) - 1;
+    n += __popc(m);
+  }
+  if (n == 0) {
+    if (lane == 0) act[0] = 0;
+    n = 1;
+    lo = 0;
+    first = 0;
+  }
+  if (lane == 0) {
+    cnt[0] = n;
+    cnt[1] = lo;
+    cnt[2] = hi;
+    cnt[3] = first;
+  }
+  return n;
+}
+
 template <int PIECES, int COMPS, int CHUNK>
 __device__ __forceinline__ void produce_kblock(const uint8_t* rec, const double* pts, int64_t p_first, int64_t P,
                                                double cutoff, const int* rexp, uint32_t a_base, int j, int lane) {

@@ -101,50 +101,15 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
   if (PIECES == 2) row_exponents<PTS>(rb, pts, pidx, rexp, tid, kThreadsF);
   // K blocks that are not identically zero over the tile's points
   if (tinfo == nullptr) {
-    const int2* kb_sh = (const int2*)kskip;
-    const double4* sph = (const double4*)(kskip + kskip_sph_offset(kblocks));
-    for (int kb = warp; kb < kblocks; kb += kThreadsF / 32) {
-      bool live = kskip == nullptr;
-      if (!live) {
-        const int2 r = kb_sh[kb];
-        for (int g = 0; g < (PTS + 31) / 32; ++g) {
-          const int i = lane + 32 * g;
-          if (i < PTS && p0 + i < P) {
-            const double px = pts[i], py = pts[PTS + i], pz = pts[2 * PTS + i];
-            for (int q = r.x; q < r.y && !live; ++q) {
-              const double4 c = sph[q];
-              const double x = px - c.x, y = py - c.y, z = pz - c.z;
-              live = x * x + y * y + z * z <= c.w;
-            }
-          }
-        }
+    tile_kblock_flags<PTS>(kskip, kblocks, pts, (int)(P - p0 < PTS ? P - p0 : PTS), kflag, warp, lane, kThreadsF / 32);
+    __syncthreads();
+    if (warp == 0) {
+      const int n = tile_kblock_list(kflag, kblocks, act, nact_p, lane);
+      if (kstat != nullptr && lane == 0) {   // K blocks evaluated / in the dense contraction, summed over CTAs
+        atomicAdd(&kstat[0], (unsigned long long)n);
+        atomicAdd(&kstat[1], (unsigned long long)kblocks);
       }
-      live = __any_sync(0xffffffffu, live);
-      if (lane == 0) kflag[kb] = live ? 1 : 0;
     }
-  }
-  __syncthreads();
-  if (tid == 0 && tinfo == nullptr) {
-    int n = 0;
-    int lo = -1, hi = -1;
-    for (int kb = 0; kb < kblocks; ++kb)
-      if (kflag[kb]) {
-        act[n++] = kb;
-        if (2 * kb >= kblocks) { if (hi < 0) hi = kb; }
-        else if (lo < 0) lo = kb;
-      }
-    if (n == 0) {   // all outputs zero: one (zero) block initialises the accumulators
-      act[n++] = 0;
-      lo = 0;
-    }
-    if (kstat != nullptr) {   // K blocks evaluated / in the dense contraction, summed over CTAs
-      atomicAdd(&kstat[0], (unsigned long long)n);
-      atomicAdd(&kstat[1], (unsigned long long)kblocks);
-    }
-    nact_p[0] = n;
-    nact_p[1] = lo;   // -1: no block of the first half (accumulator 0 unused)
-    nact_p[2] = hi;   // -1: none of the second half
-    nact_p[3] = act[0];
   }
   // rows PTS*COMPS .. 127 of the A tiles stay zero for the whole kernel
   zero_pad_rows<PIECES, COMPS, STAGES>(smem, STAGE, tid, kThreadsF);
@@ -278,54 +243,13 @@ tile_plan_kernel(const int64_t P, const double* __restrict__ coord, const int64_
     tpts[tile * 3 * PTS + t] = v;
   }
   __syncthreads();
-  const int2* kb_sh = (const int2*)kskip;
-  const double4* sph = kskip ? (const double4*)(kskip + kskip_sph_offset(kblocks)) : nullptr;
-  for (int kb = warp; kb < kblocks; kb += (int)(blockDim.x >> 5)) {
-    bool live = kskip == nullptr;
-    if (!live) {
-      const int2 r = kb_sh[kb];
-      for (int q0 = r.x; q0 < r.y && !live; q0 += 32) {
-        bool l = false;
-        if (q0 + lane < r.y) {
-          const double4 c = sph[q0 + lane];
-          for (int i = 0; i < np && !l; ++i) {
-            const double x = spts[i] - c.x, y = spts[PTS + i] - c.y, z = spts[2 * PTS + i] - c.z;
-            l = x * x + y * y + z * z <= c.w;
-          }
-        }
-        live = __any_sync(0xffffffffu, l);
-      }
-    }
-    if (lane == 0) sflag[kb] = live ? 1 : 0;
-  }
+  tile_kblock_flags<PTS>(kskip, kblocks, spts, np, sflag, warp, lane, (int)(blockDim.x >> 5));
   __syncthreads();
   if (warp != 0) return;
   int* ti = tinfo + tile * (kblocks + 4);
-  int n = 0, lo = -1, hi = -1, first = -1;
-  for (int kb0 = 0; kb0 < kblocks; kb0 += 32) {
-    const int kb = kb0 + lane;
-    const bool f = kb < kblocks && sflag[kb] != 0;
-    const unsigned int m = __ballot_sync(0xffffffffu, f);
-    const unsigned int mlo = __ballot_sync(0xffffffffu, f && 2 * kb < kblocks);
-    const unsigned int mhi = __ballot_sync(0xffffffffu, f && 2 * kb >= kblocks);
-    if (f) ti[4 + n + __popc(m & ((1u << lane) - 1u))] = kb;
-    if (first < 0 && m != 0u) first = kb0 + __ffs(m) - 1;
-    if (lo < 0 && mlo != 0u) lo = kb0 + __ffs(mlo) - 1;
-    if (hi < 0 && mhi != 0u) hi = kb0 + __ffs(mhi) - 1;
-    n += __popc(m);
-  }
-  if (n == 0) {   // all outputs zero: one (zero) block initialises the accumulators
-    if (lane == 0) ti[4] = 0;
-    n = 1;
-    lo = 0;
-    first = 0;
-  }
+  const int n = tile_kblock_list(sflag, kblocks, ti + 4, ti, lane);
   for (int t = n + lane; t < kblocks; t += 32) ti[4 + t] = 0;
   if (lane == 0) {
-    ti[0] = n;
-    ti[1] = lo;
-    ti[2] = hi;
-    ti[3] = first;
     if (kstat != nullptr) {   // counted per CTA of the fused kernel: once per MO tile
       atomicAdd(&kstat[0], (unsigned long long)n * n_tiles);
       atomicAdd(&kstat[1], (unsigned long long)kblocks * n_tiles);
