@@ -160,7 +160,63 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     bool ok = mbar_wait(acc_full, 0, err, 3);
     ok = __all_sync(0xffffffffu, ok && *(volatile int*)err == 0);   // warp-uniform for tcgen05.ld
     tc_fence_after();
-    if (ok) {
+    // When the tile's rows fit in the idle stage memory and are 16-byte
+    // aligned in `out`, they are staged there (rows padded by 16 bytes, so a
+    // warp's 16-byte stores fall on distinct banks) and each row leaves in
+    // one bulk copy; otherwise each warp writes its rows through a small
+    // staging buffer.
+    constexpr int kPadT = 16 / (int)sizeof(OutT);
+    const int ldst = n_tile + kPadT;
+    const int ncols = n_out - n0 < n_tile ? n_out - n0 : n_tile;
+    const bool bulk = (size_t)BM * ldst * sizeof(OutT) <= (size_t)STAGES * STAGE &&
+                      ((size_t)ncols * sizeof(OutT)) % 16 == 0 && ((size_t)ldo * sizeof(OutT)) % 16 == 0 &&
+                      (reinterpret_cast<uintptr_t>(out) & 15) == 0;
+    if (bulk) {
+      OutT* stg = (OutT*)smem;
+      const int r = warp * 32 + lane;   // this thread's TMEM lane = tile row
+      const int64_t row = m0 + r;
+      const bool has_second = !TWO_ACC && kblocks >= 2;
+      if (ok) {
+        for (int c0 = 0; c0 < n_tile; c0 += 16) {
+          uint32_t r0[16], r1[16], r2[16];
+          const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+          tmem_ld16(ta, r0);
+          if (has_second) tmem_ld16(ta + (uint32_t)n_tile, r1);
+          tmem_ld16(ta + (uint32_t)((NACC - 1) * n_tile), r2);
+          OutT vals[16];
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            double v = (double)__uint_as_float(r0[j]) + (double)__uint_as_float(r2[j]);
+            if (has_second) v += (double)__uint_as_float(r1[j]);
+            if constexpr (PIECES == 2) {
+              const int col = n0 + c0 + j;
+              v *= scales[(int)(row % comps)] * (col < n_out ? scales[kScaleCols + col] : 1.0);
+            }
+            vals[j] = (OutT)v;
+          }
+          uint4* dst = reinterpret_cast<uint4*>(stg + (size_t)r * ldst + c0);
+          if constexpr (sizeof(OutT) == 4) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+              dst[q] = make_uint4(__float_as_uint(vals[4 * q]), __float_as_uint(vals[4 * q + 1]),
+                                  __float_as_uint(vals[4 * q + 2]), __float_as_uint(vals[4 * q + 3]));
+          } else {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              const unsigned long long a = __double_as_longlong(vals[2 * q]), b = __double_as_longlong(vals[2 * q + 1]);
+              dst[q] = make_uint4((uint32_t)a, (uint32_t)(a >> 32), (uint32_t)b, (uint32_t)(b >> 32));
+            }
+          }
+        }
+      }
+      fence_async_smem();
+      named_bar_sync(1, kEpiWarps * 32);   // all epilogue warps arrive, whatever their `ok`
+      if (ok && row < M) {
+        bulk_store(out + row * ldo + n0, stg + (size_t)r * ldst, (uint32_t)(ncols * sizeof(OutT)));
+        bulk_commit();
+        bulk_wait_read();
+      }
+    } else if (ok) {
       double* stage = (double*)smem + warp * 32 * 16;     // [32 rows][16 cols] per warp; stages are idle now
       const int row_base = warp * 32;
       const bool has_second = !TWO_ACC && kblocks >= 2;
