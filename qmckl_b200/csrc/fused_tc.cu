@@ -73,7 +73,18 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
   uint32_t tmem_cols = 32;
   while ((int)tmem_cols < 3 * n_tile) tmem_cols <<= 1;
 
-  if (tid == 0) {
+  // loads of K block kb (the it-th of the tile) into stage it % STAGES: the
+  // block's record and its coefficient pieces
+  auto issue_loads = [&](int it, int kb) {
+    const int s = it & 1;
+    mbar_expect_tx(&rec_full[s], (uint32_t)rec_bytes);
+    bulk_load(recs + s * rec_bytes, krec + (size_t)kb * rec_bytes, (uint32_t)rec_bytes, &rec_full[s]);
+    uint8_t* st = smem + s * STAGE + A_BYTES;
+    mbar_expect_tx(&full[s], (uint32_t)(PIECES * B_TILE));
+    for (int q = 0; q < PIECES; ++q) tma_load_3d(st + q * B_TILE, &tmB, &full[s], kb * BK, n0, q);
+  };
+  int tma_pre = 0;   // K blocks whose loads the TMA thread issued during the prologue
+  if (tid == kTmaWarp * 32) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(&full[s], kProd + 1);
       mbar_init(&empty[s], 1);
@@ -81,6 +92,14 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
     }
     mbar_init(acc_full, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    if (tinfo != nullptr) {
+      // with a tile plan the first K blocks are known at once: their loads
+      // (into stages not used yet, nothing to wait for) run under the prologue
+      const int* ti = tinfo + (size_t)blockIdx.x * (kblocks + 4);
+      const int n = ti[0];
+      tma_pre = n < STAGES ? n : STAGES;
+      for (int it = 0; it < tma_pre; ++it) issue_loads(it, ti[4 + it]);
+    }
   }
   for (int t = tid; t < 3 * PTS; t += kThreadsF) {
     const int d = t / PTS, i = t - d * PTS;
@@ -144,16 +163,11 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
   } else if (warp == kTmaWarp) {
     // ---------------- coefficient pieces
     if (lane == 0) {
-      for (int it = 0; it < nact; ++it) {
-        const int kb = act[it];
+      for (int it = tma_pre; it < nact; ++it) {
         const int s = it & 1;
         const uint32_t phase = (uint32_t)(it >> 1) & 1u;
         if (!mbar_wait(&empty[s], phase ^ 1u, err, 12)) break;
-        mbar_expect_tx(&rec_full[s], (uint32_t)rec_bytes);
-        bulk_load(recs + s * rec_bytes, krec + (size_t)kb * rec_bytes, (uint32_t)rec_bytes, &rec_full[s]);
-        uint8_t* st = smem + s * STAGE + A_BYTES;
-        mbar_expect_tx(&full[s], (uint32_t)(PIECES * B_TILE));
-        for (int q = 0; q < PIECES; ++q) tma_load_3d(st + q * B_TILE, &tmB, &full[s], kb * BK, n0, q);
+        issue_loads(it, act[it]);
       }
     }
   } else {
@@ -442,26 +456,45 @@ __global__ void point_keys_kernel(const double* __restrict__ coord, int64_t P, i
   }
 }
 
-// exclusive scan of kSortCells counts in one CTA of 1024 threads
+// exclusive scan of kSortCells counts in one CTA of 1024 threads: warp w
+// scans cells [1024 w, 1024 w + 1024) as 32 rows of 32 (coalesced loads and
+// stores, shuffles within a row, a carry from row to row), then the warps'
+// totals are scanned and added
 __global__ void __launch_bounds__(1024) scan_cells_kernel(unsigned int* counts) {
-  constexpr int PER = kSortCells / 1024;
-  __shared__ unsigned int part[1024];
-  unsigned int local[PER];
-  unsigned int sum = 0;
-  const int base = threadIdx.x * PER;
+  static_assert(kSortCells == 32 * 1024, "32 warps x 32 rows x 32 cells");
+  __shared__ unsigned int wbase[32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  unsigned int* c = counts + warp * 1024;
+  unsigned int v[32];
+  unsigned int carry = 0u;
 #pragma unroll
-  for (int i = 0; i < PER; ++i) { local[i] = counts[base + i]; sum += local[i]; }
-  part[threadIdx.x] = sum;
-  __syncthreads();
-  for (int off = 1; off < 1024; off <<= 1) {
-    const unsigned int v = threadIdx.x >= off ? part[threadIdx.x - off] : 0u;
-    __syncthreads();
-    part[threadIdx.x] += v;
-    __syncthreads();
+  for (int i = 0; i < 32; ++i) {
+    const unsigned int x = c[32 * i + lane];
+    unsigned int y = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned int t = __shfl_up_sync(0xffffffffu, y, o);
+      if (lane >= o) y += t;
+    }
+    v[i] = carry + y - x;
+    carry += __shfl_sync(0xffffffffu, y, 31);
   }
-  unsigned int run = part[threadIdx.x] - sum;
+  if (lane == 0) wbase[warp] = carry;
+  __syncthreads();
+  if (warp == 0) {
+    const unsigned int x = wbase[lane];
+    unsigned int y = x;
 #pragma unroll
-  for (int i = 0; i < PER; ++i) { counts[base + i] = run; run += local[i]; }
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned int t = __shfl_up_sync(0xffffffffu, y, o);
+      if (lane >= o) y += t;
+    }
+    wbase[lane] = y - x;
+  }
+  __syncthreads();
+  const unsigned int base = wbase[warp];
+#pragma unroll
+  for (int i = 0; i < 32; ++i) c[32 * i + lane] = base + v[i];
 }
 
 __global__ void scatter_points_kernel(const int* __restrict__ keys, int64_t P, unsigned int* __restrict__ offsets,
