@@ -507,7 +507,7 @@ def main():
         executed = 2.0 * (kb_eval / args.steps) * 128 * n_tile * 64 * nprod
         t = traffic.get(("fused_mo_kernel", "mixed"))
         kname = ("fused_mo_kernel<3,5> (AO -> split-BF16 tcgen05 MO VGL" if args.pieces == 3 else
-                 "fused_mo_kernel<2,5> (AO -> split-FP16 tcgen05 MO VGL") + "; step = 3 ordering kernels + this)"
+                 "fused_mo_kernel<2,5> (AO -> split-FP16 tcgen05 MO VGL") + "; step = 3 ordering kernels + tile plan + this)"
         if args.unfused:
             # AO pieces to HBM, then 128-row tiles of the 5P x A pieces matrix x 6 products
             executed = 2.0 * (-(-5 * P // 128) * 128) * (n_tile * n_tiles) * (-(-A // 64) * 64) * 6
