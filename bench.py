@@ -108,29 +108,71 @@ class ClockSampler:
                 "reasons": sorted(self.reasons), "samples": len(self.samples), "source": "NVML, 10 ms polling"}
 
 
-def cpu_baseline(sysd, seconds=15.0, nthreads=0):
-    """Time the CPU oracle (a restatement of the reference's C HPC path) on a bounded sample."""
-    from oracle import pyoracle as O
-    pts = sysd["elec_coord"].reshape(-1, 3)
-    b = O.Basis(sysd)
-    nthreads = nthreads or os.cpu_count() or 1
-    n = 64
-    done, t_total = 0, 0.0
+def physical_cores():
+    """(physical cores, how counted): unique (core, socket) pairs of lscpu, else os.cpu_count()."""
+    import subprocess
+    try:
+        out = subprocess.run(["lscpu", "-p=CORE,SOCKET"], capture_output=True, text=True, timeout=10).stdout
+        pairs = {tuple(line.split(",")) for line in out.splitlines() if line and not line.startswith("#")}
+        if pairs:
+            return len(pairs), "physical (lscpu)"
+    except Exception:
+        pass
+    return os.cpu_count() or 1, "logical (os.cpu_count)"
+
+
+def _cpu_rate(evaluate, pts, seconds, first_chunk):
+    """points/s of evaluate(chunk) over chunks of the workload's points until `seconds` have passed."""
+    n, done, t_total = first_chunk, 0, 0.0
     while t_total < seconds and done < pts.shape[0]:
         chunk = pts[done:done + n]
         t0 = time.perf_counter()
-        ao = O.ao_vgl(b, chunk, sysd["nucl_coord"], nthreads=nthreads)
-        O.mo_vgl(sysd["mo_coef"], ao, nthreads=nthreads)
+        evaluate(chunk)
         t_total += time.perf_counter() - t0
         done += chunk.shape[0]
-        n = min(2 * n, 4096)
-    return {"value": done / t_total, "unit": "electron-points/s", "cores": nthreads, "kind": "port",
-            "sample": f"{done} of {pts.shape[0]} points of the workload, AO VGL + MO VGL, {t_total:.1f} s"}
+        n = min(2 * n, 8192)
+    return done / t_total, done, t_total
+
+
+def cpu_baseline(sysd, seconds=12.0, nthreads=0, single_thread_seconds=4.0):
+    """Time the CPU path on a bounded sample of the workload's points: the
+    reference's own C HPC kernels when they were built into oracle/_ref,
+    else the oracle (a restatement of the same path); all physical cores,
+    plus a 1-thread figure."""
+    from oracle import pyoracle as O
+    pts = sysd["elec_coord"].reshape(-1, 3)
+    cores, how = physical_cores()
+    nthreads = nthreads or cores
+    ref = None
+    try:
+        from oracle import refpath
+        ref = refpath.RefSystem(sysd) if refpath.available() else None
+    except Exception:
+        ref = None
+    if ref is not None:
+        kind, what = "reference", "the reference's C HAVE_HPC kernels (oracle/_ref)"
+        evaluate = lambda c, t: ref.mo_vgl(c, nthreads=t)
+    else:
+        kind, what = "port", "the oracle (C restatement of the reference's HPC path)"
+        b = O.Basis(sysd)
+        evaluate = lambda c, t: O.mo_vgl(sysd["mo_coef"], O.ao_vgl(b, c, sysd["nucl_coord"], nthreads=t), nthreads=t)
+    v, done, t = _cpu_rate(lambda c: evaluate(c, nthreads), pts, seconds, 16 * nthreads)
+    v1, done1, t1 = _cpu_rate(lambda c: evaluate(c, 1), pts, single_thread_seconds, 64)
+    return {"value": v, "unit": "electron-points/s", "cores": nthreads, "cores_counted": how, "kind": kind,
+            "sample": f"{done} of {pts.shape[0]} points of the workload, AO VGL + MO VGL by {what}, {t:.1f} s",
+            "single_thread": {"value": v1, "sample": f"{done1} points, {t1:.1f} s"}}
+
+
+def workload_config(P, A, M, world):
+    """The config dict both arms print (identical keys and values)."""
+    return {"workload": WORKLOAD, "points": P, "ao_num": A, "mo_num": M,
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "l2": "GPU arm: L2 flushed (256 MB write) before every timed step; AO matrix >> L2"}
 
 
 def run_reference(args):
-    import torch.distributed as dist  # noqa: F401  (only for rank detection)
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
     from qmckl_b200 import gen
@@ -138,8 +180,9 @@ def run_reference(args):
     P = sysd["elec_coord"].shape[0] * sysd["elec_coord"].shape[1]
     vals = []
     base = None
+    per_step = max(2.0, 20.0 / max(1, args.warmup + args.steps))
     for i in range(args.warmup + args.steps):
-        base = cpu_baseline(sysd, seconds=max(2.0, 20.0 / max(1, args.steps)))
+        base = cpu_baseline(sysd, seconds=per_step, single_thread_seconds=0.5 if i < args.warmup + args.steps - 1 else 3.0)
         if i >= args.warmup:
             vals.append(base["value"])
     v = statistics.median(vals)
@@ -148,27 +191,39 @@ def run_reference(args):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 * P / v, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, qmckl_b200/gen.py)",
-            "config": {"workload": WORKLOAD, "points": P, "form": "reference CPU path"},
+            "config": workload_config(P, sysd["ao_num"], sysd["mo_num"], world),
+            "form": "reference CPU path (" + base["kind"] + ")",
             "cpu_baseline": base,
             "e2e": {"value": v, "unit": "electron-points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
 def profile_case(kind, walkers=64):
-    """One evaluation of the config-1 molecule on `walkers` walkers, for ncu captures."""
+    """One evaluation of the config-1 molecule on `walkers` walkers, for ncu
+    captures; "adjoint": the config-3 workload (config-1 molecule, 128
+    walkers), mixed-form forward and MO VGL adjoint, called twice."""
     import torch
     from qmckl_b200 import gen
     from qmckl_b200 import qmckl as pq
     from qmckl_b200.system import make_context
-    d = gen.config(1, walk_num=walkers)
+    d = gen.config(3) if kind == "adjoint" else gen.config(1, walk_num=walkers)
     P = d["elec_coord"].shape[0] * d["elec_coord"].shape[1]
-    M = d["mo_num"]
+    A, M, N = d["ao_num"], d["mo_num"], d["nucl_num"]
     dc = torch.tensor(np.ascontiguousarray(gen.points(d).T), dtype=torch.float64, device="cuda")
     out = torch.empty(P * 5 * M, dtype=torch.float64, device="cuda")
     ctx = make_context(d, points=False, form=pq.FORM_FP64 if kind == "fp64" else pq.FORM_MIXED)
-    if kind != "fp64":
+    if kind in ("fused", "split"):
         pq.b200_set_mixed_kernel(ctx, kind == "fused")
     pq.b200_mo_vgl_device(ctx, P, dc.data_ptr(), out.data_ptr())
+    if kind == "adjoint":
+        w = torch.randn((P, 5, M), dtype=torch.float64, device="cuda",
+                        generator=torch.Generator("cuda").manual_seed(3))
+        gc = torch.empty((M, A), dtype=torch.float64, device="cuda")
+        gn = torch.empty((N, 3), dtype=torch.float64, device="cuda")
+        gr = torch.empty((3, P), dtype=torch.float64, device="cuda")
+        for _ in range(2):
+            pq.b200_mo_vgl_adjoint_device(ctx, P, dc.data_ptr(), w.data_ptr(), gc.data_ptr(), gn.data_ptr(),
+                                          gr.data_ptr())
     pq.b200_synchronize(ctx)
     pq.context_destroy(ctx)
     print(f"profile case {kind}: {P} points")
@@ -237,17 +292,17 @@ def case_batched(args):
         loop()
     t_l, _ = _events_time(stream, loop, n, flush)
     flops = sum(10.0 * p * s["ao_num"] * s["mo_num"] for p, s in zip(P, systems))
-    line = {"case": "batched systems: 256 molecules, 5-80 nuclei, cc-pVDZ/TZ shapes, 16-256 walkers",
+    line = {"case": "config 2: 256 molecules, 5-80 nuclei, cc-pVDZ/TZ shapes, 16-256 walkers",
             "systems": len(systems), "points": int(sum(P)), "form": "mixed",
             "persistent_ms": t_p, "loop_ms": t_l, "loop_over_persistent": t_l / t_p,
             "points_per_s": sum(P) / (t_p * 1e-3), "dense_equivalent_tflops": flops / (t_p * 1e-3) / 1e12,
             "tuning": {"producer_warps": tuning[0], "queue_order": tuning[1], "tuned_ms": best},
             "graph": True, "setup_s": setup_s, "steps": n,
             "timing": "CUDA events on the batch stream, median, 256 MB L2 flush before each step"}
-    print(json.dumps(line))
     pq.b200_batch_destroy(b)
     for c in ctxs:
         pq.context_destroy(c)
+    return line
 
 
 def case_adjoint(args):
@@ -283,9 +338,9 @@ def case_adjoint(args):
         tb, _ = _events_time(stream, bwd, max(3, min(args.steps, 20)), flush)
         res[name] = {"forward_ms": tf, "backward_ms": tb, "points_per_s_fwd_bwd": P / ((tf + tb) * 1e-3)}
         pq.context_destroy(ctx)
-    print(json.dumps({"case": "adjoint: config-1 molecule, 128 walkers, L = sum W * mo_vgl", "points": P,
-                      "ao_num": A, "mo_num": M, "results": res,
-                      "timing": "CUDA events, median, 256 MB L2 flush before each call"}))
+    return {"case": "config 3, adjoint: config-1 molecule, 128 walkers, L = sum W * mo_vgl", "points": P,
+            "ao_num": A, "mo_num": M, "results": res, "steps": max(3, min(args.steps, 20)),
+            "timing": "CUDA events, median, 256 MB L2 flush before each call"}
 
 
 def case_large(args):
@@ -322,9 +377,9 @@ def case_large(args):
                 for c, n in enumerate(["value", "grad_x", "grad_y", "grad_z", "laplacian"])}
         pq.context_destroy(ctx)
     res["speedup"] = res["fp64_unfused"]["ms"] / res["mixed_fused"]["ms"]
-    print(json.dumps({"case": "large: 200 nuclei, 5000 AOs, 350 MOs, 700 electrons x 256 walkers", "points": P,
-                      "ao_num": A, "mo_num": M, "results": res,
-                      "timing": "CUDA events, median, 256 MB L2 flush before each call"}))
+    return {"case": "config 4, large: 200 nuclei, 5000 AOs, 350 MOs, 700 electrons x 256 walkers", "points": P,
+            "ao_num": A, "mo_num": M, "results": res, "steps": max(3, min(args.steps, 10)),
+            "timing": "CUDA events, median, 256 MB L2 flush before each call"}
 
 
 def main():
@@ -335,23 +390,27 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default=os.environ.get("QMCKL_B200_BENCH_FORM", "mixed"), choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the configs 2, 3 and 4 measured after the headline workload")
     ap.add_argument("--unfused", action="store_true",
                     help="mixed form with the AO pieces written to HBM and a separate tensor-core GEMM")
     ap.add_argument("--pieces", type=int, default=3, choices=[2, 3],
                     help="operand split of the mixed form: 3 bfloat16 pieces (default) or 2 float16 pieces")
-    ap.add_argument("--profile", choices=["fused", "split", "fp64"],
+    ap.add_argument("--profile", choices=["fused", "split", "fp64", "adjoint"],
                     help="run one evaluation of a small case (config-1 molecule, 64 walkers) for ncu; no timing")
+    ap.add_argument("--walkers", type=int, default=64, help="walkers of the --profile case (config-1 molecule)")
     ap.add_argument("--case", choices=["batched", "adjoint", "large"],
                     help="measure another workload instead of the headline one (one JSON line)")
     args = ap.parse_args()
     if args.case:
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        return {"batched": case_batched, "adjoint": case_adjoint, "large": case_large}[args.case](args)
+        print(json.dumps({"batched": case_batched, "adjoint": case_adjoint, "large": case_large}[args.case](args)))
+        return
     if args.impl == "reference":
         return run_reference(args)
     if args.profile:
-        return profile_case(args.profile)
+        return profile_case(args.profile, args.walkers)
 
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -385,33 +444,14 @@ def main():
     coord_t = np.ascontiguousarray(gen.points(sysd).T)               # [3][P]
     d_coord = torch.tensor(coord_t, dtype=torch.float64, device="cuda")
     d_mo = torch.empty(P * 5 * M, dtype=torch.float64, device="cuda")
-    d_ao = torch.empty(P * 5 * A, dtype=torch.float64, device="cuda") if form == pq.FORM_FP64 else None
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def step():
         pq.b200_mo_vgl_device(ctx, P, d_coord.data_ptr(), d_mo.data_ptr())
 
-    # accuracy of the timed form against the FP64 form on the same points
-    err = None
-    if form == pq.FORM_MIXED:
-        step()
-        torch.cuda.synchronize()
-        mixed = d_mo.clone()
-        ctx64 = make_context(sysd, points=False, form=pq.FORM_FP64)
-        pq.b200_set_stream(ctx64, stream.cuda_stream)
-        pq.b200_mo_vgl_device(ctx64, P, d_coord.data_ptr(), d_mo.data_ptr())
-        torch.cuda.synchronize()
-        ref = d_mo.view(P, 5, M)
-        diff = (mixed.view(P, 5, M) - ref).abs()
-        err = {"max_abs_over_max_ref": {n: float(diff[:, c, :].max() / ref[:, c, :].abs().max())
-                                         for c, n in enumerate(["value", "grad_x", "grad_y", "grad_z", "laplacian"])},
-               "reference": "FP64 form on the GPU (itself checked against the CPU oracle in tests/)"}
-        pq.context_destroy(ctx64)
-        del mixed, ref, diff
-
     for _ in range(args.warmup):
         step()
-    torch.cuda.synchronize()
+    pq.b200_synchronize(ctx)
     if dist:
         dist.barrier()
     sampler = ClockSampler(local)
@@ -430,23 +470,55 @@ def main():
         e1.record(stream)
         e1.synchronize()
         times.append(e0.elapsed_time(e1))
-    torch.cuda.synchronize()
+    pq.b200_synchronize(ctx)   # also reports a bounded wait that gave up
     launches = pq.b200_kernel_launch_count() - launches0
     kb_eval, kb_total = pq.b200_get_kblock_stats(ctx) if fused_path else (0, 0)
-    # dominant-kernel timing: the AO kernel alone (same stream, same events)
-    ao_times = []
-    if form == pq.FORM_FP64:
-        for _ in range(max(3, args.steps // 2)):
-            flush.zero_()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            pq.b200_ao_vgl_device(ctx, P, d_coord.data_ptr(), d_ao.data_ptr())
-            e1.record(stream)
-            e1.synchronize()
-            ao_times.append(e0.elapsed_time(e1))
     clocks = sampler.stop()
     ms = replicas.max_over_ranks(statistics.mean(times), device="cuda")
+
+    # the FP64 form on the same GPU: the whole step and the FP64 AO kernel alone
+    ctx64 = make_context(sysd, points=False, form=pq.FORM_FP64)
+    pq.b200_set_stream(ctx64, stream.cuda_stream)
+    d_ref = torch.empty(P * 5 * M, dtype=torch.float64, device="cuda")
+    fp64_step = lambda: pq.b200_mo_vgl_device(ctx64, P, d_coord.data_ptr(), d_ref.data_ptr())
+    for _ in range(3):
+        fp64_step()
+    pq.b200_synchronize(ctx64)
+    n64 = max(3, min(args.steps, 10))
+    fp64_ms, _ = _events_time(stream, fp64_step, n64, flush)
+    d_ao = torch.empty(P * 5 * A, dtype=torch.float64, device="cuda")
+    ao_step = lambda: pq.b200_ao_vgl_device(ctx64, P, d_coord.data_ptr(), d_ao.data_ptr())
+    ao_step()
+    ao_ms, _ = _events_time(stream, ao_step, n64, flush)
+    del d_ao
+    pq.b200_synchronize(ctx64)
+    fp64_ms = replicas.max_over_ranks(fp64_ms, device="cuda")
+    ao_ms = replicas.max_over_ranks(ao_ms, device="cuda")
+    hbm, bf16, bf16_sus, peak_src = load_peaks()
+    ao_bytes = 5.0 * P * A * 8 + 24.0 * P      # dense FP64 ao_vgl write + coordinates
+    fp64_form = {"ms_per_step": fp64_ms, "points_per_s": world * P / (fp64_ms * 1e-3),
+                 "ao_kernel": {"kernel": "ao_f64_kernel<5> (AO VGL, FP64)", "ms_per_launch": ao_ms,
+                               "algorithmic_bytes_per_launch": ao_bytes,
+                               "achieved_gbs": ao_bytes / (ao_ms * 1e-3) / 1e9,
+                               "hbm_frac": ao_bytes / (ao_ms * 1e-3) / 1e9 / hbm},
+                 "mo_gemm_ms": fp64_ms - ao_ms,
+                 "timing": f"CUDA events, median of {n64}, L2 flushed before each step"}
+
+    # accuracy of the timed form: against the FP64 form on every point, and
+    # against the CPU oracle on a fixed sample of the points
+    err = None
+    if form == pq.FORM_MIXED:
+        step()
+        fp64_step()
+        pq.b200_synchronize(ctx)
+        pq.b200_synchronize(ctx64)
+        err = {"vs_fp64_gpu_all_points": device_error_report(d_mo.view(P, 5, M), d_ref.view(P, 5, M)),
+               "vs_oracle_sample": None}
+        if rank == 0:
+            sample = np.arange(0, P, 39)
+            err["vs_oracle_sample"] = oracle_error_report(sysd, sample, d_mo.view(P, 5, M), d_ref.view(P, 5, M))
+    pq.context_destroy(ctx64)
+    del d_ref
 
     # end to end through the public host API (pinned host buffers)
     h_coord = torch.from_numpy(np.ascontiguousarray(sysd["elec_coord"].reshape(-1))).pin_memory()
@@ -479,50 +551,16 @@ def main():
     pq.context_destroy(ctx_e)
     e2e_ms = replicas.max_over_ranks(statistics.mean(e2e_times), device="cuda")
 
-    hbm, bf16, bf16_sus, peak_src = load_peaks()
-    traffic = load_traffic()
     if form == pq.FORM_FP64:
-        ao_ms = statistics.mean(ao_times)
-        algo_bytes = 5.0 * P * A * 8 + 24.0 * P      # dense ao_vgl write + coordinates
-        achieved = algo_bytes / (ao_ms * 1e-3) / 1e9
-        roofline = {"kernel": "ao_f64_kernel<5> (AO VGL, FP64)", "bound": "hbm", "achieved": achieved,
-                    "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_source": peak_src,
-                    "traffic": traffic.get(("ao_f64_kernel", "fp64")), "ms_per_launch": ao_ms,
-                    "algorithmic_bytes_per_launch": algo_bytes,
+        roofline = {"kernel": "ao_f64_kernel<5> (AO VGL, FP64)", "bound": "hbm",
+                    "achieved": fp64_form["ao_kernel"]["achieved_gbs"], "peak": hbm, "unit": "GB/s",
+                    "frac": fp64_form["ao_kernel"]["hbm_frac"], "peak_source": peak_src,
+                    "traffic": None, "ms_per_launch": ao_ms, "algorithmic_bytes_per_launch": ao_bytes,
                     "other_kernel": {"kernel": "dgemm_kernel (MO VGL, FP64 mma.sync m8n8k4)",
                                      "ms_per_launch": ms - ao_ms,
                                      "tflops": 2.0 * 5 * P * A * M / ((ms - ao_ms) * 1e-3) / 1e12}}
     else:
-        # fused kernel: 25 points x 5 components per 128-row MMA tile, MOs in
-        # N tiles of n_tile columns, 64-AO K blocks (those that vanish over a
-        # tile are skipped: the kernel counts the blocks it evaluates);
-        # 6 split-BF16 products (3 for float16 x 2) per K step
-        flops = 2.0 * 5 * P * A * M
-        n_tiles = -(-M // 256)
-        n_tile = -(-(-(-M // n_tiles)) // 16) * 16
-        while n_tile > 160:
-            n_tiles += 1
-            n_tile = -(-(-(-M // n_tiles)) // 16) * 16
-        nprod = 6 if args.pieces == 3 else 3
-        executed = 2.0 * (kb_eval / args.steps) * 128 * n_tile * 64 * nprod
-        t = traffic.get(("fused_mo_kernel", "mixed"))
-        kname = ("fused_mo_kernel<3,5> (AO -> split-BF16 tcgen05 MO VGL" if args.pieces == 3 else
-                 "fused_mo_kernel<2,5> (AO -> split-FP16 tcgen05 MO VGL") + "; step = 3 ordering kernels + tile plan + this)"
-        if args.unfused:
-            # AO pieces to HBM, then 128-row tiles of the 5P x A pieces matrix x 6 products
-            executed = 2.0 * (-(-5 * P // 128) * 128) * (n_tile * n_tiles) * (-(-A // 64) * 64) * 6
-            kname = "ao_tile_kernel<3,5> + tc_gemm_kernel<3,2> (unfused mixed form; whole step)"
-            t = None
-        achieved = executed / (ms * 1e-3) / 1e12
-        roofline = {"kernel": kname,
-                    "bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
-                    "frac": achieved / bf16, "peak_source": peak_src,
-                    "traffic": t * P / 20352.0 if t else None,
-                    "traffic_note": "ncu dram bytes of a 20,352-point launch scaled by points" if t else None,
-                    "executed_tensor_flop_per_launch": executed,
-                    "dense_equivalent_tflops": flops / (ms * 1e-3) / 1e12,
-                    "k_blocks_evaluated_fraction": (kb_eval / kb_total) if kb_total else None,
-                    "output_bytes_per_launch": 40.0 * P * M}
+        roofline = mixed_roofline(args, P, A, M, ms, kb_eval, kb_total, bf16, peak_src)
 
     value = world * P / (ms * 1e-3)
     line = {
@@ -530,26 +568,144 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if form == pq.FORM_FP64 else ("f32/bf16x3" if args.pieces == 3 else "f32/f16x2"),
         "data": "synthetic (seeded generator qmckl_b200/gen.py, no dataset)",
-        "config": {"workload": WORKLOAD, "points": P, "ao_num": A, "mo_num": M,
-                   "form": args.form, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "l2": "flushed (256 MB write) before every timed step; AO matrix >> L2"},
+        "config": workload_config(P, A, M, world),
+        "form": args.form + (" (unfused)" if args.unfused else ""),
         "e2e": {"value": world * P / (e2e_ms * 1e-3), "unit": "electron-points/s",
                 "h2d_bytes_per_step": int(P * 3 * 8), "d2h_bytes_per_step": int(P * 5 * M * 8),
                 "ms_per_step": e2e_ms},
         "gpu_launches": int(launches),
         "clocks": clocks,
         "roofline": roofline,
+        "fp64_form": fp64_form,
+        "mixed_over_fp64": fp64_ms / ms if form == pq.FORM_MIXED else None,
     }
     if err is not None:
-        line["error_vs_fp64"] = err
+        line["error"] = err
+    pq.context_destroy(ctx)
+    del d_mo
+    torch.cuda.empty_cache()
+    if rank == 0 and not args.no_extras and world == 1:
+        line["other_workloads"] = other_workloads(args)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(sysd)
-    pq.context_destroy(ctx)
     if rank == 0:
         print(json.dumps(line))
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def mixed_roofline(args, P, A, M, ms, kb_eval, kb_total, bf16, peak_src):
+    """Roofline of the mixed step's dominant kernel against the bf16 tensor peak.
+
+    The fused kernel evaluates 25 points x 5 components per 128-row MMA tile,
+    MOs in N tiles of n_tile columns, 64-AO K blocks (the blocks that vanish
+    over a tile are skipped: the kernel counts the blocks it evaluates);
+    6 split-BF16 products (3 for float16 x 2) per K step.  Reported two ways:
+    the issued MMA flops and the algorithmic split count (3 x 10 P A M)."""
+    flops = 2.0 * 5 * P * A * M
+    n_tiles = -(-M // 256)
+    n_tile = -(-(-(-M // n_tiles)) // 16) * 16
+    while n_tile > 160:
+        n_tiles += 1
+        n_tile = -(-(-(-M // n_tiles)) // 16) * 16
+    nprod = 6 if args.pieces == 3 else 3
+    issued = 2.0 * (kb_eval / args.steps) * 128 * n_tile * 64 * nprod
+    kname = ("fused_mo_kernel<3,5> (AO -> split-BF16 tcgen05 MO VGL" if args.pieces == 3 else
+             "fused_mo_kernel<2,5> (AO -> split-FP16 tcgen05 MO VGL") + "; step = 3 ordering kernels + tile plan + this)"
+    if args.unfused:
+        # AO pieces to HBM, then 128-row tiles of the 5P x A pieces matrix x 6 products
+        issued = 2.0 * (-(-5 * P // 128) * 128) * (n_tile * n_tiles) * (-(-A // 64) * 64) * 6
+        kname = "ao_tile_kernel<3,5> + tc_gemm_kernel<3,2> (unfused mixed form; whole step)"
+    split3 = 3.0 * flops
+    achieved = issued / (ms * 1e-3) / 1e12
+    return {"kernel": kname, "bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
+            "frac": achieved / bf16, "peak_source": peak_src,
+            "achieved_basis": "issued split-BF16 MMA flops per step / step time",
+            "split3_count": {"flop_per_step": split3, "tflops": split3 / (ms * 1e-3) / 1e12,
+                             "frac": split3 / (ms * 1e-3) / 1e12 / bf16,
+                             "note": "3 x 10 P A M: the 3-term split of the dense contraction"},
+            "traffic": None,
+            "traffic_note": "DRAM bytes per launch: profiles/ (ncu capture); the algorithmic bytes are the mo_vgl output",
+            "executed_tensor_flop_per_launch": issued,
+            "dense_equivalent_tflops": flops / (ms * 1e-3) / 1e12,
+            "k_blocks_evaluated_fraction": (kb_eval / kb_total) if kb_total else None,
+            "output_bytes_per_launch": 40.0 * P * M}
+
+
+def _torch_error_measures(got, ref):
+    """The three error measures per component, on the device (torch tensors [P][5][M])."""
+    import torch
+    out = {"max_abs_over_max_ref": {}, "row_floored_rel": {}, "elementwise_rel": {}, "avg_bits": {}}
+    for c, name in enumerate(COMPONENTS):
+        g, r = got[:, c, :], ref[:, c, :]
+        d = (g - r).abs()
+        ar = r.abs()
+        s = ar.max()
+        out["max_abs_over_max_ref"][name] = float(d.max() / s)
+        den = torch.maximum(ar, 1e-2 * ar.amax(dim=1, keepdim=True))
+        den = torch.where(den == 0, torch.ones_like(den), den)
+        out["row_floored_rel"][name] = float((d / den).max())
+        m = ar > 1e-8 * s
+        out["elementwise_rel"][name] = float((d[m] / ar[m]).max()) if bool(m.any()) else 0.0
+        out["avg_bits"][name] = float(_torch_bits(g, r).double().mean())
+    return out
+
+
+def _torch_bits(a, b):
+    """Bits of agreement of two FP64 tensors: the reference's
+    qmckl_test_precision_64 (org/qmckl_numprec.org:384-430), on the device."""
+    import torch
+    x = a.contiguous().view(torch.int64)
+    y = b.contiguous().view(torch.int64)
+    same = (x < 0) == (y < 0)
+    d = torch.where(same, (x - y).abs(), torch.zeros_like(x))
+    e = torch.frexp(d.double())[1]
+    bits = 53 - torch.clamp(e, max=53)
+    zero = (a == 0) | (b == 0)
+    return torch.where(same | zero, bits, torch.zeros_like(bits))
+
+
+COMPONENTS = ("value", "grad_x", "grad_y", "grad_z", "laplacian")
+
+
+def device_error_report(got, ref):
+    rep = _torch_error_measures(got, ref)
+    rep["points"] = int(got.shape[0])
+    rep["reference"] = "FP64 form on the GPU"
+    return rep
+
+
+def oracle_error_report(sysd, sample, d_mixed, d_fp64):
+    """Mixed and FP64 GPU results on the sampled points against the CPU oracle."""
+    import torch
+    from oracle import pyoracle as O
+    pts = sysd["elec_coord"].reshape(-1, 3)[sample]
+    ref = O.mo_vgl(sysd["mo_coef"], O.ao_vgl(O.Basis(sysd), pts, sysd["nucl_coord"]))
+    idx = torch.tensor(sample, device=d_mixed.device)
+    ref_t = torch.from_numpy(ref).to(d_mixed.device)
+    rep = _torch_error_measures(d_mixed.index_select(0, idx), ref_t)
+    f64 = d_fp64.index_select(0, idx)
+    d = (f64 - ref_t).abs()
+    den = torch.maximum(ref_t.abs(), 1e-2 * ref_t.abs().amax(dim=2, keepdim=True))
+    den = torch.where(den == 0, torch.ones_like(den), den)
+    rep["fp64_form_parity"] = float((d / den).max())
+    rep["points"] = int(len(sample))
+    rep["reference"] = "CPU oracle (restatement of the reference's HPC path), every 39th point"
+    return rep
+
+
+def other_workloads(args):
+    """Configs 2, 3 and 4 at a few steps each (one line per workload)."""
+    out = {}
+    for name, fn in (("config4_large", case_large), ("config3_adjoint", case_adjoint), ("config2_batched", case_batched)):
+        t0 = time.time()
+        try:
+            out[name] = fn(argparse.Namespace(steps=min(args.steps, 5), warmup=3))
+        except Exception as e:   # reported, not fatal: the headline line still prints
+            out[name] = {"error": repr(e)}
+        out[name]["wall_s"] = time.time() - t0
+    return out
 
 
 if __name__ == "__main__":

@@ -49,7 +49,11 @@ qmckl_exit_code qmckl_b200_set_mixed_kernel(qmckl_context context, const int32_t
 /* The CUDA device and stream (cudaStream_t passed as void*) the context uses.
  * Default: the current device at the first evaluation, and a non-blocking
  * stream owned by the context.  A stream handle of 0 selects the legacy
- * default stream.  Set the device before the first evaluation. */
+ * default stream.  Set the device before the first evaluation.
+ * qmckl_b200_synchronize waits for the context's stream and returns
+ * QMCKL_FAILURE when a bounded barrier wait of a mixed-form tensor-core
+ * kernel gave up since the last synchronization point (the host getters
+ * check the same at their end). */
 qmckl_exit_code qmckl_b200_set_device(qmckl_context context, const int32_t device);
 qmckl_exit_code qmckl_b200_set_stream(qmckl_context context, void* stream);
 qmckl_exit_code qmckl_b200_synchronize(qmckl_context context);
@@ -59,7 +63,9 @@ qmckl_exit_code qmckl_b200_synchronize(qmckl_context context);
  * device memory in the reference layouts ao_vgl[point][5][ao],
  * ao_value[point][ao], mo_vgl[point][5][mo], mo_value[point][mo].  The basis
  * and MO coefficients come from the context.  Work is enqueued on the
- * context's stream; the call returns without synchronizing. */
+ * context's stream; the call returns without synchronizing (the first call
+ * of a context, or one after the basis, coefficients or precision changed,
+ * first uploads its tables, which waits for the copies). */
 qmckl_exit_code qmckl_b200_ao_vgl_device(qmckl_context context, const int64_t point_num,
                                          const double* d_coord, double* d_ao_vgl);
 qmckl_exit_code qmckl_b200_ao_value_device(qmckl_context context, const int64_t point_num,
@@ -142,29 +148,30 @@ qmckl_exit_code qmckl_b200_batch_set_wait_limit(qmckl_b200_batch batch, const in
  *
  * For callers that cannot allocate device memory when they evaluate the
  * orbitals: codes whose device memory is held by a pool allocator that has
- * already reserved the free memory (cudaMalloc would fail), work issued from
- * a CUDA host callback (where allocating CUDA calls are not permitted), or
- * time-step loops that cannot take the device synchronization of
- * cudaMalloc/cudaFree.  Same arguments, result and arithmetic as
- * qmckl_b200_mo_vgl_device in the mixed form (it always evaluates the mixed
- * form, whatever qmckl_b200_set_form says), but the scratch it needs lives in
- * one fixed 32 MiB array inside the library, held by every GPU that loads the
- * library until the process exits.  The caller passes the coordinates and the
- * output buffer (device memory).
+ * already reserved the free memory (cudaMalloc would fail, and memory freed
+ * with cudaFree would escape the pool).  Same arguments, result and
+ * arithmetic as qmckl_b200_mo_vgl_device in the mixed form with the unfused
+ * kernels (it always evaluates the mixed form, whatever qmckl_b200_set_form
+ * says), but the scratch it needs lives in one fixed 32 MiB array inside the
+ * library, held by every GPU that loads the library until the process exits.
+ * The caller passes the coordinates and the output buffer (device memory).
  *   - Limit: point_num * 5 rows of the AO matrix in 3 bfloat16 pieces
  *     of ao_num rounded up to 64 columns must fit in the 32 MiB; larger
  *     point_num is rejected with QMCKL_INVALID_ARG_2 and a message giving the
- *     largest point count for the basis (546 points for 2000 AOs, 3 pieces).
- *   - The basis tables and the split MO coefficients must already be on the
- *     device: run one regular mixed-form evaluation of the context first (that
- *     one allocates); otherwise QMCKL_NOT_PROVIDED.
- *   - The first call on a device looks up the array's device address (once
- *     per device); make that first call before any stream capture.
+ *     largest point count for the basis (546 points for 2000 AOs).
+ *   - The basis tables, the split MO coefficients and the context's error
+ *     word must already be on the device: run one regular mixed-form
+ *     evaluation of the context first (that one allocates, and it also loads
+ *     the kernels and the fixed array this call uses); otherwise
+ *     QMCKL_NOT_PROVIDED.
  *   - Every call uses the same array and it keeps the previous call's
- *     contents; the timeout word is cleared at the start of each call.  Calls
+ *     contents (every byte a call reads was written by that call).  Calls
  *     whose GPU work overlaps (other streams, other host threads, other
  *     contexts) race on the array: order them on one stream.
- *   - The call synchronizes the context's stream before returning. */
+ *   - The work is enqueued on the context's stream and the call returns
+ *     without synchronizing; a bounded wait of its kernels that gives up is
+ *     reported by the context's next synchronization point
+ *     (qmckl_b200_synchronize or a host getter) as QMCKL_FAILURE. */
 qmckl_exit_code qmckl_b200_mo_vgl_device_noalloc(qmckl_context context, const int64_t point_num,
                                                  const double* d_coord, double* d_mo_vgl);
 
@@ -175,6 +182,12 @@ qmckl_exit_code qmckl_b200_mo_vgl_device_noalloc(qmckl_context context, const in
  * Both 0 before any fused evaluation.  Synchronizes the context's stream. */
 qmckl_exit_code qmckl_b200_get_kblock_stats(qmckl_context context, int64_t* evaluated, int64_t* total,
                                            const int32_t reset);
+
+/* Test hook: write `code` into the context's error word of the mixed-form
+ * tensor-core kernels, as a bounded barrier wait that gave up would, so that
+ * the next synchronization point reports QMCKL_FAILURE.  Needs one mixed-form
+ * evaluation of the context first (QMCKL_NOT_PROVIDED otherwise). */
+qmckl_exit_code qmckl_b200_inject_wait_failure(qmckl_context context, const int32_t code);
 
 /* Number of kernels this library launched since the process started. */
 int64_t qmckl_b200_kernel_launch_count(void);

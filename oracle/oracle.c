@@ -35,6 +35,12 @@ struct oracle_basis {
 
 static int64_t lstart(int l) { return (int64_t)l * (l + 1) * (l + 2) / 6; }
 
+/* Monomial tables hold every cartesian power of degree <= ORACLE_MAX_L
+ * (120 monomials at l = 7); power tables pw[.][i + 2] = Y^i for
+ * i = -2 .. ORACLE_MAX_L + 1 (the Hessian reads one power past lmax). */
+#define ORACLE_NPOLY 120
+#define ORACLE_NPW (ORACLE_MAX_L + 4)
+
 double oracle_cutoff(int32_t precision) {
   /* org/qmckl_ao.org:7814: cutoff = log(2^(precision-1)) */
   return log((double)(((uint64_t)1) << (precision - 1)));
@@ -53,6 +59,8 @@ static int cmp_expo(const void* l, const void* r) {
 /* qmckl_finalize_basis (org/qmckl_ao.org:2965-3226) and
  * qmckl_finalize_basis_hpc (org/qmckl_ao.org:3280-3410). */
 oracle_basis* oracle_basis_create(const oracle_basis_in* in) {
+  for (int64_t s = 0; s < in->shell_num; ++s)
+    if (in->shell_ang_mom[s] < 0 || in->shell_ang_mom[s] > ORACLE_MAX_L) return NULL;
   oracle_basis* b = (oracle_basis*)calloc(1, sizeof(oracle_basis));
   const int64_t N = in->nucl_num, S = in->shell_num, Pn = in->prim_num, A = in->ao_num;
   b->nucl_num = N; b->shell_num = S; b->prim_num = Pn; b->ao_num = A;
@@ -163,10 +171,10 @@ int64_t oracle_prim_per_nucleus(const oracle_basis* b, int64_t n) { return b->np
 /* Cartesian monomials of degree <= lmax with value/gradient/Laplacian, HPC
  * ordering and arithmetic (org/qmckl_ao.org:6624-6914 generic branch;
  * 8700-8760 for the l=1 and l=2 tables).  vgl[c][m], c = 0..4. */
-static void poly_vgl_hpc(int lmax, double x, double y, double z, double vgl[5][20]) {
+static void poly_vgl_hpc(int lmax, double x, double y, double z, double vgl[5][ORACLE_NPOLY]) {
   const double shift = 1.e-20;
   for (int c = 0; c < 5; ++c)
-    for (int m = 0; m < 20; ++m) vgl[c][m] = 0.0;
+    for (int m = 0; m < ORACLE_NPOLY; ++m) vgl[c][m] = 0.0;
   vgl[0][0] = 1.0;
   if (lmax == 0) return;
   vgl[0][1] = x + shift; vgl[0][2] = y + shift; vgl[0][3] = z + shift;
@@ -181,7 +189,7 @@ static void poly_vgl_hpc(int lmax, double x, double y, double z, double vgl[5][2
     vgl[4][4] = 2.0; vgl[4][7] = 2.0; vgl[4][9] = 2.0;
     return;
   }
-  double pw[3][8];  /* pw[.][i+2] = coordinate^i, pw[.][0..2] = 1 */
+  double pw[3][ORACLE_NPW];  /* pw[.][i+2] = coordinate^i, pw[.][0..2] = 1 */
   const double Y[3] = {x, y, z};
   for (int d = 0; d < 3; ++d) {
     pw[d][0] = pw[d][1] = pw[d][2] = 1.0;
@@ -229,7 +237,7 @@ int oracle_ao_vgl_hpc(const oracle_basis* b, int32_t precision, int64_t point_nu
     double* ar2 = (double*)malloc(sizeof(double) * PM);
     double (*em)[5] = (double (*)[5])malloc(sizeof(double) * 5 * PM);
     double (*ce)[5] = (double (*)[5])malloc(sizeof(double) * 5 * SM);
-    double poly[5][20];
+    double poly[5][ORACLE_NPOLY];
 #ifdef _OPENMP
 #pragma omp for schedule(dynamic, 16)
 #endif
@@ -319,7 +327,7 @@ int oracle_ao_value_hpc(const oracle_basis* b, int32_t precision, int64_t point_
     double* ar2 = (double*)malloc(sizeof(double) * PM);
     double* em = (double*)malloc(sizeof(double) * PM);
     double* ce = (double*)malloc(sizeof(double) * SM);
-    double poly[5][20];
+    double poly[5][ORACLE_NPOLY];
 #ifdef _OPENMP
 #pragma omp for schedule(dynamic, 16)
 #endif
@@ -433,11 +441,11 @@ int oracle_shell_vgl_doc(const oracle_basis* b, int32_t precision, int64_t point
 
 /* qmckl_ao_polynomial_vgl_doc (org/qmckl_ao.org:6233-6364): the 1e-20 shift is
  * added to the displacement before the powers are formed. vgl[c][m]. */
-static void poly_vgl_doc(int lmax, const double X[3], const double R[3], double vgl[5][20]) {
-  double Y[3], pw[3][8];  /* pw[.][i+2] = Y^i, i >= -2 */
+static void poly_vgl_doc(int lmax, const double X[3], const double R[3], double vgl[5][ORACLE_NPOLY]) {
+  double Y[3], pw[3][ORACLE_NPW];  /* pw[.][i+2] = Y^i, i >= -2 */
   for (int i = 0; i < 3; ++i) Y[i] = (X[i] - R[i]) + 1.e-20;
   for (int c = 0; c < 5; ++c)
-    for (int m = 0; m < 20; ++m) vgl[c][m] = 0.0;
+    for (int m = 0; m < ORACLE_NPOLY; ++m) vgl[c][m] = 0.0;
   vgl[0][0] = 1.0;
   if (lmax == 0) return;
   for (int d = 0; d < 3; ++d) {
@@ -474,6 +482,16 @@ static void poly_vgl_doc(int lmax, const double X[3], const double R[3], double 
   }
 }
 
+int oracle_poly_vgl(int32_t which, int32_t lmax, const double* X, const double* R, double* vgl) {
+  if (lmax < 0 || lmax > ORACLE_MAX_L) return -1;
+  double (*v)[ORACLE_NPOLY] = (double (*)[ORACLE_NPOLY])vgl;
+  if (which == 1)
+    poly_vgl_hpc(lmax, X[0] - R[0], X[1] - R[1], X[2] - R[2], v);
+  else
+    poly_vgl_doc(lmax, X, R, v);
+  return (int)lstart(lmax + 1);
+}
+
 /* qmckl_compute_ao_vgl_doc (org/qmckl_ao.org:8438-8570) on top of the doc shell
  * VGL and doc polynomials. */
 int oracle_ao_vgl_doc(const oracle_basis* b, int32_t precision, int64_t point_num,
@@ -482,7 +500,7 @@ int oracle_ao_vgl_doc(const oracle_basis* b, int32_t precision, int64_t point_nu
   const int64_t N = b->nucl_num, S = b->shell_num, A = b->ao_num;
   double* sv = (double*)malloc(sizeof(double) * 5 * S * point_num);
   oracle_shell_vgl_doc(b, precision, point_num, coord, nucl_coord, sv);
-  double poly[5][20];
+  double poly[5][ORACLE_NPOLY];
   for (int64_t ip = 0; ip < point_num; ++ip) {
     double* out = ao_vgl + ip * 5 * A;
     memset(out, 0, sizeof(double) * 5 * A);
@@ -660,10 +678,10 @@ int oracle_shell_hessian_doc(const oracle_basis* b, int32_t precision, int64_t p
 
 /* hess[n][m][k] = d_k d_m P_n (m < 3), hess[n][3][k] = d_k lap P_n, with the
  * 1e-20 shift on the displacement (org/qmckl_ao.org:7113-7236). */
-static void poly_hessian_doc(int lmax, const double X[3], const double R[3], double hess[20][4][3]) {
-  double Y[3], pw[3][8];  /* pw[.][i+2] = Y^i for i >= -2 */
+static void poly_hessian_doc(int lmax, const double X[3], const double R[3], double hess[ORACLE_NPOLY][4][3]) {
+  double Y[3], pw[3][ORACLE_NPW];  /* pw[.][i+2] = Y^i for i >= -2 */
   for (int i = 0; i < 3; ++i) Y[i] = (X[i] - R[i]) + 1.e-20;
-  memset(hess, 0, sizeof(double) * 20 * 4 * 3);
+  memset(hess, 0, sizeof(double) * ORACLE_NPOLY * 4 * 3);
   if (lmax < 2) return;
   for (int d = 0; d < 3; ++d) {
     pw[d][0] = pw[d][1] = pw[d][2] = 1.0;
@@ -716,7 +734,7 @@ int oracle_ao_hessian_doc(const oracle_basis* b, int32_t precision, int64_t poin
   double* sh = (double*)malloc(sizeof(double) * 12 * S * point_num);
   oracle_shell_vgl_doc(b, precision, point_num, coord, nucl_coord, sv);
   oracle_shell_hessian_doc(b, precision, point_num, coord, nucl_coord, sh);
-  double poly[5][20], ph[20][4][3];
+  double poly[5][ORACLE_NPOLY], ph[ORACLE_NPOLY][4][3];
   for (int64_t ip = 0; ip < point_num; ++ip) {
     for (int i = 0; i < 3; ++i) memset(ao_hessian + (i * point_num + ip) * 4 * A, 0, sizeof(double) * 4 * A);
     const double X[3] = {coord[ip], coord[ip + point_num], coord[ip + 2 * point_num]};

@@ -43,6 +43,12 @@ typedef struct oracle_basis_in {
 
 typedef struct oracle_basis oracle_basis;  /* finalized tables (opaque) */
 
+/* Largest shell angular momentum the oracle evaluates (k shells, l = 7,
+ * the largest the reference's own polynomial tests exercise,
+ * org/qmckl_ao.org:7042-7076). */
+#define ORACLE_MAX_L 7
+
+/* NULL when a shell has l < 0 or l > ORACLE_MAX_L. */
 oracle_basis* oracle_basis_create(const oracle_basis_in* in);
 void          oracle_basis_destroy(oracle_basis* b);
 double        oracle_nucleus_range(const oracle_basis* b, int64_t inucl);
@@ -66,6 +72,14 @@ int oracle_shell_vgl_doc(const oracle_basis* b, int32_t precision, int64_t point
                          const double* coord, const double* nucl_coord, double* shell_vgl);
 int oracle_ao_vgl_doc(const oracle_basis* b, int32_t precision, int64_t point_num,
                       const double* coord, const double* nucl_coord, double* ao_vgl);
+
+/* Cartesian monomials of degree <= lmax at X - R with their gradient and
+ * Laplacian, vgl[c * 120 + m] (c = 0..4, m in the canonical order of
+ * org/qmckl_ao.org:5928-5933), by the HPC arithmetic (which = 1; shift added
+ * after the products, org/qmckl_ao.org:6624-6914) or the doc arithmetic
+ * (which = 0; shift added to the displacement, 6233-6364).  Returns the
+ * number of monomials, -1 for lmax outside 0..ORACLE_MAX_L. */
+int oracle_poly_vgl(int32_t which, int32_t lmax, const double* X, const double* R, double* vgl);
 
 /* MO contraction, skipping AOs whose value is zero (org/qmckl_mo.org:2015-2163). */
 int oracle_mo_vgl(int64_t ao_num, int64_t mo_num, int64_t point_num,

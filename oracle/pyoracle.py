@@ -46,6 +46,8 @@ def lib():
                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.oracle_forces.argtypes = [C.c_void_p, C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oracle_poly_vgl.restype = C.c_int
+        L.oracle_poly_vgl.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]
         for f in ("oracle_mo_vgl", "oracle_mo_value"):
             getattr(L, f).argtypes = [C.c_int64, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]
         _lib = L
@@ -75,11 +77,43 @@ class Basis:
                                             "shell_prim_num", "shell_prim_index", "shell_factor",
                                             "exponent", "coefficient", "prim_factor", "ao_factor")))
         self.h = lib().oracle_basis_create(C.byref(bi))
+        if not self.h:
+            raise ValueError("oracle: shell angular momentum outside 0..7")
 
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:
             _lib.oracle_basis_destroy(self.h)
             self.h = None
+
+
+MAX_L = 7
+NPOLY = 120
+
+
+def poly_vgl(lmax, X, R, path="hpc"):
+    """Cartesian monomials of degree <= lmax at X - R: (vgl[5][n], n).
+
+    path "hpc" adds the 1e-20 shift after the products
+    (org/qmckl_ao.org:6624-6914), "doc" to the displacement (6233-6364)."""
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    R = np.ascontiguousarray(R, dtype=np.float64)
+    out = np.zeros((5, NPOLY), dtype=np.float64)
+    n = lib().oracle_poly_vgl(1 if path == "hpc" else 0, lmax, _p(X), _p(R), _p(out))
+    if n < 0:
+        raise ValueError("lmax outside 0..7")
+    return out[:, :n], n
+
+
+def monomial_powers(lmax):
+    """(a, b, c) of every monomial of degree <= lmax in the reference's
+    canonical order: l ascending, then a descending, then b descending
+    (org/qmckl_ao.org:5928-5933)."""
+    out = []
+    for l in range(lmax + 1):
+        for a in range(l, -1, -1):
+            for b in range(l - a, -1, -1):
+                out.append((a, b, l - a - b))
+    return out
 
 
 def _coords(coord, nucl_coord):

@@ -363,6 +363,10 @@ struct DeviceState {
   std::vector<int64_t> fused_perm;
   DevBuf kskip, kstat;   // kstat: K blocks evaluated / dense, summed over the fused launches
   double krec_cutoff = -1.0;
+  // error word of the mixed form's tensor-core kernels: a bounded barrier
+  // wait that gives up writes its code here; it is read (and cleared) at the
+  // context's next synchronization point, never by the evaluation itself
+  DevBuf tc_err;
 };
 
 namespace {
@@ -673,12 +677,31 @@ qmckl_exit_code sync_cusp(qmckl_context context, DeviceState* ds, const double**
   return QMCKL_SUCCESS;
 }
 
+// Wait for the context's stream, then report (and clear) a bounded barrier
+// wait that gave up in a tensor-core kernel since the last check.
+qmckl_exit_code sync_and_check(qmckl_context context, DeviceState* ds, const char* where) {
+  int h = 0;
+  if (ds->tc_err.p != nullptr)
+    QB_CUDA(cudaMemcpyAsync(&h, ds->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, ds->stream), where);
+  QB_CUDA(cudaStreamSynchronize(ds->stream), where);
+  if (h != 0) {
+    QB_CUDA(cudaMemsetAsync(ds->tc_err.p, 0, sizeof(int), ds->stream), where);
+    QB_CUDA(cudaStreamSynchronize(ds->stream), where);
+    char msg[QMCKL_MAX_MSG_LEN];
+    std::snprintf(msg, sizeof msg,
+                  "a bounded barrier wait of a tensor-core kernel gave up (code %d): the mixed-form results "
+                  "enqueued since the last synchronization are not valid",
+                  h);
+    return qmckl_failwith(context, QMCKL_FAILURE, where, msg);
+  }
+  return QMCKL_SUCCESS;
+}
+
 qmckl_exit_code copy_out(qmckl_context context, DeviceState* ds, double* host, const void* dev, size_t bytes,
                          const char* where) {
   if (host != nullptr && bytes > 0)
     QB_CUDA(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, ds->stream), where);
-  QB_CUDA(cudaStreamSynchronize(ds->stream), where);
-  return QMCKL_SUCCESS;
+  return sync_and_check(context, ds, where);
 }
 
 DeviceState* state(qmckl_context context) { return ctx_of(context)->extra; }
@@ -777,6 +800,15 @@ qmckl_exit_code prepare_fused(qmckl_context context, DeviceState* ds, bool* usab
 qmckl_exit_code prepare_mixed(qmckl_context context, DeviceState* ds) {
   Context* ctx = ctx_of(context);
   const int64_t A = ctx->ao_basis.ao_num, M = ctx->mo_basis.mo_num;
+  if (ds->tc_err.p == nullptr) {
+    qmckl_exit_code rc = ensure(context, ds->tc_err, sizeof(int), "qmckl_b200_mo_mixed");
+    if (rc != QMCKL_SUCCESS) return rc;
+    QB_CUDA(cudaMemsetAsync(ds->tc_err.p, 0, sizeof(int), ds->stream), "qmckl_b200_mo_mixed");
+    // the allocation-free entry point's code and fixed scratch are loaded
+    // now, with this allocating call (a failure here only matters to it, and
+    // it reports its own)
+    if (tc_prime_unfused() != cudaSuccess || noalloc_prime() != cudaSuccess) cudaGetLastError();
+  }
   if (ds->tc3_coef_version != ctx->mo_basis.coef_version || !ds->tc3_coef.p) {
     TcPlan plan = tc_plan(A, M, 3);
     qmckl_exit_code rc = ensure(context, ds->tc3_coef, plan.coef_bytes, "qmckl_b200_mo_mixed");
@@ -851,7 +883,7 @@ qmckl_exit_code run_mo_mixed(qmckl_context context, DeviceState* ds, int64_t P, 
         double* o = out + a * comps * M;
         QB_CUDA(point_order(coord + a, n, lo, hi, keys, counts, perm, ds->stream, P), "qmckl_b200_mo_mixed");
         QB_CUDA(tc_run_fused(ds->T, ds->tc, n, comps, coord + a, cutoff_of(ctx), ds->tc_coef.p, ds->krec.p,
-                             ds->rec_bytes, perm, rb, o, ds->stream, P, ds->kskip.p,
+                             ds->rec_bytes, perm, rb, o, (int*)ds->tc_err.p, ds->stream, P, ds->kskip.p,
                              (unsigned long long*)ds->kstat.p, tplan),
                 "qmckl_b200_mo_mixed");
         if (cr != nullptr)
@@ -877,7 +909,8 @@ qmckl_exit_code run_mo_mixed(qmckl_context context, DeviceState* ds, int64_t P, 
   const size_t abytes = tc_a_bytes(ds->tc3, rows);
   qmckl_exit_code rc = ensure(context, ds->tc_a, abytes, "qmckl_b200_mo_mixed");
   if (rc != QMCKL_SUCCESS) return rc;
-  QB_CUDA(tc_run(ds->T, ds->tc3, P, comps, coord, cutoff_of(ctx), ds->tc3_coef.p, ds->tc_a.p, out, ds->stream,
+  QB_CUDA(tc_run(ds->T, ds->tc3, P, comps, coord, cutoff_of(ctx), ds->tc3_coef.p, ds->tc_a.p, out,
+                 (int*)ds->tc_err.p, ds->stream,
                  ds->tiles.ntiles > 0 ? &ds->tiles : nullptr, cr),
           "qmckl_b200_mo_mixed");
   if (cr != nullptr)
@@ -951,7 +984,8 @@ void dev_detach(Context* ctx) {
                     &ds->mo_vgl, &ds->mo_value, &ds->coef_t, &ds->tc_coef, &ds->tc_a, &ds->krec, &ds->order,
                     &ds->ao_hessian, &ds->coef_rows, &ds->adj_coord, &ds->adj_buf, &ds->adj_part, &ds->adj_nucl,
                     &ds->tc3_coef, &ds->env, &ds->nuc_ao, &ds->forces, &ds->adj_wp, &ds->adj_ct, &ds->adj_err,
-                    &ds->cusp, &ds->ao_masked, &ds->en_dist, &ds->mo_hessian, &ds->kskip, &ds->kstat})
+                    &ds->cusp, &ds->ao_masked, &ds->en_dist, &ds->mo_hessian, &ds->kskip, &ds->kstat,
+                    &ds->tc_err})
     release(*b);
   if (ds->copy_stream) {
     cudaStreamSynchronize(ds->copy_stream);
@@ -973,7 +1007,7 @@ qmckl_exit_code dev_prepared_mixed(qmckl_context context, PreparedMixed* out) {
   DeviceState* ds = ctx->extra;
   const char* fname = "qmckl_b200_mo_vgl_device_noalloc";
   if (ds == nullptr || ds->tables.p == nullptr || ds->basis_version != ctx->ao_basis.basis_version ||
-      ds->tc3_coef.p == nullptr || ds->tc3_coef_version != ctx->mo_basis.coef_version ||
+      ds->tc3_coef.p == nullptr || ds->tc3_coef_version != ctx->mo_basis.coef_version || ds->tc_err.p == nullptr ||
       (ds->stream == nullptr && !ds->stream_given))
     return qmckl_failwith(context, QMCKL_NOT_PROVIDED, fname,
                           "basis or MO coefficients not on the device yet: run one regular mixed-form "
@@ -992,6 +1026,7 @@ qmckl_exit_code dev_prepared_mixed(qmckl_context context, PreparedMixed* out) {
   out->coef = ds->tc3_coef.p;
   out->stream = ds->stream;
   out->cutoff = cutoff_of(ctx);
+  out->err = (int*)ds->tc_err.p;
   if (!ctx->mo_basis.r_cusp.empty()) {
     if (ds->cusp.p == nullptr || ds->cusp_version != ctx->mo_basis.cusp_version)
       return qmckl_failwith(context, QMCKL_NOT_PROVIDED, fname,
@@ -1404,8 +1439,20 @@ qmckl_exit_code qmckl_b200_set_stream(qmckl_context context, void* stream) {
 qmckl_exit_code qmckl_b200_synchronize(qmckl_context context) {
   if (qmckl_context_check(context) == QMCKL_NULL_CONTEXT) return QMCKL_INVALID_CONTEXT;
   DeviceState* ds = state(context);
-  if (!ds || !ds->stream) return QMCKL_SUCCESS;
-  QB_CUDA(cudaStreamSynchronize(ds->stream), "qmckl_b200_synchronize");
+  if (!ds || (!ds->stream && !ds->stream_given)) return QMCKL_SUCCESS;
+  if (ds->device >= 0) QB_CUDA(cudaSetDevice(ds->device), "qmckl_b200_synchronize");
+  return sync_and_check(context, ds, "qmckl_b200_synchronize");
+}
+
+qmckl_exit_code qmckl_b200_inject_wait_failure(qmckl_context context, const int32_t code) {
+  const char* fname = "qmckl_b200_inject_wait_failure";
+  if (qmckl_context_check(context) == QMCKL_NULL_CONTEXT) return QMCKL_INVALID_CONTEXT;
+  DeviceState* ds = state(context);
+  if (ds == nullptr || ds->tc_err.p == nullptr)
+    return qmckl_failwith(context, QMCKL_NOT_PROVIDED, fname, "no mixed-form evaluation on this context yet");
+  if (ds->device >= 0) QB_CUDA(cudaSetDevice(ds->device), fname);
+  QB_CUDA(cudaMemcpyAsync(ds->tc_err.p, &code, sizeof(int), cudaMemcpyHostToDevice, ds->stream), fname);
+  QB_CUDA(cudaStreamSynchronize(ds->stream), fname);
   return QMCKL_SUCCESS;
 }
 

@@ -283,19 +283,6 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-int* fused_err_word() {
-  static int* words[64] = {nullptr};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
-  if (!words[dev]) {
-    int* d = nullptr;
-    if (cudaMalloc(&d, sizeof(int)) != cudaSuccess) return nullptr;
-    if (cudaMemset(d, 0, sizeof(int)) != cudaSuccess) return nullptr;
-    words[dev] = d;
-  }
-  return words[dev];
-}
-
 size_t tile_plan_pts_bytes(int64_t tiles, int pts) { return ((size_t)tiles * 3 * pts * sizeof(double) + 255) / 256 * 256; }
 
 template <int PIECES, int COMPS>
@@ -395,28 +382,17 @@ cudaError_t tc_launch_fused(const TcPlan& plan, int64_t point_num, int comps, co
 
 cudaError_t tc_run_fused(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps, const double* coord,
                          double cutoff, const void* d_coef, const void* krec, int rec_bytes, const int* perm,
-                         const RowBound& rb, double* out, cudaStream_t s, int64_t cstride, const void* kskip,
-                         unsigned long long* kstat, void* tplan) {
+                         const RowBound& rb, double* out, int* err, cudaStream_t s, int64_t cstride,
+                         const void* kskip, unsigned long long* kstat, void* tplan) {
   (void)T;
   if (point_num <= 0) return cudaSuccess;
+  if (err == nullptr) return cudaErrorInvalidValue;
   CUtensorMap tb;
   cudaError_t e = tc_encode_coef_map(plan, d_coef, &tb);
   if (e != cudaSuccess) return e;
-  int* err = fused_err_word();
-  if (!err) return cudaErrorMemoryAllocation;
-  e = tc_launch_fused(plan, point_num, comps, coord, cutoff, tb, krec, rec_bytes, perm, d_coef, rb, out, err, s, cstride,
-                      kskip, kstat, tplan);
-  if (e != cudaSuccess) return e;
-  int h = 0;
-  e = cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s);
-  if (e != cudaSuccess) return e;
-  e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess) return e;
-  if (h != 0) {
-    cudaMemsetAsync(err, 0, sizeof(int), s);
-    return cudaErrorLaunchTimeout;
-  }
-  return cudaSuccess;
+  // a timed-out barrier wait stays in *err for the caller's next synchronization
+  return tc_launch_fused(plan, point_num, comps, coord, cutoff, tb, krec, rec_bytes, perm, d_coef, rb, out, err, s,
+                         cstride, kskip, kstat, tplan);
 }
 
 }  // namespace qb

@@ -596,20 +596,6 @@ int sm_count() {
   return sms;
 }
 
-// One error word per device, allocated on first use and kept for the process.
-int* err_word() {
-  static int* words[64] = {nullptr};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
-  if (!words[dev]) {
-    int* d = nullptr;
-    if (cudaMalloc(&d, sizeof(int)) != cudaSuccess) return nullptr;
-    if (cudaMemset(d, 0, sizeof(int)) != cudaSuccess) return nullptr;
-    words[dev] = d;
-  }
-  return words[dev];
-}
-
 template <int PIECES, int STAGES, typename OutT = double, bool TWO_ACC = false>
 cudaError_t launch_gemm(const CUtensorMap& ta, const CUtensorMap& tb, int64_t M, int n_out, int n_tile, int n_tiles,
                         int kblocks, int comps, const double* scales, OutT* out, int64_t ldo, int* err,
@@ -750,7 +736,7 @@ void tc_envelope(const ShellBound* shells, int nshell, double r_max, float r0, f
 }
 
 cudaError_t tc_run(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps, const double* coord,
-                   double cutoff, const void* d_coef, void* d_a, double* out, cudaStream_t s,
+                   double cutoff, const void* d_coef, void* d_a, double* out, int* err, cudaStream_t s,
                    const AoTiles* tiles, const double* cusp_r) {
   if (point_num <= 0) return cudaSuccess;
   if (plan.pieces != 3) return cudaErrorInvalidValue;   // the unfused kernels take 3 bfloat16 pieces
@@ -780,33 +766,26 @@ cudaError_t tc_run(const DevTables& T, const TcPlan& plan, int64_t point_num, in
   if (!make_map(&ta, a, plan.ao_num, rows, lda, plan.pieces, pstride, BM)) return cudaErrorInvalidValue;
   if (!make_map(&tb, d_coef, plan.ao_num, plan.n_pad, plan.k_pad, plan.pieces, plan.n_pad * plan.k_pad, plan.n_tile))
     return cudaErrorInvalidValue;
-  int* err = err_word();
-  if (!err) return cudaErrorMemoryAllocation;
+  if (!err) return cudaErrorInvalidValue;
   const int kblocks = (int)((plan.ao_num + BK - 1) / BK);
-  cudaError_t e;
-  e = launch_gemm<3, 2>(ta, tb, rows, (int)plan.mo_num, plan.n_tile, plan.n_tiles, kblocks, comps, sc, out,
-                        plan.mo_num, err, s);
-  if (e != cudaSuccess) return e;
-  // surface a timed-out barrier wait as an error (the word is cleared for the next call)
-  int h = 0;
-  e = cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s);
-  if (e != cudaSuccess) return e;
-  e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess) return e;
-  if (h != 0) {
-    cudaMemsetAsync(err, 0, sizeof(int), s);
-    return cudaErrorLaunchTimeout;
-  }
-  return cudaSuccess;
+  // a timed-out barrier wait stays in *err for the caller's next synchronization
+  return launch_gemm<3, 2>(ta, tb, rows, (int)plan.mo_num, plan.n_tile, plan.n_tiles, kblocks, comps, sc, out,
+                           plan.mo_num, err, s);
+}
+
+cudaError_t tc_prime_unfused() {
+  cudaFuncAttributes a;
+  cudaError_t e = cudaFuncGetAttributes(&a, ao_split_kernel<3, 5>);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, ao_split_kernel<3, 1>);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, tc_gemm_kernel<3, 2, double, false>);
+  return e;
 }
 
 cudaError_t tc_run_scratch(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps,
                            const double* coord, double cutoff, const void* d_coef, void* d_a, int* d_err,
                            double* out, cudaStream_t s, const double* cusp_r) {
   if (point_num <= 0) return cudaSuccess;
-  if (plan.pieces != 3) return cudaErrorInvalidValue;   // the unfused kernels take 3 bfloat16 pieces
-  cudaError_t e = cudaMemsetAsync(d_err, 0, sizeof(int), s);
-  if (e != cudaSuccess) return e;
+  if (plan.pieces != 3 || d_err == nullptr) return cudaErrorInvalidValue;   // 3 bfloat16 pieces
   const int64_t rows = (int64_t)comps * point_num;
   const int64_t lda = plan.k_pad;
   const int64_t pstride = rows * lda;
@@ -819,22 +798,15 @@ cudaError_t tc_run_scratch(const DevTables& T, const TcPlan& plan, int64_t point
   else
     ao_split_kernel<3, 1><<<grid, kAoWarps * 32, 0, s>>>(T, point_num, coord, cutoff, sc, a, lda, pstride, cusp_r);
   count_launch();
-  e = cudaGetLastError();
+  cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   CUtensorMap ta, tb;
   if (!make_map(&ta, a, plan.ao_num, rows, lda, plan.pieces, pstride, BM)) return cudaErrorInvalidValue;
   if (!make_map(&tb, d_coef, plan.ao_num, plan.n_pad, plan.k_pad, plan.pieces, plan.n_pad * plan.k_pad, plan.n_tile))
     return cudaErrorInvalidValue;
   const int kblocks = (int)((plan.ao_num + BK - 1) / BK);
-  e = launch_gemm<3, 2>(ta, tb, rows, (int)plan.mo_num, plan.n_tile, plan.n_tiles, kblocks, comps, sc, out,
-                        plan.mo_num, d_err, s);
-  if (e != cudaSuccess) return e;
-  int h = 0;
-  e = cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, s);
-  if (e != cudaSuccess) return e;
-  e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess) return e;
-  return h != 0 ? cudaErrorLaunchTimeout : cudaSuccess;
+  return launch_gemm<3, 2>(ta, tb, rows, (int)plan.mo_num, plan.n_tile, plan.n_tiles, kblocks, comps, sc, out,
+                           plan.mo_num, d_err, s);
 }
 
 // ------------------------------------------------------------ adjoint contractions

@@ -54,9 +54,12 @@ void tc_envelope(const ShellBound* shells, int nshell, double r_max, float r0, f
 // `tiles` selects the tiled AO kernel (ao_tile.cu) for the pieces when given;
 // cusp_r ([nucl], optional) leaves out the AOs of the cusp adjustment
 // (kernels.cuh cusp_masked; the untiled producer is used then).
+// err: a device word that a bounded barrier wait of the GEMM sets when it
+// gives up; it is left on the device for the caller to read at its next
+// synchronization point (the call itself does not synchronize).
 struct AoTiles;
 cudaError_t tc_run(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps, const double* coord,
-                   double cutoff, const void* d_coef, void* d_a, double* out, cudaStream_t s,
+                   double cutoff, const void* d_coef, void* d_a, double* out, int* err, cudaStream_t s,
                    const AoTiles* tiles = nullptr, const double* cusp_r = nullptr);
 
 // Fused form of tc_run: the AO pieces are produced in shared memory by the
@@ -72,7 +75,7 @@ cudaError_t tc_run(const DevTables& T, const TcPlan& plan, int64_t point_num, in
 // on their pipeline at once (the same blocks, the same results).
 cudaError_t tc_run_fused(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps, const double* coord,
                          double cutoff, const void* d_coef, const void* krec, int rec_bytes, const int* perm,
-                         const fz::RowBound& rb, double* out, cudaStream_t s, int64_t cstride = -1,
+                         const fz::RowBound& rb, double* out, int* err, cudaStream_t s, int64_t cstride = -1,
                          const void* kskip = nullptr, unsigned long long* kstat = nullptr, void* tplan = nullptr);
 size_t tc_kskip_bytes(int64_t ao_num, int64_t shell_num);
 size_t tc_tile_plan_bytes(const TcPlan& plan, int64_t point_num, int comps);
@@ -95,9 +98,8 @@ cudaError_t point_order(const double* coord, int64_t point_num, const double* bo
 // dynamic shared memory of the fused kernel (must stay <= 227 KB)
 size_t tc_fused_smem(const TcPlan& plan, int comps, int rec_bytes);
 
-// Same evaluation with caller-provided scratch: the A pieces in d_a and the
-// barrier-timeout word in d_err (cleared here before the launches).  Makes no
-// device allocation.
+// Same evaluation with caller-provided scratch: the A pieces in d_a.  Makes
+// no device allocation.
 cudaError_t tc_run_scratch(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps,
                            const double* coord, double cutoff, const void* d_coef, void* d_a, int* d_err,
                            double* out, cudaStream_t s, const double* cusp_r = nullptr);
@@ -133,6 +135,14 @@ struct PreparedMixed {
   // cubics' parameters [nucl][4][mo] on the device
   const double* cusp_r = nullptr;
   const double* cusp_prm = nullptr;
+  int* err = nullptr;   // the context's error word of the tensor-core kernels
 };
+
+// Load, during a regular evaluation, the device code and data the
+// allocation-free entry point uses later (lazy module loading would
+// otherwise allocate device memory at its first call): the unfused kernels
+// (mo_tc.cu) and the fixed scratch array (noalloc.cu).
+cudaError_t tc_prime_unfused();
+cudaError_t noalloc_prime();
 
 }  // namespace qb

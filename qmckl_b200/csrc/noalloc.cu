@@ -1,14 +1,12 @@
 // Mixed-form MO VGL with all scratch in a fixed, library-owned device array.
 //
 // Some callers cannot allocate device memory at the moment they need MO
-// values: a QMC code whose memory is owned by a pool allocator that has
-// reserved the free memory up front (a new cudaMalloc would fail), a code
-// that issues work from a CUDA host callback (where CUDA calls that allocate
-// are not permitted), or a time-step loop that cannot afford the implicit
-// device synchronization of cudaMalloc/cudaFree.  For them,
+// values: a QMC code whose device memory is owned by a pool allocator that
+// reserved the free memory up front (a new cudaMalloc would fail, and
+// cudaFree would hand memory back behind the pool's back).  For them,
 // qmckl_b200_mo_vgl_device_noalloc evaluates the mixed form exactly like
-// qmckl_b200_mo_vgl_device, but its scratch (the bfloat16 pieces of the AO
-// matrix and the barrier-timeout word) lives in g_scratch below instead of
+// qmckl_b200_mo_vgl_device with the unfused kernels, but its scratch (the
+// bfloat16 pieces of the AO matrix) lives in g_scratch below instead of
 // device memory allocated by the library.  The caller still passes the
 // coordinates and the output buffer.
 #include <cstdio>
@@ -20,34 +18,27 @@
 namespace qb {
 namespace {
 
-// Fixed scratch: 32 MiB.  The first 256 bytes hold the timeout word, the rest
-// the AO pieces.  Every GPU that loads the library holds this array until the
-// process exits.
+// Fixed scratch: 32 MiB of AO pieces.  Every GPU that loads the library holds
+// this array until the process exits.
 constexpr size_t kScratchBytes = size_t(32) << 20;
-constexpr size_t kWordBytes = 256;
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-void* g_scratch_ptr[kMaxDevices] = {nullptr};   // device address of g_scratch, per device
-
 // Device address of g_scratch on the current device.  In host code the
-// symbol g_scratch is only a host-side stand-in, never a device address.
-cudaError_t scratch_address(void** ptr) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-  if (g_scratch_ptr[dev] == nullptr) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_scratch);
-    if (e != cudaSuccess) return e;
-    g_scratch_ptr[dev] = p;
-  }
-  *ptr = g_scratch_ptr[dev];
-  return cudaSuccess;
-}
+// symbol g_scratch is only a host-side stand-in, never a device address.  The
+// lookup is repeated on every call (it costs nothing once the module is
+// loaded), so a recreated primary context never leaves a stale address.
+cudaError_t scratch_address(void** ptr) { return cudaGetSymbolAddress(ptr, g_scratch); }
 
 }  // namespace
+
+// Called by every context's first regular mixed-form evaluation: the first
+// lookup loads this file's module and with it the 32 MiB array, at a time
+// when the library is allowed to allocate.
+cudaError_t noalloc_prime() {
+  void* p = nullptr;
+  return scratch_address(&p);
+}
+
 }  // namespace qb
 
 using namespace qb;
@@ -65,9 +56,9 @@ extern "C" qmckl_exit_code qmckl_b200_mo_vgl_device_noalloc(qmckl_context contex
   PreparedMixed pm;
   qmckl_exit_code rc = dev_prepared_mixed(context, &pm);
   if (rc != QMCKL_SUCCESS) return rc;
-  const size_t need = tc_a_bytes(pm.plan, 5 * point_num);
-  if (need > kScratchBytes - kWordBytes) {
-    const int64_t max_points = (int64_t)((kScratchBytes - kWordBytes) / tc_a_bytes(pm.plan, 5));
+  // the largest point count first, so that no product below can overflow
+  const int64_t max_points = (int64_t)(kScratchBytes / tc_a_bytes(pm.plan, 5));
+  if (point_num > max_points) {
     char msg[QMCKL_MAX_MSG_LEN];
     std::snprintf(msg, sizeof msg,
                   "point_num %lld exceeds the fixed 32 MiB scratch: at most %lld points per call for this basis",
@@ -82,15 +73,11 @@ extern "C" qmckl_exit_code qmckl_b200_mo_vgl_device_noalloc(qmckl_context contex
     std::snprintf(msg, sizeof msg, "cudaGetSymbolAddress of the fixed scratch failed: %s", cudaGetErrorString(e));
     return qmckl_failwith(context, QMCKL_FAILURE, fname, msg);
   }
-  int* d_err = (int*)base;
-  void* d_a = (unsigned char*)base + kWordBytes;
-  e = tc_run_scratch(pm.T, pm.plan, point_num, 5, d_coord, pm.cutoff, pm.coef, d_a, d_err, d_mo_vgl, pm.stream,
+  e = tc_run_scratch(pm.T, pm.plan, point_num, 5, d_coord, pm.cutoff, pm.coef, base, pm.err, d_mo_vgl, pm.stream,
                      pm.cusp_r);
-  if (e == cudaSuccess && pm.cusp_r != nullptr) {
+  if (e == cudaSuccess && pm.cusp_r != nullptr)
     e = launch_cusp_mo(point_num, 5, d_coord, point_num, pm.T.nucl_num, pm.T.nucl_coord, pm.cusp_r, pm.cusp_prm,
                        (int)pm.plan.mo_num, d_mo_vgl, pm.stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(pm.stream);
-  }
   if (e != cudaSuccess) {
     char msg[QMCKL_MAX_MSG_LEN];
     std::snprintf(msg, sizeof msg, "CUDA error: %s", cudaGetErrorString(e));

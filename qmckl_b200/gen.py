@@ -39,6 +39,9 @@ SHAPES = {
     "dz_h": [0, 0, 1],
     "tz_heavy": [0, 0, 0, 0, 1, 1, 1, 2, 2, 3],
     "tz_h": [0, 0, 0, 1, 1, 2],
+    # high angular momentum: g, h shells on one kind of atom, g, i, k on the other
+    "hl_a": [0, 0, 1, 2, 3, 4, 5],
+    "hl_b": [0, 1, 2, 4, 6, 7],
 }
 
 
@@ -88,15 +91,17 @@ def _shell(rng, l, heavy, first_s):
     return expo, coef, pf
 
 
-def build_system(rng, charges, coords, shape_heavy, shape_h, mo_num, walk_num, elec_num=None):
-    """Assemble every array of the qmckl setters for one molecule."""
+def build_system(rng, charges, coords, shape_heavy, shape_h, mo_num, walk_num, elec_num=None, shapes=None):
+    """Assemble every array of the qmckl setters for one molecule (shapes:
+    optional list of shell angular momenta per nucleus, replacing the
+    heavy / H shapes)."""
     nucl_num = len(charges)
     nucleus_index, nucleus_shell_num = [], []
     shell_ang_mom, shell_prim_num, shell_prim_index = [], [], []
     exponent, coefficient, prim_factor, ao_factor = [], [], [], []
     for n, z in enumerate(charges):
         heavy = z > 1
-        shape = shape_heavy if heavy else shape_h
+        shape = shapes[n] if shapes is not None else (shape_heavy if heavy else shape_h)
         nucleus_index.append(len(shell_ang_mom))
         nucleus_shell_num.append(len(shape))
         first_s = True
@@ -171,6 +176,17 @@ def config(cid, walk_num=None, seed=None):
         return build_system(rng, charges, coords, SHAPES["tz_heavy"], SHAPES["tz_h"], 350,
                             walk_num or 256, elec_num=700)
     raise ValueError(f"no single-molecule config {cid}")
+
+
+def high_l_config(walk_num=16, seed=20260007):
+    """A small molecule whose basis reaches l = 7: 3 atoms (Z = 6) with
+    s s p d f g h shells (57 AOs each) and 3 atoms (Z = 8) with s p d g i k
+    shells (89 AOs each) in a 6-bohr cube; 438 AOs, 120 MOs, 42 electrons."""
+    rng = np.random.default_rng(seed)
+    charges = [6.0, 8.0, 6.0, 8.0, 6.0, 8.0]
+    coords = place_nuclei(rng, 6, 6.0)
+    nucleus_shapes = [SHAPES["hl_a"] if z == 6.0 else SHAPES["hl_b"] for z in charges]
+    return build_system(rng, charges, coords, None, None, 120, walk_num, shapes=nucleus_shapes)
 
 
 def batch_config(num_systems=256, seed=20260002, max_walkers=256):

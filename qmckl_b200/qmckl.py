@@ -438,6 +438,11 @@ def b200_inject_alloc_failure(n):
     lib().qmckl_b200_inject_alloc_failure(C.c_int64(n))
 
 
+def b200_inject_wait_failure(ctx, code):
+    """Test hook: mark the context's tensor-core error word as a bounded wait that gave up."""
+    _call("qmckl_b200_inject_wait_failure", ctx, C.c_int32(code))
+
+
 # ------------------------------------------------------ batched systems
 
 

@@ -54,6 +54,57 @@ def parity_error(got, ref, floor=1e-2):
     return float((np.abs(got - ref) / den).max())
 
 
+COMPONENTS = ("value", "grad_x", "grad_y", "grad_z", "laplacian")
+
+
+def elementwise_rel_error(got, ref, floor=1e-8):
+    """Per component of [P][5][n] arrays: max |got - ref| / |ref| over the
+    elements with |ref| > floor * max |ref| of that component; 5 floats."""
+    out = []
+    for c in range(ref.shape[1]):
+        r = ref[:, c, :]
+        g = got[:, c, :]
+        s = np.abs(r).max()
+        m = np.abs(r) > floor * s
+        out.append(float((np.abs(g[m] - r[m]) / np.abs(r[m])).max()) if m.any() else 0.0)
+    return out
+
+
+def row_floored_error(got, ref, floor=1e-2):
+    """Per component of [P][5][n] arrays: parity_error restricted to that component; 5 floats."""
+    return [parity_error(got[:, c, :], ref[:, c, :], floor) for c in range(ref.shape[1])]
+
+
+def bits_of_agreement(a, b):
+    """Bits two FP64 arrays agree on, element-wise: the reference's
+    qmckl_test_precision_64 (org/qmckl_numprec.org:384-430).  The distance in
+    units in the last place is the difference of the two bit patterns (0 bits
+    when the signs differ and neither value is zero); the result is 53 minus
+    the bit length of that distance, at least 0."""
+    af = np.ascontiguousarray(a, dtype=np.float64).ravel()
+    bf = np.ascontiguousarray(b, dtype=np.float64).ravel()
+    x, y = af.view(np.int64), bf.view(np.int64)
+    same = (x < 0) == (y < 0)
+    d = np.zeros(x.size, dtype=np.int64)
+    d[same] = np.abs(x[same] - y[same])          # same sign: no overflow
+    out = 53 - np.minimum(53, np.frexp(d.astype(np.float64))[1])   # frexp exponent = bit length
+    for i in np.flatnonzero(~same):
+        if af[i] != 0.0 and bf[i] != 0.0:
+            out[i] = 0
+        else:   # one of them is +-0: the plain difference of the bit patterns
+            out[i] = 53 - min(53, abs(int(x[i]) - int(y[i])).bit_length())
+    return out.astype(np.int32).reshape(np.shape(a))
+
+
+def mixed_error_report(got, ref):
+    """The three error measures of the mixed form against an FP64 reference,
+    per component: max|diff| / max|ref|, the row-floored relative error and
+    the element-wise relative error (|ref| > 1e-8 max|ref|)."""
+    return {"max_abs_over_max_ref": dict(zip(COMPONENTS, comp_error(got, ref))),
+            "row_floored_rel": dict(zip(COMPONENTS, row_floored_error(got, ref))),
+            "elementwise_rel": dict(zip(COMPONENTS, elementwise_rel_error(got, ref)))}
+
+
 def comp_error(got, ref):
     """Per-component max|got - ref| / max|ref| for arrays [P][5][n]; returns 5 floats."""
     out = []

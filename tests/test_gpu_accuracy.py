@@ -1,0 +1,143 @@
+"""Inputs at the edges of what the library accepts, and the accuracy of the
+mixed form under relative measures, against the CPU oracle (GPU).
+
+* Angular momenta up to l = 7 (g, h, i, k shells): the FP64 form within the
+  parity bar, the mixed form (fused and unfused kernels) within its bound.
+* The config-4 shape (5000 AOs, 350 MOs: three MO tiles of the fused kernel)
+  on a subset of its walkers.
+* The mixed form's error measured three ways per component (value, three
+  gradient components, Laplacian): max|diff| / max|ref|, the row-floored
+  relative error of the FP64 parity metric, and the element-wise relative
+  error over |ref| > 1e-8 max|ref|; plus the reference's own acceptance test
+  for reduced precision, the average number of bits the result shares with
+  the FP64 one (org/qmckl_mo.org:3798-3861).
+"""
+import numpy as np
+import pytest
+
+from conftest import (bits_of_agreement, comp_error, elementwise_rel_error, mixed_error_report, parity_error,
+                      row_floored_error)
+from oracle import pyoracle as O
+from qmckl_b200 import gen
+from qmckl_b200 import qmckl as pq
+from qmckl_b200.system import make_context
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+MIXED_TOL = 1e-6          # max |mixed - fp64| / max |fp64| per component
+
+
+def _oracle_mo(d, pts=None):
+    pts = gen.points(d) if pts is None else pts
+    ao = O.ao_vgl(O.Basis(d), pts, d["nucl_coord"])
+    return O.mo_vgl(d["mo_coef"], ao), ao
+
+
+def _eval(d, form, fused=1, pieces=3):
+    P = d["elec_coord"].shape[0] * d["elec_coord"].shape[1]
+    ctx = make_context(d, form=form)
+    if form == pq.FORM_MIXED:
+        pq.b200_set_mixed_kernel(ctx, fused)
+        pq.b200_set_split_terms(ctx, pieces)
+    try:
+        return pq.get_mo_basis_mo_vgl(ctx, P * 5 * d["mo_num"]).reshape(P, 5, d["mo_num"])
+    finally:
+        pq.context_destroy(ctx)
+
+
+@pytest.fixture(scope="module")
+def high_l():
+    d = gen.high_l_config(walk_num=16)
+    ref_mo, ref_ao = _oracle_mo(d)
+    return d, ref_mo, ref_ao
+
+
+def test_high_l_fp64(high_l):
+    """FP64 AO VGL, AO value, MO VGL and MO value with g, h, i, k shells."""
+    d, ref_mo, ref_ao = high_l
+    P, A, M = ref_ao.shape[0], d["ao_num"], d["mo_num"]
+    ctx = make_context(d, form=pq.FORM_FP64)
+    ao = pq.get_ao_basis_ao_vgl(ctx, P * 5 * A).reshape(P, 5, A)
+    assert parity_error(ao, ref_ao) < FP64_TOL
+    av = pq.get_ao_basis_ao_value(ctx, P * A).reshape(P, A)
+    assert parity_error(av, O.ao_value(O.Basis(d), gen.points(d), d["nucl_coord"])) < FP64_TOL
+    mo = pq.get_mo_basis_mo_vgl(ctx, P * 5 * M).reshape(P, 5, M)
+    assert parity_error(mo, ref_mo) < FP64_TOL
+    mv = pq.get_mo_basis_mo_value(ctx, P * M).reshape(P, M)
+    assert parity_error(mv, ref_mo[:, 0, :]) < FP64_TOL
+    pq.context_destroy(ctx)
+
+
+def test_high_l_ao_hessian(high_l):
+    d, _, _ = high_l
+    pts = gen.points(d)[:64]
+    dd = dict(d)
+    dd["elec_coord"] = pts.reshape(1, -1, 3)
+    dd["elec_up_num"], dd["elec_dn_num"] = 32, 32
+    ctx = make_context(dd, form=pq.FORM_FP64)
+    P, A = 64, d["ao_num"]
+    h = pq.get_ao_basis_ao_hessian(ctx, 3 * P * 4 * A).reshape(3, P, 4, A)
+    ref = O.ao_hessian(O.Basis(d), pts, d["nucl_coord"]).reshape(3, P, 4, A)
+    assert parity_error(h, ref) < FP64_TOL
+    pq.context_destroy(ctx)
+
+
+@pytest.mark.parametrize("fused", [1, 0])
+def test_high_l_mixed(high_l, fused):
+    d, ref_mo, _ = high_l
+    mo = _eval(d, pq.FORM_MIXED, fused=fused)
+    assert np.isfinite(mo).all()
+    assert max(comp_error(mo, ref_mo)) < MIXED_TOL, mixed_error_report(mo, ref_mo)
+
+
+@pytest.fixture(scope="module")
+def config4():
+    d = gen.config(4, walk_num=4)          # 2,800 points, 5000 AOs, 350 MOs
+    ref_mo, _ = _oracle_mo(d)
+    return d, ref_mo
+
+
+def test_config4_fp64(config4):
+    d, ref_mo = config4
+    mo = _eval(d, pq.FORM_FP64)
+    assert parity_error(mo, ref_mo) < FP64_TOL
+
+
+def test_config4_mixed_fused_three_mo_tiles(config4):
+    """350 MOs: the fused kernel runs three MO tiles per point tile."""
+    d, ref_mo = config4
+    mo = _eval(d, pq.FORM_MIXED, fused=1)
+    assert max(comp_error(mo, ref_mo)) < MIXED_TOL, mixed_error_report(mo, ref_mo)
+
+
+@pytest.fixture(scope="module")
+def mixed_cases(chbrclf):
+    cases = {}
+    for name, d in (("chbrclf", chbrclf), ("config0", gen.config(0)), ("config1_sub", gen.config(1, walk_num=16))):
+        ref, _ = _oracle_mo(d)
+        cases[name] = (ref, _eval(d, pq.FORM_MIXED))
+    return cases
+
+
+@pytest.mark.parametrize("name", ["chbrclf", "config0", "config1_sub"])
+def test_mixed_error_measures(mixed_cases, name):
+    """All three measures against the oracle, printed for the record
+    (pytest -s); the max-normalised one within 1e-6."""
+    ref, mo = mixed_cases[name]
+    rep = mixed_error_report(mo, ref)
+    print(name, rep)
+    assert max(comp_error(mo, ref)) < MIXED_TOL
+    assert max(row_floored_error(mo, ref)) < 1.0
+    assert max(elementwise_rel_error(mo, ref)) < 1e3
+
+
+@pytest.mark.parametrize("name", ["chbrclf", "config0", "config1_sub"])
+def test_mixed_bits_of_agreement(mixed_cases, name):
+    """The reference's single-precision acceptance test (org/qmckl_mo.org:3798-3861):
+    the average number of bits the reduced-precision MO VGL shares with the
+    FP64 one exceeds 11."""
+    ref, mo = mixed_cases[name]
+    bits = bits_of_agreement(mo, ref)
+    print(name, "average bits", bits.mean(), "per component", bits.mean(axis=(0, 2)))
+    assert bits.mean() > 11
