@@ -126,9 +126,11 @@ qmckl_exit_code qmckl_get_electron_down_num(const qmckl_context context, int64_t
 qmckl_exit_code qmckl_get_electron_walk_num(const qmckl_context context, int64_t* const walk_num);
 qmckl_exit_code qmckl_get_electron_coord(const qmckl_context context, const char transp,
                                          double* const coord, const int64_t size_max);
-/* TREXIO input (org/qmckl_trexio.org:1106-1188); this build has no TREXIO
- * and returns QMCKL_FAILURE "QMCkl was compiled without TREXIO", as the
- * reference does when built without it. */
+/* TREXIO input (org/qmckl_trexio.org:1106-1190): electrons, nuclei, AO basis
+ * and MO coefficients of a TREXIO file in the text backend (a directory of
+ * <group>.txt files), set through the context's setters as the reference's
+ * readers do.  Anything else (an HDF5 file) is QMCKL_INVALID_ARG_2, as the
+ * reference reports a file none of its backends opens. */
 qmckl_exit_code qmckl_trexio_read(const qmckl_context context, const char* file_name, const int64_t size_max);
 /* point-nucleus distances [point][nucl] (org/qmckl_electron.org:1205-1262) */
 qmckl_exit_code qmckl_get_electron_en_distance(qmckl_context context, double* const distance,

@@ -314,16 +314,6 @@ qmckl_exit_code qmckl_get_electron_coord(const qmckl_context context, const char
   return qmckl_get_point(context, transp, coord, size_max);
 }
 
-qmckl_exit_code qmckl_trexio_read(const qmckl_context context, const char* file_name, const int64_t size_max) {
-  // org/qmckl_trexio.org:1131-1188: this library is built without TREXIO
-  // (libtrexio and HDF5 are not available), which the reference reports the
-  // same way from the same entry point
-  (void)file_name;
-  (void)size_max;
-  if (qmckl_context_check(context) == QMCKL_NULL_CONTEXT) return QMCKL_INVALID_CONTEXT;
-  return qmckl_failwith(context, QMCKL_FAILURE, "qmckl_trexio_read", "QMCkl was compiled without TREXIO");
-}
-
 qmckl_exit_code qmckl_get_electron_en_distance(qmckl_context context, double* const distance, const int64_t size_max) {
   // org/qmckl_electron.org:1226-1262, 1270-1340: distances between the
   // context's points and the nuclei, [point][nucl], computed on the GPU

@@ -200,6 +200,18 @@ def get_electron_num(ctx):
     return v.value
 
 
+def get_electron_up_num(ctx):
+    v = C.c_int64()
+    _call("qmckl_get_electron_up_num", ctx, C.byref(v))
+    return v.value
+
+
+def get_electron_down_num(ctx):
+    v = C.c_int64()
+    _call("qmckl_get_electron_down_num", ctx, C.byref(v))
+    return v.value
+
+
 def get_electron_walk_num(ctx):
     v = C.c_int64()
     _call("qmckl_get_electron_walk_num", ctx, C.byref(v))
@@ -359,8 +371,8 @@ def b200_get_kblock_stats(ctx, reset=False):
 
 
 def trexio_read(ctx, file_name):
-    """qmckl_trexio_read: this build has no TREXIO and raises RuntimeError (the
-    reference's behaviour when built without it)."""
+    """qmckl_trexio_read: electrons, nuclei, AO basis and MO coefficients of a
+    TREXIO text-backend directory into the context (RuntimeError otherwise)."""
     b = file_name.encode()
     _call("qmckl_trexio_read", ctx, C.c_char_p(b), C.c_int64(len(b)))
 

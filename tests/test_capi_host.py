@@ -163,10 +163,11 @@ def test_compute_without_gpu_fails_loudly(chbrclf):
     pq.context_destroy(ctx)
 
 
-def test_trexio_read_reports_no_trexio():
-    """qmckl_trexio_read exists and fails as the reference does when built
-    without TREXIO (org/qmckl_trexio.org:1182-1186)."""
+def test_trexio_read_rejects_a_file_no_backend_opens():
+    """qmckl_trexio_read on a path that is not a TREXIO text-backend directory
+    fails with QMCKL_INVALID_ARG_2, as the reference does when none of its
+    backends opens the file (org/qmckl_trexio.org:1148-1155)."""
     ctx = pq.context_create()
-    with pytest.raises(RuntimeError, match="compiled without TREXIO"):
+    with pytest.raises(RuntimeError, match="Invalid argument 2"):
         pq.trexio_read(ctx, "fake.h5")
     pq.context_destroy(ctx)
