@@ -367,6 +367,12 @@ struct DeviceState {
   // wait that gives up writes its code here; it is read (and cleared) at the
   // context's next synchronization point, never by the evaluation itself
   DevBuf tc_err;
+  // tile-sparse FP64 contraction: AO of each fused K position, coefficient_t
+  // rows in the fused K order (built per coefficient and K order)
+  uint64_t korder_stamp = 0;            // bumped whenever fused_perm changes
+  uint64_t coef_f_version = ~0ull, coef_f_stamp = ~0ull;
+  DevBuf kidx, coef_f;
+  int64_t coef_f_ld = 0;
 };
 
 namespace {
@@ -732,14 +738,16 @@ qmckl_exit_code run_ao_value(qmckl_context context, DeviceState* ds, int64_t P, 
 // pieces of the fused plan in the same K order.  *usable = false when the AO
 // numbering allows no records or the kernel does not fit (the unfused kernels
 // are used then).
-qmckl_exit_code prepare_fused(qmckl_context context, DeviceState* ds, bool* usable) {
-  const char* fname = "qmckl_b200_mo_mixed";
+// The fused K order: K-block records, tile-skipping tables and fused_perm
+// (rebuilt on basis, nuclear, cusp or precision changes).  *ok = false when
+// the AO numbering allows no records.
+qmckl_exit_code prepare_korder(qmckl_context context, DeviceState* ds, bool* ok) {
+  const char* fname = "qmckl_b200_mo_korder";
   Context* ctx = ctx_of(context);
-  *usable = false;
+  *ok = false;
   const int64_t A = ctx->ao_basis.ao_num, M = ctx->mo_basis.mo_num;
-  const int pieces = ds->split_pieces;
   const double cutoff = cutoff_of(ctx);
-  const TcPlan plan = tc_plan(A, M, pieces);
+  const TcPlan plan = tc_plan(A, M, ds->split_pieces);
   // the VGL kernel decides the order; the value kernel (128-point tiles) may
   // still not fit, which run_mo_mixed checks per call
   auto fits = [&](int rec) { return tc_fused_smem(plan, 5, rec) <= 232448; };
@@ -770,9 +778,28 @@ qmckl_exit_code prepare_fused(qmckl_context context, DeviceState* ds, bool* usab
     if (perm != ds->fused_perm) {
       ds->fused_perm = std::move(perm);
       ds->tc_coef_version = ~0ull;   // the coefficient pieces follow the K order
+      ++ds->korder_stamp;
     }
   }
-  if (!fits(ds->rec_bytes)) return QMCKL_SUCCESS;
+  *ok = true;
+  return QMCKL_SUCCESS;
+}
+
+// The fused kernel's device tables: the K order above, and the coefficient
+// pieces of the fused plan in the same K order.  *usable = false when the AO
+// numbering allows no records or the kernel does not fit (the unfused
+// kernels are used then).
+qmckl_exit_code prepare_fused(qmckl_context context, DeviceState* ds, bool* usable) {
+  const char* fname = "qmckl_b200_mo_mixed";
+  Context* ctx = ctx_of(context);
+  *usable = false;
+  const int64_t A = ctx->ao_basis.ao_num, M = ctx->mo_basis.mo_num;
+  const int pieces = ds->split_pieces;
+  const TcPlan plan = tc_plan(A, M, pieces);
+  bool ok = false;
+  qmckl_exit_code rc0 = prepare_korder(context, ds, &ok);
+  if (rc0 != QMCKL_SUCCESS || !ok) return rc0;
+  if (tc_fused_smem(plan, 5, ds->rec_bytes) > 232448) return QMCKL_SUCCESS;
   if (ds->kstat.p == nullptr) {
     qmckl_exit_code rc = ensure(context, ds->kstat, 2 * sizeof(unsigned long long), fname);
     if (rc != QMCKL_SUCCESS) return rc;
@@ -832,6 +859,80 @@ qmckl_exit_code prepare_mixed(qmckl_context context, DeviceState* ds) {
   return QMCKL_SUCCESS;
 }
 
+// Box of the nuclei, widened by 4 bohr: the grid of the spatial point order.
+void nucleus_box(const Context* ctx, double* lo, double* hi) {
+  const int64_t N = ctx->nucleus.num;
+  for (int d = 0; d < 3; ++d) {
+    lo[d] = 1e300;
+    hi[d] = -1e300;
+  }
+  for (int64_t n = 0; n < N; ++n)
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = std::min(lo[d], ctx->nucleus.coord[n + d * N] - 4.0);
+      hi[d] = std::max(hi[d], ctx->nucleus.coord[n + d * N] + 4.0);
+    }
+}
+
+// FP64 MO contraction out[p][c][mo] = sum_k ao[p][c][k] coefficient_t[k][mo]
+// of P points (coordinates coord with stride cstride).  With the fused K
+// order available the contraction is tile-sparse: points in spatial tiles,
+// K in 64-AO blocks of the fused order, the blocks that vanish over a tile
+// (exact zeros) left out; otherwise the dense GEMM.
+qmckl_exit_code contract_f64(qmckl_context context, DeviceState* ds, int64_t P, int comps, const double* coord,
+                             int64_t cstride, const double* ao, double* out) {
+  const char* fname = "qmckl_b200_mo_fp64";
+  Context* ctx = ctx_of(context);
+  const int64_t A = ctx->ao_basis.ao_num, M = ctx->mo_basis.mo_num;
+  bool ok = false;
+  qmckl_exit_code rc = prepare_korder(context, ds, &ok);
+  if (rc != QMCKL_SUCCESS) return rc;
+  if (!ok || P <= 0) {
+    QB_CUDA(launch_gemm_f64(comps * P, M, A, ao, A, (const double*)ds->coef_t.p, M, out, M, ds->stream), fname);
+    return QMCKL_SUCCESS;
+  }
+  const int kblocks = (int)((A + 63) / 64);
+  const int64_t kpad = (int64_t)kblocks * 64;
+  if (ds->coef_f_version != ctx->mo_basis.coef_version || ds->coef_f_stamp != ds->korder_stamp || !ds->coef_f.p ||
+      !ds->kidx.p) {
+    const int64_t ld = (M + 1) / 2 * 2;
+    std::vector<int32_t> kidx((size_t)kpad, -1);
+    std::vector<double> cf((size_t)(kpad * ld), 0.0);
+    const std::vector<double>& c = ctx->mo_basis.coefficient;
+    for (int64_t k = 0; k < A; ++k) {
+      const int64_t a = ds->fused_perm[k];
+      kidx[(size_t)k] = (int32_t)a;
+      for (int64_t i = 0; i < M; ++i) cf[(size_t)(k * ld + i)] = c[(size_t)(i * A + a)];
+    }
+    rc = ensure(context, ds->kidx, sizeof(int32_t) * kidx.size(), fname);
+    if (rc != QMCKL_SUCCESS) return rc;
+    rc = ensure(context, ds->coef_f, sizeof(double) * cf.size(), fname);
+    if (rc != QMCKL_SUCCESS) return rc;
+    QB_CUDA(cudaMemcpy(ds->kidx.p, kidx.data(), sizeof(int32_t) * kidx.size(), cudaMemcpyHostToDevice), fname);
+    QB_CUDA(cudaMemcpy(ds->coef_f.p, cf.data(), sizeof(double) * cf.size(), cudaMemcpyHostToDevice), fname);
+    ds->coef_f_ld = ld;
+    ds->coef_f_version = ctx->mo_basis.coef_version;
+    ds->coef_f_stamp = ds->korder_stamp;
+  }
+  // scratch: keys[P], perm[P], cell counts, then the tile plan (256-byte aligned)
+  const TcPlan kp = tc_plan(A, M, 3);
+  const size_t sort_bytes = (sizeof(int) * 2 * (size_t)P + sizeof(unsigned int) * (kSortCells + 1) + 255) / 256 * 256;
+  rc = ensure(context, ds->order, sort_bytes + tc_tile_plan_bytes(kp, P, comps), fname);
+  if (rc != QMCKL_SUCCESS) return rc;
+  int* keys = (int*)ds->order.p;
+  int* perm = keys + P;
+  unsigned int* counts = (unsigned int*)(perm + P);
+  void* tplan = (uint8_t*)ds->order.p + sort_bytes;
+  double lo[3], hi[3];
+  nucleus_box(ctx, lo, hi);
+  QB_CUDA(point_order(coord, P, lo, hi, keys, counts, perm, ds->stream, cstride), fname);
+  const int* tinfo = nullptr;
+  QB_CUDA(tc_launch_tile_plan(P, comps, kblocks, coord, cstride, perm, ds->kskip.p, tplan, &tinfo, ds->stream), fname);
+  QB_CUDA(launch_gemm_f64_sparse(P, comps, M, ao, A, perm, tinfo, kblocks, (const int*)ds->kidx.p,
+                                 (const double*)ds->coef_f.p, ds->coef_f_ld, out, M, ds->stream),
+          fname);
+  return QMCKL_SUCCESS;
+}
+
 // Mixed-form MO VGL / value of P points into `out` (device).  With host_out
 // (the host getters), the fused path evaluates the points in slices and
 // copies each slice to the host on a second stream while the next slice is
@@ -862,13 +963,9 @@ qmckl_exit_code run_mo_mixed(qmckl_context context, DeviceState* ds, int64_t P, 
       int* perm = keys + P;
       unsigned int* counts = (unsigned int*)(perm + P);
       void* tplan = (uint8_t*)ds->order.p + sort_bytes;
-      double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+      double lo[3], hi[3];
+      nucleus_box(ctx, lo, hi);
       const int64_t N = ctx->nucleus.num;
-      for (int64_t n = 0; n < N; ++n)
-        for (int d = 0; d < 3; ++d) {
-          lo[d] = std::min(lo[d], ctx->nucleus.coord[n + d * N] - 4.0);
-          hi[d] = std::max(hi[d], ctx->nucleus.coord[n + d * N] + 4.0);
-        }
       fz::RowBound rb{(const double*)ds->nucl.p, (const float*)ds->env.p, (int)N, ds->env_r0, ds->env_inv_log2q};
       const int64_t M = ctx->mo_basis.mo_num;
       const bool slices = host_out != nullptr && P >= 8 * kSliceMinPoints;
@@ -922,7 +1019,7 @@ qmckl_exit_code run_mo_mixed(qmckl_context context, DeviceState* ds, int64_t P, 
 qmckl_exit_code run_mo(qmckl_context context, DeviceState* ds, int64_t P, const double* coord,
                        double* ao_scratch, double* out, int comps) {
   Context* ctx = ctx_of(context);
-  const int64_t A = ctx->ao_basis.ao_num, M = ctx->mo_basis.mo_num;
+  const int64_t M = ctx->mo_basis.mo_num;
   if (use_mixed(ctx)) return run_mo_mixed(context, ds, P, coord, out, comps);
   qmckl_exit_code rc = sync_coef(context, ds);
   if (rc != QMCKL_SUCCESS) return rc;
@@ -932,8 +1029,8 @@ qmckl_exit_code run_mo(qmckl_context context, DeviceState* ds, int64_t P, const 
   rc = comps == 5 ? run_ao_vgl(context, ds, P, coord, ao_scratch, cr)
                   : run_ao_value(context, ds, P, coord, ao_scratch, cr);
   if (rc != QMCKL_SUCCESS) return rc;
-  QB_CUDA(launch_gemm_f64(comps * P, M, A, ao_scratch, A, (const double*)ds->coef_t.p, M, out, M, ds->stream),
-          "qmckl_b200_mo");
+  rc = contract_f64(context, ds, P, comps, coord, P, ao_scratch, out);
+  if (rc != QMCKL_SUCCESS) return rc;
   if (cr != nullptr)
     QB_CUDA(launch_cusp_mo(P, comps, coord, P, (int)ctx->nucleus.num, (const double*)ds->nucl.p, cr, cprm, (int)M, out,
                            ds->stream),
@@ -985,7 +1082,7 @@ void dev_detach(Context* ctx) {
                     &ds->ao_hessian, &ds->coef_rows, &ds->adj_coord, &ds->adj_buf, &ds->adj_part, &ds->adj_nucl,
                     &ds->tc3_coef, &ds->env, &ds->nuc_ao, &ds->forces, &ds->adj_wp, &ds->adj_ct, &ds->adj_err,
                     &ds->cusp, &ds->ao_masked, &ds->en_dist, &ds->mo_hessian, &ds->kskip, &ds->kstat,
-                    &ds->tc_err})
+                    &ds->tc_err, &ds->kidx, &ds->coef_f})
     release(*b);
   if (ds->copy_stream) {
     cudaStreamSynchronize(ds->copy_stream);
@@ -1040,7 +1137,12 @@ qmckl_exit_code dev_prepared_mixed(qmckl_context context, PreparedMixed* out) {
 
 qmckl_exit_code dev_invalidate_mo(qmckl_context context) {
   DeviceState* ds = state(context);
-  if (ds) { ds->coef_version = ~0ull; ds->tc_coef_version = ~0ull; ds->tc3_coef_version = ~0ull; }
+  if (ds) {
+    ds->coef_version = ~0ull;
+    ds->tc_coef_version = ~0ull;
+    ds->tc3_coef_version = ~0ull;
+    ds->coef_f_version = ~0ull;
+  }
   return QMCKL_SUCCESS;
 }
 
@@ -1231,8 +1333,8 @@ qmckl_exit_code dev_provide_mo_vgl(qmckl_context context, double* host_out) {
         if (rc != QMCKL_SUCCESS) return rc;
         ctx->ao_basis.ao_vgl_date = ctx->date;
       }
-      QB_CUDA(launch_gemm_f64(5 * P, M, A, (const double*)ds->ao_vgl.p, A, (const double*)ds->coef_t.p, M,
-                              (double*)ds->mo_vgl.p, M, ds->stream), "qmckl_provide_mo_basis_mo_vgl");
+      rc = contract_f64(context, ds, P, 5, (const double*)ds->coord.p, P, (const double*)ds->ao_vgl.p,
+                        (double*)ds->mo_vgl.p);
     }
     if (rc != QMCKL_SUCCESS) return rc;
     ctx->mo_basis.mo_vgl_date = ctx->date;
@@ -1278,8 +1380,8 @@ qmckl_exit_code dev_provide_mo_value(qmckl_context context, double* host_out) {
           if (rc != QMCKL_SUCCESS) return rc;
           ctx->ao_basis.ao_value_date = ctx->date;
         }
-        QB_CUDA(launch_gemm_f64(P, M, A, (const double*)ds->ao_value.p, A, (const double*)ds->coef_t.p, M,
-                                (double*)ds->mo_value.p, M, ds->stream), "qmckl_provide_mo_basis_mo_value");
+        rc = contract_f64(context, ds, P, 1, (const double*)ds->coord.p, P, (const double*)ds->ao_value.p,
+                          (double*)ds->mo_value.p);
       }
       if (rc != QMCKL_SUCCESS) return rc;
     }

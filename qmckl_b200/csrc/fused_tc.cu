@@ -338,6 +338,27 @@ size_t tc_tile_plan_bytes(const TcPlan& plan, int64_t point_num, int comps) {
   return tile_plan_pts_bytes(tiles, pts) + sizeof(int) * (size_t)tiles * (kb + 4);
 }
 
+cudaError_t tc_launch_tile_plan(int64_t point_num, int comps, int kblocks, const double* coord, int64_t cstride,
+                                const int* perm, const void* kskip, void* tplan, const int** tinfo, cudaStream_t s) {
+  if (comps != 1 && comps != 5) return cudaErrorInvalidValue;
+  const int pts = BM / comps;
+  const int64_t tiles = (point_num + pts - 1) / pts;
+  *tinfo = (const int*)((uint8_t*)tplan + tile_plan_pts_bytes(tiles, pts));
+  if (point_num <= 0) return cudaSuccess;
+  if (cstride < point_num) cstride = point_num;
+  int* ti = (int*)*tinfo;
+  double* tp = (double*)tplan;
+  const size_t sm = sizeof(int) * (size_t)kblocks;
+  if (comps == 5)
+    tile_plan_kernel<BM / 5><<<(unsigned)tiles, 256, sm, s>>>(point_num, coord, cstride, perm, kblocks,
+                                                              (const uint8_t*)kskip, tp, ti, nullptr, 1);
+  else
+    tile_plan_kernel<BM><<<(unsigned)tiles, 256, sm, s>>>(point_num, coord, cstride, perm, kblocks,
+                                                          (const uint8_t*)kskip, tp, ti, nullptr, 1);
+  count_launch();
+  return cudaGetLastError();
+}
+
 size_t tc_kskip_bytes(int64_t ao_num, int64_t shell_num) {
   const int kb = (int)((ao_num + BK - 1) / BK);
   return (size_t)kskip_sph_offset(kb) + sizeof(double4) * (size_t)shell_num;

@@ -211,6 +211,144 @@ cudaError_t run_any(int64_t M, int64_t N, int64_t K, const double* A, int64_t ld
   return run_nt<4, TA>(M, N, K, A, lda, B, ldb, C, ldc, splits, s);
 }
 
+// Tile-sparse FP64 MO contraction.  Rows are (point, component) pairs of
+// tiles of PTS points in the spatial order perm (125 of the 128 tile rows
+// for VGL, 128 for values); the K dimension is the fused kernels' order
+// (shells by screening-radius class and nuclear position, 64-AO blocks) and
+// only the blocks that do not vanish over the tile are contracted (the
+// tile's list in tinfo, made by tile_plan_kernel): a skipped block holds
+// exact zeros, so the result is the dense product up to the summation order.
+//   ao    [P][COMPS][lda]     the AO matrix in the basis order (FP64 kernel)
+//   kidx  [kblocks * 64]      AO of each K position (-1: padding)
+//   Bf    [kblocks * 64][ldb] coefficient_t rows in the K order (zero rows
+//                             for the padding)
+//   out   [P][COMPS][ldc]
+// The A tile is gathered with 8-byte cp.async (the AOs of a K block are runs
+// of whole shells in the basis order); 128 x (16 NT) tiles, BK = 16, 3
+// stages, 8 warps as 4 (M) x 2 (N), mma.sync m8n8k4 f64 as the dense kernel.
+template <int NT, int COMPS>
+__global__ void __launch_bounds__(256)
+sparse_dgemm_kernel(int64_t P, int64_t N, const double* __restrict__ ao, int64_t lda, const int* __restrict__ perm,
+                    const int* __restrict__ tinfo, int kblocks, const int* __restrict__ kidx,
+                    const double* __restrict__ Bf, int64_t ldb, double* __restrict__ C, int64_t ldc,
+                    int64_t ntiles) {
+  constexpr int PTS = BM / COMPS;
+  constexpr int BN = 16 * NT;
+  constexpr int LDB_S = BN + 4;
+  extern __shared__ __align__(16) double smem[];
+  double* As = smem;                               // [STAGES][BM][LDA_S]
+  double* Bs = smem + STAGES * BM * LDA_S;         // [STAGES][BK][LDB_S]
+  __shared__ const double* rowp[BM];               // source row of each tile row (null: padding)
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp & 3, wn = warp >> 2;
+  const int g = lane >> 2, t = lane & 3;
+  const int64_t n0 = (int64_t)blockIdx.x * BN;
+
+  for (int64_t tile = blockIdx.y; tile < ntiles; tile += gridDim.y) {
+    const int64_t p0 = tile * PTS;
+    const int* ti = tinfo + tile * (int64_t)(kblocks + 4);
+    if (tid < BM) {
+      const int i = tid / COMPS, c = tid - i * COMPS;
+      const double* r = nullptr;
+      if (i < PTS && p0 + i < P) r = ao + ((int64_t)perm[p0 + i] * COMPS + c) * lda;
+      rowp[tid] = r;
+    }
+    __syncthreads();
+    const int ktiles = ti[0] * (64 / BK);
+    double acc[4][NT][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+    auto load_tile = [&](int kt, int st) {
+      const int64_t k0 = (int64_t)ti[4 + kt / (64 / BK)] * 64 + (kt % (64 / BK)) * BK;
+      double* as = As + st * BM * LDA_S;
+      double* bs = Bs + st * BK * LDB_S;
+#pragma unroll
+      for (int i = 0; i < BM * BK / 256; ++i) {
+        const int c = tid + i * 256;
+        const int row = c / BK, col = c % BK;
+        const double* r = rowp[row];
+        const int k = kidx[k0 + col];
+        const bool ok = r != nullptr && k >= 0;
+        cp_async8(as + row * LDA_S + col, ok ? r + k : ao, ok ? 8 : 0);
+      }
+      constexpr int BCH = BK * BN / 2;
+      for (int c = tid; c < BCH; c += 256) {
+        const int row = c / (BN / 2), col = (c % (BN / 2)) * 2;
+        const int64_t gn = n0 + col;
+        const int bytes = gn < N ? (int)((N - gn) < 2 ? (N - gn) : 2) * 8 : 0;
+        cp_async16(bs + row * LDB_S + col, bytes ? Bf + (k0 + row) * ldb + gn : Bf, bytes);
+      }
+    };
+
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; ++s) {
+      if (s < ktiles) load_tile(s, s);
+      cp_commit();
+    }
+    for (int kt = 0; kt < ktiles; ++kt) {
+      cp_wait<STAGES - 2>();
+      __syncthreads();
+      const int nk = kt + STAGES - 1;
+      if (nk < ktiles) load_tile(nk, nk % STAGES);
+      cp_commit();
+      const double* as = As + (kt % STAGES) * BM * LDA_S;
+      const double* bs = Bs + (kt % STAGES) * BK * LDB_S + wn * (8 * NT);
+#pragma unroll
+      for (int kk = 0; kk < BK; kk += 4) {
+        double af[4], bf[NT];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) af[i] = as[(wm * 32 + i * 8 + g) * LDA_S + kk + t];
+#pragma unroll
+        for (int j = 0; j < NT; ++j) bf[j] = bs[(kk + t) * LDB_S + j * 8 + g];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < NT; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+      }
+    }
+    cp_wait<0>();
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int r = wm * 32 + i * 8 + g;
+      if (rowp[r] == nullptr) continue;
+      const int ip = r / COMPS, c = r - ip * COMPS;
+      double* crow = C + ((int64_t)perm[p0 + ip] * COMPS + c) * ldc;
+#pragma unroll
+      for (int j = 0; j < NT; ++j) {
+        const int64_t n = n0 + wn * (8 * NT) + j * 8 + 2 * t;
+        if (n + 1 < N && ((ldc & 1) == 0)) {
+          *reinterpret_cast<double2*>(crow + n) = make_double2(acc[i][j][0], acc[i][j][1]);
+        } else {
+          if (n < N) crow[n] = acc[i][j][0];
+          if (n + 1 < N) crow[n + 1] = acc[i][j][1];
+        }
+      }
+    }
+    __syncthreads();   // rowp is rewritten for the next tile
+  }
+}
+
+template <int NT, int COMPS>
+cudaError_t run_sparse(int64_t P, int64_t N, const double* ao, int64_t lda, const int* perm, const int* tinfo,
+                       int kblocks, const int* kidx, const double* Bf, int64_t ldb, double* C, int64_t ldc,
+                       cudaStream_t s) {
+  constexpr int BN = 16 * NT;
+  constexpr int PTS = BM / COMPS;
+  const size_t smem = sizeof(double) * STAGES * (BM * LDA_S + BK * (BN + 4));
+  auto kern = sparse_dgemm_kernel<NT, COMPS>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int64_t ntiles = (P + PTS - 1) / PTS;
+  dim3 grid((unsigned)((N + BN - 1) / BN), (unsigned)std::min<int64_t>(ntiles, 65535));
+  kern<<<grid, 256, smem, s>>>(P, N, ao, lda, perm, tinfo, kblocks, kidx, Bf, ldb, C, ldc, ntiles);
+  count_launch();
+  return cudaGetLastError();
+}
+
 // out[n][m] (+)= sum_z part[z][m][n], through 32 x 32 shared tiles
 __global__ void add_transposed_kernel(const double* __restrict__ part, int splits, int64_t M, int64_t N,
                                       double* __restrict__ out, bool accumulate) {
@@ -244,6 +382,22 @@ cudaError_t launch_gemm_f64_tn_split(int64_t M, int64_t N, int64_t K, const doub
                                      int64_t ldb, double* part, int splits, cudaStream_t s) {
   if (splits < 1) return cudaErrorInvalidValue;
   return run_any<true>(M, N, K, A, lda, B, ldb, part, N, splits, s);
+}
+
+cudaError_t launch_gemm_f64_sparse(int64_t point_num, int comps, int64_t N, const double* ao, int64_t lda,
+                                   const int* perm, const int* tinfo, int kblocks, const int* kidx, const double* Bf,
+                                   int64_t ldb, double* C, int64_t ldc, cudaStream_t s) {
+  if (point_num <= 0 || N <= 0) return cudaSuccess;
+  if ((ldb & 1) != 0 || (reinterpret_cast<uintptr_t>(Bf) & 15) != 0) return cudaErrorInvalidValue;
+  // the N tile (64 or 80 columns) that wastes fewer padded columns
+  const bool nt5 = ((N + 79) / 80) * 80 - N < ((N + 63) / 64) * 64 - N;
+  if (comps == 5)
+    return nt5 ? run_sparse<5, 5>(point_num, N, ao, lda, perm, tinfo, kblocks, kidx, Bf, ldb, C, ldc, s)
+               : run_sparse<4, 5>(point_num, N, ao, lda, perm, tinfo, kblocks, kidx, Bf, ldb, C, ldc, s);
+  if (comps == 1)
+    return nt5 ? run_sparse<5, 1>(point_num, N, ao, lda, perm, tinfo, kblocks, kidx, Bf, ldb, C, ldc, s)
+               : run_sparse<4, 1>(point_num, N, ao, lda, perm, tinfo, kblocks, kidx, Bf, ldb, C, ldc, s);
+  return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_add_transposed(const double* part, int splits, int64_t M, int64_t N, double* out, bool accumulate,

@@ -118,6 +118,15 @@ cudaError_t launch_ao_vgl_split(const DevTables& T, int64_t point_num, const dou
 cudaError_t launch_gemm_f64(int64_t M, int64_t N, int64_t K, const double* A, int64_t lda,
                             const double* B, int64_t ldb, double* C, int64_t ldc, cudaStream_t s);
 
+// Tile-sparse FP64 MO contraction (gemm_f64.cu): out[p][c][n] = sum over the
+// K blocks of each tile's list (tinfo, from the tile plan of the fused
+// kernels; K in their order, kidx[k] = AO at K position k, -1 padding) of
+// ao[p][c][kidx[k]] * Bf[k][n]; points in tiles of 128 / comps in the order
+// perm.  Bf: ldb even and 16-byte aligned.
+cudaError_t launch_gemm_f64_sparse(int64_t point_num, int comps, int64_t N, const double* ao, int64_t lda,
+                                   const int* perm, const int* tinfo, int kblocks, const int* kidx, const double* Bf,
+                                   int64_t ldb, double* C, int64_t ldc, cudaStream_t s);
+
 // Split-K FP64 GEMM with A transposed: part[z][m][n] = sum over the z-th K
 // range of A[k][m] * B[k][n] (A element (m, k) at A[k * lda + m]), for
 // z < splits; part is [splits][M][N].
