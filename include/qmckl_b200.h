@@ -89,13 +89,13 @@ qmckl_exit_code qmckl_b200_ao_hessian_device(qmckl_context context, const int64_
  *   d_grad_coord [3][point] dL/d point coordinates (the d_coord layout)
  * Outputs are overwritten.  Nothing of a forward evaluation is reused: the
  * AOs and their derivatives are recomputed.  The context's form selects the
- * arithmetic: FP64 throughout (asynchronous on the context's stream, like the
- * other device entry points), or mixed: the contractions dL/dC = AO^T W and
+ * arithmetic: FP64 throughout, or mixed: the contractions dL/dC = AO^T W and
  * W C^T on the tensor cores as split-bfloat16 products accumulated in FP32
  * over slices of 2048 rows summed in FP64, FP32 exponentials and FP32
  * per-AO derivative arithmetic (gradients within ~4e-7 of the FP64 form's
- * largest entries); the mixed form synchronizes the stream before returning
- * to check its kernels' bounded waits. */
+ * largest entries).  Both forms return without synchronizing; a bounded
+ * wait of the mixed form's kernels that gives up is reported by the next
+ * qmckl_b200_synchronize. */
 qmckl_exit_code qmckl_b200_mo_vgl_adjoint_device(qmckl_context context, const int64_t point_num,
                                                  const double* d_coord, const double* d_weight,
                                                  double* d_grad_coef, double* d_grad_nucl, double* d_grad_coord);

@@ -349,10 +349,9 @@ struct DeviceState {
   DevBuf ao_hessian;
   uint64_t coef_rows_version = ~0ull;
   DevBuf coef_rows, adj_coord, adj_buf, adj_part, adj_nucl;
-  // mixed-form adjoint: bfloat16 pieces of the weights and of coefficient_t,
-  // the error word of its tensor-core kernels
+  // mixed-form adjoint: bfloat16 pieces of the weights and of coefficient_t
   uint64_t adj_ct_version = ~0ull;
-  DevBuf adj_wp, adj_ct, adj_err;
+  DevBuf adj_wp, adj_ct;
   // cusp adjustment: radii [nucl] followed by the cubics' parameters
   // [nucl][4][mo]; AO arrays with the left-out AOs zeroed, which feed only the
   // MO step; point-nucleus distances; MO Hessian
@@ -1080,7 +1079,7 @@ void dev_detach(Context* ctx) {
   for (DevBuf* b : {&ds->tables, &ds->nucl, &ds->coord, &ds->prim_vgl, &ds->shell_vgl, &ds->ao_vgl, &ds->ao_value,
                     &ds->mo_vgl, &ds->mo_value, &ds->coef_t, &ds->tc_coef, &ds->tc_a, &ds->krec, &ds->order,
                     &ds->ao_hessian, &ds->coef_rows, &ds->adj_coord, &ds->adj_buf, &ds->adj_part, &ds->adj_nucl,
-                    &ds->tc3_coef, &ds->env, &ds->nuc_ao, &ds->forces, &ds->adj_wp, &ds->adj_ct, &ds->adj_err,
+                    &ds->tc3_coef, &ds->env, &ds->nuc_ao, &ds->forces, &ds->adj_wp, &ds->adj_ct,
                     &ds->cusp, &ds->ao_masked, &ds->en_dist, &ds->mo_hessian, &ds->kskip, &ds->kstat,
                     &ds->tc_err, &ds->kidx, &ds->coef_f})
     release(*b);
@@ -1731,15 +1730,19 @@ qmckl_exit_code adjoint_mixed(qmckl_context context, DeviceState* ds, int64_t P,
   rc = ensure(context, ds->adj_coord, sizeof(double) * 3 * chunk, fname);
   if (rc == QMCKL_SUCCESS) rc = ensure(context, ds->adj_buf, (size_t)row_bytes * chunk, fname);
   if (rc == QMCKL_SUCCESS) rc = ensure(context, ds->adj_wp, sizeof(uint16_t) * 3 * 5 * chunk * ldw, fname);
-  if (rc == QMCKL_SUCCESS) rc = ensure(context, ds->adj_err, sizeof(int), fname);
+  if (rc == QMCKL_SUCCESS && ds->tc_err.p == nullptr) {
+    rc = ensure(context, ds->tc_err, sizeof(int), fname);
+    if (rc == QMCKL_SUCCESS) QB_CUDA(cudaMemsetAsync(ds->tc_err.p, 0, sizeof(int), s), fname);
+  }
   if (rc == QMCKL_SUCCESS && d_grad_coef) rc = ensure(context, ds->adj_part, sizeof(double) * splits * A * M, fname);
   if (rc == QMCKL_SUCCESS && !d_grad_nucl) rc = ensure(context, ds->adj_nucl, sizeof(double) * 3 * N, fname);
   if (rc != QMCKL_SUCCESS) return rc;
   double* gnucl = d_grad_nucl ? d_grad_nucl : (double*)ds->adj_nucl.p;
   void* buf = ds->adj_buf.p;
   double* cc = (double*)ds->adj_coord.p;
-  int* err = (int*)ds->adj_err.p;
-  QB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s), fname);
+  // a bounded wait that gives up is left in the context's error word for its
+  // next synchronization point (qmckl_b200_synchronize, a host getter)
+  int* err = (int*)ds->tc_err.p;
   for (int64_t p0 = 0; p0 < P; p0 += chunk) {
     const int64_t n = std::min<int64_t>(chunk, P - p0), rows = 5 * n;
     const double* w = d_weight + p0 * 5 * M;
@@ -1763,14 +1766,6 @@ qmckl_exit_code adjoint_mixed(qmckl_context context, DeviceState* ds, int64_t P,
                                         d_grad_coord ? d_grad_coord + p0 : nullptr, P, s),
               fname);
     }
-  }
-  int h = 0;
-  QB_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s), fname);
-  QB_CUDA(cudaStreamSynchronize(s), fname);
-  if (h != 0) {
-    char msg[QMCKL_MAX_MSG_LEN];
-    std::snprintf(msg, sizeof msg, "a tensor-core kernel of the adjoint gave up waiting (code %d)", h);
-    return qmckl_failwith(context, QMCKL_FAILURE, fname, msg);
   }
   return QMCKL_SUCCESS;
 }

@@ -141,3 +141,32 @@ def test_mixed_bits_of_agreement(mixed_cases, name):
     bits = bits_of_agreement(mo, ref)
     print(name, "average bits", bits.mean(), "per component", bits.mean(axis=(0, 2)))
     assert bits.mean() > 11
+
+
+def test_fp64_tile_sparse_contraction_ragged_and_far(chbrclf):
+    """The FP64 form's tile-sparse contraction (spatial tiles of 25 points, K
+    blocks that vanish over a tile skipped): point counts that end mid-tile,
+    MO VGL and MO value through the device entry points, and points far from
+    every nucleus (every block skipped: exact zeros)."""
+    import torch
+    ctx = make_context(chbrclf, points=False, form=pq.FORM_FP64)
+    A, M = chbrclf["ao_num"], chbrclf["mo_num"]
+    b = O.Basis(chbrclf)
+    for npts in (1, 25, 26, 131):
+        pts = gen.points(chbrclf)[:npts].copy()
+        if npts == 26:
+            pts[-1] += 300.0
+        dc = torch.tensor(np.ascontiguousarray(pts.T), dtype=torch.float64, device="cuda")
+        mo = torch.full((npts * 5 * M,), float("nan"), dtype=torch.float64, device="cuda")
+        mv = torch.full((npts * M,), float("nan"), dtype=torch.float64, device="cuda")
+        pq.b200_mo_vgl_device(ctx, npts, dc.data_ptr(), mo.data_ptr())
+        pq.b200_mo_value_device(ctx, npts, dc.data_ptr(), mv.data_ptr())
+        pq.b200_synchronize(ctx)
+        ref = O.mo_vgl(chbrclf["mo_coef"], O.ao_vgl(b, pts, chbrclf["nucl_coord"]))
+        got = mo.cpu().numpy().reshape(npts, 5, M)
+        assert parity_error(got, ref) < FP64_TOL, npts
+        refv = O.mo_value(chbrclf["mo_coef"], O.ao_value(b, pts, chbrclf["nucl_coord"]))
+        assert parity_error(mv.cpu().numpy().reshape(npts, M), refv) < FP64_TOL, npts
+        if npts == 26:
+            assert not got[-1].any()
+    pq.context_destroy(ctx)
