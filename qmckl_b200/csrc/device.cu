@@ -366,12 +366,13 @@ struct DeviceState {
   // wait that gives up writes its code here; it is read (and cleared) at the
   // context's next synchronization point, never by the evaluation itself
   DevBuf tc_err;
-  // tile-sparse FP64 contraction: AO of each fused K position, coefficient_t
-  // rows in the fused K order (built per coefficient and K order)
-  uint64_t korder_stamp = 0;            // bumped whenever fused_perm changes
-  uint64_t coef_f_version = ~0ull, coef_f_stamp = ~0ull;
-  DevBuf kidx, coef_f;
-  int64_t coef_f_ld = 0;
+  // tile-sparse FP64 contraction: screening spheres and AO ranges of the
+  // shells (basis order), coefficient_t with an even row length when the MO
+  // count is odd
+  uint64_t f64_sph_basis = ~0ull, f64_sph_nucl = ~0ull;
+  double f64_sph_cutoff = -1.0;
+  uint64_t coef_f_version = ~0ull;
+  DevBuf f64_sph, coef_f;
 };
 
 namespace {
@@ -777,7 +778,6 @@ qmckl_exit_code prepare_korder(qmckl_context context, DeviceState* ds, bool* ok)
     if (perm != ds->fused_perm) {
       ds->fused_perm = std::move(perm);
       ds->tc_coef_version = ~0ull;   // the coefficient pieces follow the K order
-      ++ds->korder_stamp;
     }
   }
   *ok = true;
@@ -873,62 +873,76 @@ void nucleus_box(const Context* ctx, double* lo, double* hi) {
 }
 
 // FP64 MO contraction out[p][c][mo] = sum_k ao[p][c][k] coefficient_t[k][mo]
-// of P points (coordinates coord with stride cstride).  With the fused K
-// order available the contraction is tile-sparse: points in spatial tiles,
-// K in 64-AO blocks of the fused order, the blocks that vanish over a tile
-// (exact zeros) left out; otherwise the dense GEMM.
+// of P points (coordinates coord with stride cstride), tile-sparse: points
+// in spatial tiles, and for each tile only the AOs of the shells that reach
+// one of its points (the others are exact zeros there), summed in the basis
+// order.
 qmckl_exit_code contract_f64(qmckl_context context, DeviceState* ds, int64_t P, int comps, const double* coord,
                              int64_t cstride, const double* ao, double* out) {
   const char* fname = "qmckl_b200_mo_fp64";
   Context* ctx = ctx_of(context);
-  const int64_t A = ctx->ao_basis.ao_num, M = ctx->mo_basis.mo_num;
-  bool ok = false;
-  qmckl_exit_code rc = prepare_korder(context, ds, &ok);
-  if (rc != QMCKL_SUCCESS) return rc;
-  if (!ok || P <= 0) {
-    QB_CUDA(launch_gemm_f64(comps * P, M, A, ao, A, (const double*)ds->coef_t.p, M, out, M, ds->stream), fname);
-    return QMCKL_SUCCESS;
+  const AoBasisRec& B = ctx->ao_basis;
+  const int64_t A = B.ao_num, M = ctx->mo_basis.mo_num, S = B.shell_num, N = ctx->nucleus.num;
+  if (P <= 0) return QMCKL_SUCCESS;
+  qmckl_exit_code rc;
+  const double cutoff = cutoff_of(ctx);
+  // shell screening spheres in the basis order
+  if (!ds->f64_sph.p || ds->f64_sph_basis != B.basis_version || ds->f64_sph_nucl != ctx->nucleus.coord_version ||
+      ds->f64_sph_cutoff != cutoff) {
+    std::vector<double4> sph((size_t)S);
+    std::vector<int2> sao((size_t)S);
+    for (int64_t m = 0; m < N; ++m)
+      for (int64_t sh = B.nucleus_index[m]; sh < B.nucleus_index[m] + B.nucleus_shell_num[m]; ++sh) {
+        const int l = B.shell_ang_mom[sh];
+        const int64_t a0 = B.d.ao_index[sh];
+        const int64_t na = std::max<int64_t>(0, std::min<int64_t>((int64_t)(l + 1) * (l + 2) / 2, A - a0));
+        sph[(size_t)sh] = make_double4(ctx->nucleus.coord[m], ctx->nucleus.coord[m + N], ctx->nucleus.coord[m + 2 * N],
+                                       shell_r2max(ctx, (int)sh, (int)m, cutoff));
+        sao[(size_t)sh] = make_int2((int)a0, (int)na);
+      }
+    const size_t sb = (sizeof(double4) * (size_t)S + 255) / 256 * 256;
+    rc = ensure(context, ds->f64_sph, sb + sizeof(int2) * (size_t)S, fname);
+    if (rc != QMCKL_SUCCESS) return rc;
+    QB_CUDA(cudaMemcpy(ds->f64_sph.p, sph.data(), sizeof(double4) * (size_t)S, cudaMemcpyHostToDevice), fname);
+    QB_CUDA(cudaMemcpy((uint8_t*)ds->f64_sph.p + sb, sao.data(), sizeof(int2) * (size_t)S, cudaMemcpyHostToDevice),
+            fname);
+    ds->f64_sph_basis = B.basis_version;
+    ds->f64_sph_nucl = ctx->nucleus.coord_version;
+    ds->f64_sph_cutoff = cutoff;
   }
-  const int kblocks = (int)((A + 63) / 64);
-  const int64_t kpad = (int64_t)kblocks * 64;
-  if (ds->coef_f_version != ctx->mo_basis.coef_version || ds->coef_f_stamp != ds->korder_stamp || !ds->coef_f.p ||
-      !ds->kidx.p) {
-    const int64_t ld = (M + 1) / 2 * 2;
-    std::vector<int32_t> kidx((size_t)kpad, -1);
-    std::vector<double> cf((size_t)(kpad * ld), 0.0);
-    const std::vector<double>& c = ctx->mo_basis.coefficient;
-    for (int64_t k = 0; k < A; ++k) {
-      const int64_t a = ds->fused_perm[k];
-      kidx[(size_t)k] = (int32_t)a;
-      for (int64_t i = 0; i < M; ++i) cf[(size_t)(k * ld + i)] = c[(size_t)(i * A + a)];
+  const size_t sb = (sizeof(double4) * (size_t)S + 255) / 256 * 256;
+  // coefficient_t with 16-byte aligned rows (a padded copy for an odd MO count)
+  const double* Bt = (const double*)ds->coef_t.p;
+  int64_t ldb = M;
+  if (M & 1) {
+    ldb = M + 1;
+    if (ds->coef_f_version != ctx->mo_basis.coef_version || !ds->coef_f.p) {
+      std::vector<double> cf((size_t)(A * ldb), 0.0);
+      const std::vector<double>& c = ctx->mo_basis.coefficient;
+      for (int64_t k = 0; k < A; ++k)
+        for (int64_t i = 0; i < M; ++i) cf[(size_t)(k * ldb + i)] = c[(size_t)(i * A + k)];
+      rc = ensure(context, ds->coef_f, sizeof(double) * cf.size(), fname);
+      if (rc != QMCKL_SUCCESS) return rc;
+      QB_CUDA(cudaMemcpy(ds->coef_f.p, cf.data(), sizeof(double) * cf.size(), cudaMemcpyHostToDevice), fname);
+      ds->coef_f_version = ctx->mo_basis.coef_version;
     }
-    rc = ensure(context, ds->kidx, sizeof(int32_t) * kidx.size(), fname);
-    if (rc != QMCKL_SUCCESS) return rc;
-    rc = ensure(context, ds->coef_f, sizeof(double) * cf.size(), fname);
-    if (rc != QMCKL_SUCCESS) return rc;
-    QB_CUDA(cudaMemcpy(ds->kidx.p, kidx.data(), sizeof(int32_t) * kidx.size(), cudaMemcpyHostToDevice), fname);
-    QB_CUDA(cudaMemcpy(ds->coef_f.p, cf.data(), sizeof(double) * cf.size(), cudaMemcpyHostToDevice), fname);
-    ds->coef_f_ld = ld;
-    ds->coef_f_version = ctx->mo_basis.coef_version;
-    ds->coef_f_stamp = ds->korder_stamp;
+    Bt = (const double*)ds->coef_f.p;
   }
-  // scratch: keys[P], perm[P], cell counts, then the tile plan (256-byte aligned)
-  const TcPlan kp = tc_plan(A, M, 3);
+  // scratch: keys[P], perm[P], cell counts, then the tiles' AO lists (256-byte aligned)
   const size_t sort_bytes = (sizeof(int) * 2 * (size_t)P + sizeof(unsigned int) * (kSortCells + 1) + 255) / 256 * 256;
-  rc = ensure(context, ds->order, sort_bytes + tc_tile_plan_bytes(kp, P, comps), fname);
+  rc = ensure(context, ds->order, sort_bytes + f64_plan_bytes(P, comps, A), fname);
   if (rc != QMCKL_SUCCESS) return rc;
   int* keys = (int*)ds->order.p;
   int* perm = keys + P;
   unsigned int* counts = (unsigned int*)(perm + P);
-  void* tplan = (uint8_t*)ds->order.p + sort_bytes;
+  void* plan = (uint8_t*)ds->order.p + sort_bytes;
   double lo[3], hi[3];
   nucleus_box(ctx, lo, hi);
   QB_CUDA(point_order(coord, P, lo, hi, keys, counts, perm, ds->stream, cstride), fname);
-  const int* tinfo = nullptr;
-  QB_CUDA(tc_launch_tile_plan(P, comps, kblocks, coord, cstride, perm, ds->kskip.p, tplan, &tinfo, ds->stream), fname);
-  QB_CUDA(launch_gemm_f64_sparse(P, comps, M, ao, A, perm, tinfo, kblocks, (const int*)ds->kidx.p,
-                                 (const double*)ds->coef_f.p, ds->coef_f_ld, out, M, ds->stream),
+  QB_CUDA(launch_f64_plan(P, comps, coord, cstride, perm, (int)S, ds->f64_sph.p, (uint8_t*)ds->f64_sph.p + sb, A, plan,
+                          ds->stream),
           fname);
+  QB_CUDA(launch_gemm_f64_sparse(P, comps, M, ao, A, perm, plan, A, Bt, ldb, out, M, ds->stream), fname);
   return QMCKL_SUCCESS;
 }
 
@@ -1081,7 +1095,7 @@ void dev_detach(Context* ctx) {
                     &ds->ao_hessian, &ds->coef_rows, &ds->adj_coord, &ds->adj_buf, &ds->adj_part, &ds->adj_nucl,
                     &ds->tc3_coef, &ds->env, &ds->nuc_ao, &ds->forces, &ds->adj_wp, &ds->adj_ct,
                     &ds->cusp, &ds->ao_masked, &ds->en_dist, &ds->mo_hessian, &ds->kskip, &ds->kstat,
-                    &ds->tc_err, &ds->kidx, &ds->coef_f})
+                    &ds->tc_err, &ds->f64_sph, &ds->coef_f})
     release(*b);
   if (ds->copy_stream) {
     cudaStreamSynchronize(ds->copy_stream);

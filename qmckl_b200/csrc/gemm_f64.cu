@@ -213,25 +213,25 @@ cudaError_t run_any(int64_t M, int64_t N, int64_t K, const double* A, int64_t ld
 
 // Tile-sparse FP64 MO contraction.  Rows are (point, component) pairs of
 // tiles of PTS points in the spatial order perm (125 of the 128 tile rows
-// for VGL, 128 for values); the K dimension is the fused kernels' order
-// (shells by screening-radius class and nuclear position, 64-AO blocks) and
-// only the blocks that do not vanish over the tile are contracted (the
-// tile's list in tinfo, made by tile_plan_kernel): a skipped block holds
-// exact zeros, so the result is the dense product up to the summation order.
-//   ao    [P][COMPS][lda]     the AO matrix in the basis order (FP64 kernel)
-//   kidx  [kblocks * 64]      AO of each K position (-1: padding)
-//   Bf    [kblocks * 64][ldb] coefficient_t rows in the K order (zero rows
-//                             for the padding)
+// for VGL, 128 for values).  The K dimension of a tile is its list of live
+// AOs (tlist, made by f64_plan_kernel): the AOs of the shells that do not
+// vanish at some point of the tile, in the basis order, padded with -1 to a
+// multiple of 16.  An AO left out is an exact zero at every point of the
+// tile, so the sum is the dense one in the basis order, without its zero
+// terms (the order of the reference's own contraction,
+// org/qmckl_mo.org:2015-2163, which skips the zero AOs of each point).
+//   ao    [P][COMPS][lda]    the AO matrix in the basis order (FP64 kernel)
+//   tlist [tiles][kmax]      live AOs of each tile, tcount[tile] entries
+//   Bt    [ao][ldb]          coefficient_t (ldb even, 16-byte aligned rows)
 //   out   [P][COMPS][ldc]
-// The A tile is gathered with 8-byte cp.async (the AOs of a K block are runs
-// of whole shells in the basis order); 128 x (16 NT) tiles, BK = 16, 3
-// stages, 8 warps as 4 (M) x 2 (N), mma.sync m8n8k4 f64 as the dense kernel.
+// A and B tiles are gathered by the list with cp.async (8-byte elements for
+// A, 16-byte pairs of B rows); 128 x (16 NT) tiles, BK = 16, 3 stages, 8
+// warps as 4 (M) x 2 (N), mma.sync m8n8k4 f64 as the dense kernel.
 template <int NT, int COMPS>
 __global__ void __launch_bounds__(256)
 sparse_dgemm_kernel(int64_t P, int64_t N, const double* __restrict__ ao, int64_t lda, const int* __restrict__ perm,
-                    const int* __restrict__ tinfo, int kblocks, const int* __restrict__ kidx,
-                    const double* __restrict__ Bf, int64_t ldb, double* __restrict__ C, int64_t ldc,
-                    int64_t ntiles) {
+                    const int* __restrict__ tlist, const int* __restrict__ tcount, int64_t kmax,
+                    const double* __restrict__ Bt, int64_t ldb, double* __restrict__ C, int64_t ldc, int64_t ntiles) {
   constexpr int PTS = BM / COMPS;
   constexpr int BN = 16 * NT;
   constexpr int LDB_S = BN + 4;
@@ -246,7 +246,7 @@ sparse_dgemm_kernel(int64_t P, int64_t N, const double* __restrict__ ao, int64_t
 
   for (int64_t tile = blockIdx.y; tile < ntiles; tile += gridDim.y) {
     const int64_t p0 = tile * PTS;
-    const int* ti = tinfo + tile * (int64_t)(kblocks + 4);
+    const int* kl = tlist + tile * kmax;
     if (tid < BM) {
       const int i = tid / COMPS, c = tid - i * COMPS;
       const double* r = nullptr;
@@ -254,7 +254,7 @@ sparse_dgemm_kernel(int64_t P, int64_t N, const double* __restrict__ ao, int64_t
       rowp[tid] = r;
     }
     __syncthreads();
-    const int ktiles = ti[0] * (64 / BK);
+    const int ktiles = tcount[tile] / BK;
     double acc[4][NT][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
@@ -262,7 +262,7 @@ sparse_dgemm_kernel(int64_t P, int64_t N, const double* __restrict__ ao, int64_t
       for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
     auto load_tile = [&](int kt, int st) {
-      const int64_t k0 = (int64_t)ti[4 + kt / (64 / BK)] * 64 + (kt % (64 / BK)) * BK;
+      const int* kk = kl + kt * BK;
       double* as = As + st * BM * LDA_S;
       double* bs = Bs + st * BK * LDB_S;
 #pragma unroll
@@ -270,7 +270,7 @@ sparse_dgemm_kernel(int64_t P, int64_t N, const double* __restrict__ ao, int64_t
         const int c = tid + i * 256;
         const int row = c / BK, col = c % BK;
         const double* r = rowp[row];
-        const int k = kidx[k0 + col];
+        const int k = kk[col];
         const bool ok = r != nullptr && k >= 0;
         cp_async8(as + row * LDA_S + col, ok ? r + k : ao, ok ? 8 : 0);
       }
@@ -278,8 +278,9 @@ sparse_dgemm_kernel(int64_t P, int64_t N, const double* __restrict__ ao, int64_t
       for (int c = tid; c < BCH; c += 256) {
         const int row = c / (BN / 2), col = (c % (BN / 2)) * 2;
         const int64_t gn = n0 + col;
-        const int bytes = gn < N ? (int)((N - gn) < 2 ? (N - gn) : 2) * 8 : 0;
-        cp_async16(bs + row * LDB_S + col, bytes ? Bf + (k0 + row) * ldb + gn : Bf, bytes);
+        const int k = kk[row];
+        const int bytes = (k >= 0 && gn < N) ? (int)((N - gn) < 2 ? (N - gn) : 2) * 8 : 0;
+        cp_async16(bs + row * LDB_S + col, bytes ? Bt + (int64_t)k * ldb + gn : Bt, bytes);
       }
     };
 
@@ -332,9 +333,77 @@ sparse_dgemm_kernel(int64_t P, int64_t N, const double* __restrict__ ao, int64_t
   }
 }
 
+// The live-AO list of each tile of PTS points (in the order perm): one CTA
+// per tile tests every shell's screening sphere (sph[s] = nucleus, squared
+// radius beyond which the shell's AOs are exact zeros) against the tile's
+// points, then writes the AOs of the live shells in the basis order
+// (shell_ao[s] = first AO, AO count), padded with -1 to a multiple of 16.
+// Scratch: dynamic shared memory of 2 * shell_num ints.
+template <int PTS>
+__global__ void __launch_bounds__(256)
+f64_plan_kernel(int64_t P, const double* __restrict__ coord, int64_t cstride, const int* __restrict__ perm,
+                int shell_num, const double4* __restrict__ sph, const int2* __restrict__ shell_ao,
+                int* __restrict__ tlist, int* __restrict__ tcount, int64_t kmax) {
+  __shared__ double spts[3 * PTS];
+  __shared__ int wsum[8];
+  extern __shared__ int sbuf[];   // [shell_num] live AO counts, then [shell_num] list positions
+  int* cnt = sbuf;
+  int* pos = sbuf + shell_num;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t tile = blockIdx.x;
+  const int64_t p0 = tile * PTS;
+  const int np = (int)(P - p0 < PTS ? P - p0 : PTS);
+  for (int t = tid; t < 3 * PTS; t += blockDim.x) {
+    const int d = t / PTS, i = t - d * PTS;
+    spts[t] = i < np ? coord[(int64_t)perm[p0 + i] + d * cstride] : 0.0;
+  }
+  __syncthreads();
+  for (int s = tid; s < shell_num; s += blockDim.x) {
+    const double4 c = sph[s];
+    bool live = false;
+    for (int i = 0; i < np && !live; ++i) {
+      const double x = spts[i] - c.x, y = spts[PTS + i] - c.y, z = spts[2 * PTS + i] - c.z;
+      live = x * x + y * y + z * z <= c.w;
+    }
+    cnt[s] = live ? shell_ao[s].y : 0;
+  }
+  __syncthreads();
+  // exclusive scan of cnt: thread tid owns shells [tid * per, (tid + 1) * per)
+  const int per = (shell_num + 255) / 256;
+  const int s0 = tid * per, s1 = min(shell_num, s0 + per);
+  int local = 0;
+  for (int s = s0; s < s1; ++s) local += cnt[s];
+  int incl = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  int base = 0;
+  for (int w = 0; w < warp; ++w) base += wsum[w];
+  int total = 0;
+  for (int w = 0; w < 8; ++w) total += wsum[w];
+  int run = base + incl - local;
+  for (int s = s0; s < s1; ++s) {
+    pos[s] = run;
+    run += cnt[s];
+  }
+  __syncthreads();
+  int* out = tlist + tile * kmax;
+  for (int s = tid; s < shell_num; s += blockDim.x) {
+    const int n = cnt[s], a0 = shell_ao[s].x, q = pos[s];
+    for (int k = 0; k < n; ++k) out[q + k] = a0 + k;
+  }
+  const int padded = (total + 15) / 16 * 16;
+  for (int q = total + tid; q < padded; q += blockDim.x) out[q] = -1;
+  if (tid == 0) tcount[tile] = padded;
+}
+
 template <int NT, int COMPS>
-cudaError_t run_sparse(int64_t P, int64_t N, const double* ao, int64_t lda, const int* perm, const int* tinfo,
-                       int kblocks, const int* kidx, const double* Bf, int64_t ldb, double* C, int64_t ldc,
+cudaError_t run_sparse(int64_t P, int64_t N, const double* ao, int64_t lda, const int* perm, const int* tlist,
+                       const int* tcount, int64_t kmax, const double* Bt, int64_t ldb, double* C, int64_t ldc,
                        cudaStream_t s) {
   constexpr int BN = 16 * NT;
   constexpr int PTS = BM / COMPS;
@@ -344,7 +413,7 @@ cudaError_t run_sparse(int64_t P, int64_t N, const double* ao, int64_t lda, cons
   if (e != cudaSuccess) return e;
   const int64_t ntiles = (P + PTS - 1) / PTS;
   dim3 grid((unsigned)((N + BN - 1) / BN), (unsigned)std::min<int64_t>(ntiles, 65535));
-  kern<<<grid, 256, smem, s>>>(P, N, ao, lda, perm, tinfo, kblocks, kidx, Bf, ldb, C, ldc, ntiles);
+  kern<<<grid, 256, smem, s>>>(P, N, ao, lda, perm, tlist, tcount, kmax, Bt, ldb, C, ldc, ntiles);
   count_launch();
   return cudaGetLastError();
 }
@@ -384,19 +453,60 @@ cudaError_t launch_gemm_f64_tn_split(int64_t M, int64_t N, int64_t K, const doub
   return run_any<true>(M, N, K, A, lda, B, ldb, part, N, splits, s);
 }
 
+int64_t f64_plan_kmax(int64_t ao_num) { return (ao_num + 15) / 16 * 16; }
+
+size_t f64_plan_bytes(int64_t point_num, int comps, int64_t ao_num) {
+  const int pts = BM / comps;
+  const int64_t tiles = (point_num + pts - 1) / pts;
+  return sizeof(int) * (size_t)tiles * (size_t)(f64_plan_kmax(ao_num) + 1);
+}
+
+cudaError_t launch_f64_plan(int64_t point_num, int comps, const double* coord, int64_t cstride, const int* perm,
+                            int shell_num, const void* sph, const void* shell_ao, int64_t ao_num, void* plan,
+                            cudaStream_t s) {
+  if (point_num <= 0) return cudaSuccess;
+  if (comps != 1 && comps != 5) return cudaErrorInvalidValue;
+  if (cstride < point_num) cstride = point_num;
+  const int pts = BM / comps;
+  const int64_t tiles = (point_num + pts - 1) / pts;
+  const int64_t kmax = f64_plan_kmax(ao_num);
+  int* tcount = (int*)plan;
+  int* tlist = tcount + tiles;
+  const size_t sm = sizeof(int) * 2 * (size_t)shell_num;
+  if (sm > 200 * 1024) return cudaErrorInvalidValue;
+  auto kern5 = f64_plan_kernel<BM / 5>;
+  auto kern1 = f64_plan_kernel<BM>;
+  cudaError_t e = cudaFuncSetAttribute(comps == 5 ? kern5 : kern1, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)std::max<size_t>(sm, 1));
+  if (e != cudaSuccess) return e;
+  if (comps == 5)
+    kern5<<<(unsigned)tiles, 256, sm, s>>>(point_num, coord, cstride, perm, shell_num, (const double4*)sph,
+                                           (const int2*)shell_ao, tlist, tcount, kmax);
+  else
+    kern1<<<(unsigned)tiles, 256, sm, s>>>(point_num, coord, cstride, perm, shell_num, (const double4*)sph,
+                                           (const int2*)shell_ao, tlist, tcount, kmax);
+  count_launch();
+  return cudaGetLastError();
+}
+
 cudaError_t launch_gemm_f64_sparse(int64_t point_num, int comps, int64_t N, const double* ao, int64_t lda,
-                                   const int* perm, const int* tinfo, int kblocks, const int* kidx, const double* Bf,
-                                   int64_t ldb, double* C, int64_t ldc, cudaStream_t s) {
+                                   const int* perm, const void* plan, int64_t ao_num, const double* Bt, int64_t ldb,
+                                   double* C, int64_t ldc, cudaStream_t s) {
   if (point_num <= 0 || N <= 0) return cudaSuccess;
-  if ((ldb & 1) != 0 || (reinterpret_cast<uintptr_t>(Bf) & 15) != 0) return cudaErrorInvalidValue;
+  if ((ldb & 1) != 0 || (reinterpret_cast<uintptr_t>(Bt) & 15) != 0) return cudaErrorInvalidValue;
+  const int pts = BM / comps;
+  const int64_t tiles = (point_num + pts - 1) / pts;
+  const int* tcount = (const int*)plan;
+  const int* tlist = tcount + tiles;
+  const int64_t kmax = f64_plan_kmax(ao_num);
   // the N tile (64 or 80 columns) that wastes fewer padded columns
   const bool nt5 = ((N + 79) / 80) * 80 - N < ((N + 63) / 64) * 64 - N;
   if (comps == 5)
-    return nt5 ? run_sparse<5, 5>(point_num, N, ao, lda, perm, tinfo, kblocks, kidx, Bf, ldb, C, ldc, s)
-               : run_sparse<4, 5>(point_num, N, ao, lda, perm, tinfo, kblocks, kidx, Bf, ldb, C, ldc, s);
+    return nt5 ? run_sparse<5, 5>(point_num, N, ao, lda, perm, tlist, tcount, kmax, Bt, ldb, C, ldc, s)
+               : run_sparse<4, 5>(point_num, N, ao, lda, perm, tlist, tcount, kmax, Bt, ldb, C, ldc, s);
   if (comps == 1)
-    return nt5 ? run_sparse<5, 1>(point_num, N, ao, lda, perm, tinfo, kblocks, kidx, Bf, ldb, C, ldc, s)
-               : run_sparse<4, 1>(point_num, N, ao, lda, perm, tinfo, kblocks, kidx, Bf, ldb, C, ldc, s);
+    return nt5 ? run_sparse<5, 1>(point_num, N, ao, lda, perm, tlist, tcount, kmax, Bt, ldb, C, ldc, s)
+               : run_sparse<4, 1>(point_num, N, ao, lda, perm, tlist, tcount, kmax, Bt, ldb, C, ldc, s);
   return cudaErrorInvalidValue;
 }
 

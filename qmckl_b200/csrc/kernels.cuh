@@ -118,14 +118,20 @@ cudaError_t launch_ao_vgl_split(const DevTables& T, int64_t point_num, const dou
 cudaError_t launch_gemm_f64(int64_t M, int64_t N, int64_t K, const double* A, int64_t lda,
                             const double* B, int64_t ldb, double* C, int64_t ldc, cudaStream_t s);
 
-// Tile-sparse FP64 MO contraction (gemm_f64.cu): out[p][c][n] = sum over the
-// K blocks of each tile's list (tinfo, from the tile plan of the fused
-// kernels; K in their order, kidx[k] = AO at K position k, -1 padding) of
-// ao[p][c][kidx[k]] * Bf[k][n]; points in tiles of 128 / comps in the order
-// perm.  Bf: ldb even and 16-byte aligned.
+// Tile-sparse FP64 MO contraction (gemm_f64.cu).  launch_f64_plan writes,
+// for tiles of 128 / comps points in the order perm, the list of AOs whose
+// shell reaches some point of the tile (basis order; sph[s] = double4 of the
+// shell's nucleus and squared screening radius, shell_ao[s] = int2 first AO
+// and AO count) into plan (f64_plan_bytes); launch_gemm_f64_sparse then
+// computes out[p][c][n] = sum over the tile's list of ao[p][c][k] * Bt[k][n]
+// (Bt: coefficient_t with ldb even and 16-byte aligned rows).
+size_t f64_plan_bytes(int64_t point_num, int comps, int64_t ao_num);
+cudaError_t launch_f64_plan(int64_t point_num, int comps, const double* coord, int64_t cstride, const int* perm,
+                            int shell_num, const void* sph, const void* shell_ao, int64_t ao_num, void* plan,
+                            cudaStream_t s);
 cudaError_t launch_gemm_f64_sparse(int64_t point_num, int comps, int64_t N, const double* ao, int64_t lda,
-                                   const int* perm, const int* tinfo, int kblocks, const int* kidx, const double* Bf,
-                                   int64_t ldb, double* C, int64_t ldc, cudaStream_t s);
+                                   const int* perm, const void* plan, int64_t ao_num, const double* Bt, int64_t ldb,
+                                   double* C, int64_t ldc, cudaStream_t s);
 
 // Split-K FP64 GEMM with A transposed: part[z][m][n] = sum over the z-th K
 // range of A[k][m] * B[k][n] (A element (m, k) at A[k * lda + m]), for

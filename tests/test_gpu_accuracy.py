@@ -26,6 +26,12 @@ pytestmark = pytest.mark.gpu
 
 FP64_TOL = 1e-12
 MIXED_TOL = 1e-6          # max |mixed - fp64| / max |fp64| per component
+# Relative measures the mixed form meets (measured: row-floored <= 4.2e-4,
+# element-wise <= 9e-2 over |ref| > 1e-8 max|ref|, 20.7-23.2 average bits;
+# FP32 AO values and FP32 accumulation bound it, not the 1e-6 target)
+MIXED_ROW_TOL = 1e-3
+MIXED_ELEM_TOL = 0.2
+MIXED_MIN_BITS = 20.0
 
 
 def _oracle_mo(d, pts=None):
@@ -122,30 +128,33 @@ def mixed_cases(chbrclf):
 
 @pytest.mark.parametrize("name", ["chbrclf", "config0", "config1_sub"])
 def test_mixed_error_measures(mixed_cases, name):
-    """All three measures against the oracle, printed for the record
-    (pytest -s); the max-normalised one within 1e-6."""
+    """All three measures against the oracle (printed for the record with
+    pytest -s): the max-normalised one within 1e-6, the row-floored and the
+    element-wise relative errors within the bounds the form meets."""
     ref, mo = mixed_cases[name]
     rep = mixed_error_report(mo, ref)
     print(name, rep)
     assert max(comp_error(mo, ref)) < MIXED_TOL
-    assert max(row_floored_error(mo, ref)) < 1.0
-    assert max(elementwise_rel_error(mo, ref)) < 1e3
+    assert max(row_floored_error(mo, ref)) < MIXED_ROW_TOL
+    assert max(elementwise_rel_error(mo, ref)) < MIXED_ELEM_TOL
 
 
 @pytest.mark.parametrize("name", ["chbrclf", "config0", "config1_sub"])
 def test_mixed_bits_of_agreement(mixed_cases, name):
     """The reference's single-precision acceptance test (org/qmckl_mo.org:3798-3861):
     the average number of bits the reduced-precision MO VGL shares with the
-    FP64 one exceeds 11."""
+    FP64 one exceeds 11; this form keeps at least 20."""
     ref, mo = mixed_cases[name]
     bits = bits_of_agreement(mo, ref)
     print(name, "average bits", bits.mean(), "per component", bits.mean(axis=(0, 2)))
     assert bits.mean() > 11
+    assert bits.mean(axis=(0, 2)).min() >= MIXED_MIN_BITS
 
 
 def test_fp64_tile_sparse_contraction_ragged_and_far(chbrclf):
-    """The FP64 form's tile-sparse contraction (spatial tiles of 25 points, K
-    blocks that vanish over a tile skipped): point counts that end mid-tile,
+    """The FP64 form's tile-sparse contraction (spatial tiles of 25 points,
+    each summing only the AOs of the shells that reach one of its points, in
+    the basis order): point counts that end mid-tile,
     MO VGL and MO value through the device entry points, and points far from
     every nucleus (every block skipped: exact zeros)."""
     import torch
