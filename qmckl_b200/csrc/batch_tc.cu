@@ -262,9 +262,9 @@ batch_mo_kernel(const BatchDesc* __restrict__ desc, const CUtensorMap* __restric
     int* kflag = act + kb_max;
     int* kcnt = kflag + kb_max;
     tile_kblock_flags<kPts>(D.kskip, kblocks, C.pts, (int)(P - p0 < kPts ? P - p0 : kPts), kflag, warp, lane,
-                            NTHREADS / 32);
+                            NTHREADS / 32, true);
     __syncthreads();
-    if (warp == 0) tile_kblock_list(kflag, kblocks, act, kcnt, lane);
+    if (warp == 0) tile_kblock_list(kflag, kblocks, act, kcnt, lane, true);
     __syncthreads();
     const int nact = kcnt[0];
     if (warp < PRODW) {
@@ -275,8 +275,9 @@ batch_mo_kernel(const BatchDesc* __restrict__ desc, const CUtensorMap* __restric
         bool ok = mbar_wait(&C.empty[s], phase ^ 1u, err, 21);
         ok = ok && mbar_wait(&C.rec_full[s], phase, err, 25);
         if (!__all_sync(0xffffffffu, ok)) break;
-        produce_kblock<PIECES, COMPS, CHUNK>(recs + s * rec_max, C.pts, p0, P, D.cutoff, C.rexp,
-                                             smem_addr(smem + s * STAGE), warp, lane);
+        if (kstep_live(act[it], warp, CHUNK))
+          produce_kblock<PIECES, COMPS, CHUNK>(recs + s * rec_max, C.pts, p0, P, D.cutoff, C.rexp,
+                                               smem_addr(smem + s * STAGE), warp, lane);
         fence_async_smem();
         mbar_arrive(&C.full[s]);
       }
@@ -284,7 +285,7 @@ batch_mo_kernel(const BatchDesc* __restrict__ desc, const CUtensorMap* __restric
       if (lane == 0) {
         const CUtensorMap* map = tmaps + sys;
         for (int it = 0; it < nact; ++it) {
-          const int kb = act[it];
+          const int kb = act[it] & 0xFFFF;
           const uint32_t g = kbase + (uint32_t)it;
           const int s = (int)(g & 1u);
           const uint32_t phase = (g >> 1) & 1u;
@@ -299,14 +300,15 @@ batch_mo_kernel(const BatchDesc* __restrict__ desc, const CUtensorMap* __restric
     } else {
       if (lane == 0) {
         const uint32_t idesc = mma_idesc<PIECES>(n_tile);
+        bool init[3] = {false, false, false};   // accumulators written in this item
         for (int it = 0; it < nact; ++it) {
           const uint32_t g = kbase + (uint32_t)it;
           const int s = (int)(g & 1u);
           const uint32_t phase = (g >> 1) & 1u;
           if (!mbar_wait(&C.full[s], phase, err, 23)) break;
           tc_fence_after();
-          mma_kblock<PIECES>(smem_addr(smem + s * STAGE), (uint32_t)(PIECES * A_TILE), (uint32_t)B_TILE, tmem, n_tile,
-                             idesc, act[it], kblocks, kcnt[1], kcnt[2] < 0 ? kblocks : kcnt[2], kcnt[3]);
+          mma_kblock_masked<PIECES>(smem_addr(smem + s * STAGE), (uint32_t)(PIECES * A_TILE), (uint32_t)B_TILE, tmem,
+                                    n_tile, idesc, act[it] & 0xFFFF, kblocks, (uint32_t)act[it] >> 16, init);
           umma_commit(&C.empty[s]);
         }
         umma_commit(&C.acc_full);

@@ -53,7 +53,7 @@ double shell_r2max(const Context* ctx, int s, int n, double cutoff) {
 // vanish (shell_r2max).
 bool build_krec_records(const Context* ctx, std::vector<uint8_t>& h, int& rec_bytes,
                         const std::vector<int32_t>* order, std::vector<int64_t>* ao_perm, std::vector<int2>* kb_sh,
-                        std::vector<double4>* sph, double cutoff) {
+                        std::vector<double4>* sph, double cutoff, std::vector<int2>* kpos = nullptr) {
   const AoBasisRec& B = ctx->ao_basis;
   const AoDerived& d = B.d;
   const int64_t A = B.ao_num, N = ctx->nucleus.num, S = B.shell_num;
@@ -85,11 +85,13 @@ bool build_krec_records(const Context* ctx, std::vector<uint8_t>& h, int& rec_by
   }
   std::vector<int32_t> kq(A);
   std::vector<int64_t> korig(A);
+  if (kpos) kpos->assign(S, make_int2(0, 0));
   {
     int64_t k = 0;
     for (int64_t q = 0; q < S; ++q) {
       const int s = seq[q];
       const int64_t nk = (int64_t)(B.shell_ang_mom[s] + 1) * (B.shell_ang_mom[s] + 2) / 2;
+      if (kpos) (*kpos)[q] = make_int2((int)k, (int)nk);
       for (int64_t t = 0; t < nk; ++t, ++k) {
         if (k >= A) return false;
         kq[k] = (int32_t)q;
@@ -221,21 +223,24 @@ std::vector<int32_t> fused_shell_order(const Context* ctx, double cutoff) {
 // fused_shell_order, or in the basis order when the reordered records would
 // exceed max_rec_bytes (the shared memory they get); kskip is laid out as
 // the kernels read it (int2 per K block, double4 per shell from
-// tc_kskip_bytes - 32 * shell_num on) and ao_perm[k] is the AO at K
-// position k.  False when the AO numbering allows no records.
+// kskip_sph_offset, int2 K position and AO count per shell from
+// kskip_kpos_offset) and ao_perm[k] is the AO at K position k.  False when
+// the AO numbering allows no records.
 bool build_fused_records(const Context* ctx, double cutoff, size_t max_rec_bytes, std::vector<uint8_t>& recs,
                          int& rec_bytes, std::vector<uint8_t>& kskip, std::vector<int64_t>& ao_perm) {
   const int64_t A = ctx->ao_basis.ao_num, S = ctx->ao_basis.shell_num;
-  std::vector<int2> kb_sh;
+  std::vector<int2> kb_sh, kpos;
   std::vector<double4> sph;
   const std::vector<int32_t> order = fused_shell_order(ctx, cutoff);
-  bool ok = build_krec_records(ctx, recs, rec_bytes, &order, &ao_perm, &kb_sh, &sph, cutoff) &&
+  bool ok = build_krec_records(ctx, recs, rec_bytes, &order, &ao_perm, &kb_sh, &sph, cutoff, &kpos) &&
             (size_t)rec_bytes <= max_rec_bytes;
-  if (!ok && !build_krec_records(ctx, recs, rec_bytes, nullptr, &ao_perm, &kb_sh, &sph, cutoff)) return false;
-  const size_t kbytes = tc_kskip_bytes(A, S);
-  kskip.assign(kbytes, 0);
+  if (!ok && !build_krec_records(ctx, recs, rec_bytes, nullptr, &ao_perm, &kb_sh, &sph, cutoff, &kpos)) return false;
+  const int kblocks = (int)((A + 63) / 64);
+  if (kb_sh.empty() || kb_sh.back().y != (int)S) return false;   // the kernels read shell_num there
+  kskip.assign(tc_kskip_bytes(A, S), 0);
   std::memcpy(kskip.data(), kb_sh.data(), sizeof(int2) * kb_sh.size());
-  std::memcpy(kskip.data() + (kbytes - sizeof(double4) * (size_t)S), sph.data(), sizeof(double4) * sph.size());
+  std::memcpy(kskip.data() + fz::kskip_sph_offset(kblocks), sph.data(), sizeof(double4) * sph.size());
+  std::memcpy(kskip.data() + fz::kskip_kpos_offset(kblocks, (int)S), kpos.data(), sizeof(int2) * kpos.size());
   return true;
 }
 

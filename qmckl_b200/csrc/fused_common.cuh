@@ -53,6 +53,13 @@ struct KRecShell {
 // shell's nucleus and the squared radius beyond which its AOs vanish in the
 // producers).
 __host__ __device__ constexpr int kskip_sph_offset(int kblocks) { return (kblocks * 8 + 31) / 32 * 32; }
+// After the spheres: int2 kpos[shell_num], the K position of the first AO of
+// each sphere's shell and its AO count (the 16-AO k-steps a live shell
+// occupies).  shell_num is kb_sh[kblocks - 1].y, the end of the last block's
+// range.
+__host__ __device__ constexpr int kskip_kpos_offset(int kblocks, int shell_num) {
+  return kskip_sph_offset(kblocks) + 32 * shell_num;
+}
 
 constexpr int kRecAoOff = 16;
 constexpr int kRecShellOff = 16 + 64 * 8;
@@ -208,26 +215,41 @@ __device__ __forceinline__ void ao_product(int code, float f, const float (&s)[5
 // memory (one load per lane, no chain of dependent loads).
 template <int PTS>
 __device__ __forceinline__ void tile_kblock_flags(const uint8_t* kskip, int kblocks, const double* pts, int np,
-                                                  int* flags, int warp, int lane, int nwarps) {
+                                                  int* flags, int warp, int lane, int nwarps, bool ksteps = false) {
+  // ksteps: the flag is the mask of the block's 16-AO k-steps that hold an AO
+  // of a live shell (kpos table); otherwise 1 for a live block
   const int2* kb_sh = (const int2*)kskip;
   const double4* sph = kskip ? (const double4*)(kskip + kskip_sph_offset(kblocks)) : nullptr;
+  const int2* kpos = (kskip && ksteps) ? (const int2*)(kskip + kskip_kpos_offset(kblocks, kb_sh[kblocks - 1].y))
+                                       : nullptr;
   for (int kb = warp; kb < kblocks; kb += nwarps) {
-    bool live = kskip == nullptr;
-    if (!live) {
+    unsigned int mask = kskip == nullptr ? 1u : 0u;
+    if (kskip != nullptr) {
       const int2 r = kb_sh[kb];
-      for (int q0 = r.x; q0 < r.y && !live; q0 += 32) {
+      for (int q0 = r.x; q0 < r.y && (kpos != nullptr || mask == 0u); q0 += 32) {
+        const int q = q0 + lane;
         bool l = false;
-        if (q0 + lane < r.y) {
-          const double4 c = sph[q0 + lane];
+        if (q < r.y) {
+          const double4 c = sph[q];
           for (int i = 0; i < np && !l; ++i) {
             const double x = pts[i] - c.x, y = pts[PTS + i] - c.y, z = pts[2 * PTS + i] - c.z;
             l = x * x + y * y + z * z <= c.w;
           }
         }
-        live = __any_sync(0xffffffffu, l);
+        unsigned int m = 0u;
+        if (l) {
+          if (kpos != nullptr) {
+            const int2 kp = kpos[q];
+            const int k0 = max(kp.x, kb * 64) - kb * 64, k1 = min(kp.x + kp.y, kb * 64 + 64) - kb * 64;
+            for (int kk = k0 >> 4; kk <= (k1 - 1) >> 4; ++kk) m |= 1u << kk;
+          } else {
+            m = 1u;
+          }
+        }
+        mask |= __reduce_or_sync(0xffffffffu, m);
       }
     }
-    if (lane == 0) flags[kb] = live ? 1 : 0;
+    if (lane == 0) flags[kb] = (int)mask;
   }
 }
 
@@ -235,7 +257,9 @@ __device__ __forceinline__ void tile_kblock_flags(const uint8_t* kskip, int kblo
 // count, the first block of each half of K (-1: none) and the first block.
 // With no block alive, one (zero) block 0 initialises the accumulators.
 // Returns the count.
-__device__ __forceinline__ int tile_kblock_list(const int* flags, int kblocks, int* act, int* cnt, int lane) {
+// With masks, each entry of act[] is kb | (k-step mask << 16).
+__device__ __forceinline__ int tile_kblock_list(const int* flags, int kblocks, int* act, int* cnt, int lane,
+                                                bool masks = false) {
   int n = 0, lo = -1, hi = -1, first = -1;
   for (int kb0 = 0; kb0 < kblocks; kb0 += 32) {
     const int kb = kb0 + lane;
@@ -243,14 +267,14 @@ __device__ __forceinline__ int tile_kblock_list(const int* flags, int kblocks, i
     const unsigned int m = __ballot_sync(0xffffffffu, f);
     const unsigned int mlo = __ballot_sync(0xffffffffu, f && 2 * kb < kblocks);
     const unsigned int mhi = __ballot_sync(0xffffffffu, f && 2 * kb >= kblocks);
-    if (f) act[n + __popc(m & ((1u << lane) - 1u))] = kb;
+    if (f) act[n + __popc(m & ((1u << lane) - 1u))] = kb | (masks ? (flags[kb] << 16) : 0);
     if (first < 0 && m != 0u) first = kb0 + __ffs(m) - 1;
     if (lo < 0 && mlo != 0u) lo = kb0 + __ffs(mlo) - 1;
     if (hi < 0 && mhi != 0u) hi = kb0 + __ffs(mhi) - 1;
     n += __popc(m);
   }
   if (n == 0) {
-    if (lane == 0) act[0] = 0;
+    if (lane == 0) act[0] = masks ? (0xF << 16) : 0;
     n = 1;
     lo = 0;
     first = 0;
@@ -344,38 +368,48 @@ __device__ __forceinline__ void produce_kblock(const uint8_t* rec, const double*
   }
 }
 
-// The split-BF16 MMA chain of one K block (kb of kblocks) from the stage at
-// shared address `base` (A pieces, then B pieces): leading product into
-// accumulator 0 (first K half) or 1 (second half), corrections into 2.
+// The split-BF16 MMA chain of one K block from the stage at shared address
+// `base` (A pieces, then B pieces): per 16-AO k-step the products of total
+// order <= 2 (corrections into accumulator 2, the leading product A1 B1 last,
+// into accumulator 0 for the first half of the K blocks and 1 for the
+// second, whatever blocks a tile skips, so that a row's sums never depend on
+// the other rows of its tile), with the k-steps that vanish over the tile
+// skipped.  kmask: bit kk
+// set when k-step kk (AOs [16 kk, 16 kk + 16) of the block) holds an AO of a
+// live shell (0: all four); a skipped k-step would add exact zeros, so the
+// sums are those of the full chain.  init[3]: whether accumulator 0 (leading
+// product, first half of K), 1 (leading product, second half) or 2
+// (corrections) holds a sum yet; the first MMA into each overwrites it.
 template <int PIECES>
-__device__ __forceinline__ void mma_kblock(uint32_t base, uint32_t a_bytes, uint32_t b_tile, uint32_t tmem,
-                                           int n_tile, uint32_t idesc, int kb, int kblocks, int first_lo = 0,
-                                           int first_hi = -1, int first_any = 0) {
-  // kb: this K block; the leading product goes to accumulator 0 for the
-  // first half of the K blocks (2 kb < kblocks), to accumulator 1 for the
-  // second half, whatever blocks a tile skips, so that a row's sums never
-  // depend on the other rows of its tile.  first_lo / first_hi / first_any:
-  // the first block of the first half, of the second half and overall that
-  // the tile evaluates (they overwrite instead of accumulating).
-  if (first_hi < 0) first_hi = (kblocks + 1) / 2;
+__device__ __forceinline__ void mma_kblock_masked(uint32_t base, uint32_t a_bytes, uint32_t b_tile, uint32_t tmem,
+                                                  int n_tile, uint32_t idesc, int kb, int kblocks, uint32_t kmask,
+                                                  bool (&init)[3]) {
+  if (kmask == 0u) kmask = 0xFu;
   constexpr int NPROD = PIECES == 3 ? 6 : 3;
   constexpr int pa3[6] = {2, 1, 0, 1, 0, 0}, pb3[6] = {0, 1, 2, 0, 1, 0};
   constexpr int pa2[3] = {1, 0, 0}, pb2[3] = {0, 1, 0};
+  const int li = 2 * kb >= kblocks ? 1 : 0;
   for (int kk = 0; kk < BK / UMMA_K; ++kk) {
+    if (!((kmask >> kk) & 1u)) continue;
 #pragma unroll
     for (int t = 0; t < NPROD; ++t) {
       const int ia = PIECES == 3 ? pa3[t] : pa2[t];
       const int ib = PIECES == 3 ? pb3[t] : pb2[t];
       const uint32_t a_addr = base + ia * A_TILE + kk * UMMA_K * 2;
       const uint32_t b_addr = base + a_bytes + ib * b_tile + kk * UMMA_K * 2;
-      const bool lead = (t == NPROD - 1);
-      const bool second = lead && (2 * kb >= kblocks);
-      const uint32_t d = tmem + (uint32_t)((lead ? (second ? 1 : 0) : 2) * n_tile);
-      const bool first_use = lead ? (second ? (kb == first_hi && kk == 0) : (kb == first_lo && kk == 0))
-                                  : (kb == first_any && kk == 0 && t == 0);
-      umma_bf16(d, smem_desc(a_addr), smem_desc(b_addr), idesc, first_use ? 0u : 1u);
+      const int acc = t == NPROD - 1 ? li : 2;   // the leading product comes last
+      umma_bf16(tmem + (uint32_t)(acc * n_tile), smem_desc(a_addr), smem_desc(b_addr), idesc, init[acc] ? 1u : 0u);
+      init[acc] = true;
     }
   }
+}
+
+// Whether producer warp `warp` (AOs [chunk * warp, chunk * warp + chunk) of
+// a K block) has work in a block whose act[] entry is `entry`: not when
+// its k-step is skipped by the MMAs (its A tile is then never read).
+__device__ __forceinline__ bool kstep_live(int entry, int warp, int chunk) {
+  const uint32_t m = (uint32_t)entry >> 16;
+  return m == 0u || ((m >> ((warp * chunk) >> 4)) & 1u) != 0u;
 }
 
 // Instruction descriptor of tcgen05.mma kind::f16: FP32 accumulator, A and B

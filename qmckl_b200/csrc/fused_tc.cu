@@ -98,7 +98,7 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
       const int* ti = tinfo + (size_t)blockIdx.x * (kblocks + 4);
       const int n = ti[0];
       tma_pre = n < STAGES ? n : STAGES;
-      for (int it = 0; it < tma_pre; ++it) issue_loads(it, ti[4 + it]);
+      for (int it = 0; it < tma_pre; ++it) issue_loads(it, ti[4 + it] & 0xFFFF);
     }
   }
   for (int t = tid; t < 3 * PTS; t += kThreadsF) {
@@ -120,10 +120,11 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
   if (PIECES == 2) row_exponents<PTS>(rb, pts, pidx, rexp, tid, kThreadsF);
   // K blocks that are not identically zero over the tile's points
   if (tinfo == nullptr) {
-    tile_kblock_flags<PTS>(kskip, kblocks, pts, (int)(P - p0 < PTS ? P - p0 : PTS), kflag, warp, lane, kThreadsF / 32);
+    tile_kblock_flags<PTS>(kskip, kblocks, pts, (int)(P - p0 < PTS ? P - p0 : PTS), kflag, warp, lane, kThreadsF / 32,
+                           true);
     __syncthreads();
     if (warp == 0) {
-      const int n = tile_kblock_list(kflag, kblocks, act, nact_p, lane);
+      const int n = tile_kblock_list(kflag, kblocks, act, nact_p, lane, true);
       if (kstat != nullptr && lane == 0) {   // K blocks evaluated / in the dense contraction, summed over CTAs
         atomicAdd(&kstat[0], (unsigned long long)n);
         atomicAdd(&kstat[1], (unsigned long long)kblocks);
@@ -156,7 +157,8 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
       ok = ok && mbar_wait(&rec_full[s], phase, err, 15);
       if (!__all_sync(0xffffffffu, ok)) break;
       const uint32_t a_base = smem_addr(smem + s * STAGE);
-      produce_kblock<PIECES, COMPS, kChunk>(recs + s * rec_bytes, pts, p0, P, cutoff, rexp, a_base, j, lane);
+      if (kstep_live(act[it], j, kChunk))
+        produce_kblock<PIECES, COMPS, kChunk>(recs + s * rec_bytes, pts, p0, P, cutoff, rexp, a_base, j, lane);
       fence_async_smem();
       mbar_arrive(&full[s]);
     }
@@ -167,20 +169,21 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
         const int s = it & 1;
         const uint32_t phase = (uint32_t)(it >> 1) & 1u;
         if (!mbar_wait(&empty[s], phase ^ 1u, err, 12)) break;
-        issue_loads(it, act[it]);
+        issue_loads(it, act[it] & 0xFFFF);
       }
     }
   } else {
     // ---------------- MMA issuer
     if (lane == 0) {
       const uint32_t idesc = mma_idesc<PIECES>(n_tile);
+      bool init[3] = {false, false, false};   // accumulators written so far
       for (int it = 0; it < nact; ++it) {
         const int s = it & 1;
         const uint32_t phase = (uint32_t)(it >> 1) & 1u;
         if (!mbar_wait(&full[s], phase, err, 13)) break;
         tc_fence_after();
-        mma_kblock<PIECES>(smem_addr(smem + s * STAGE), (uint32_t)A_BYTES, (uint32_t)B_TILE, tmem, n_tile, idesc,
-                           act[it], kblocks, nact_p[1], nact_p[2] < 0 ? kblocks : nact_p[2], nact_p[3]);
+        mma_kblock_masked<PIECES>(smem_addr(smem + s * STAGE), (uint32_t)A_BYTES, (uint32_t)B_TILE, tmem, n_tile,
+                                  idesc, act[it] & 0xFFFF, kblocks, (uint32_t)act[it] >> 16, init);
         umma_commit(&empty[s]);
       }
       umma_commit(acc_full);
@@ -257,11 +260,11 @@ tile_plan_kernel(const int64_t P, const double* __restrict__ coord, const int64_
     tpts[tile * 3 * PTS + t] = v;
   }
   __syncthreads();
-  tile_kblock_flags<PTS>(kskip, kblocks, spts, np, sflag, warp, lane, (int)(blockDim.x >> 5));
+  tile_kblock_flags<PTS>(kskip, kblocks, spts, np, sflag, warp, lane, (int)(blockDim.x >> 5), true);
   __syncthreads();
   if (warp != 0) return;
   int* ti = tinfo + tile * (kblocks + 4);
-  const int n = tile_kblock_list(sflag, kblocks, ti + 4, ti, lane);
+  const int n = tile_kblock_list(sflag, kblocks, ti + 4, ti, lane, true);
   for (int t = n + lane; t < kblocks; t += 32) ti[4 + t] = 0;
   if (lane == 0) {
     if (kstat != nullptr) {   // counted per CTA of the fused kernel: once per MO tile
@@ -338,30 +341,9 @@ size_t tc_tile_plan_bytes(const TcPlan& plan, int64_t point_num, int comps) {
   return tile_plan_pts_bytes(tiles, pts) + sizeof(int) * (size_t)tiles * (kb + 4);
 }
 
-cudaError_t tc_launch_tile_plan(int64_t point_num, int comps, int kblocks, const double* coord, int64_t cstride,
-                                const int* perm, const void* kskip, void* tplan, const int** tinfo, cudaStream_t s) {
-  if (comps != 1 && comps != 5) return cudaErrorInvalidValue;
-  const int pts = BM / comps;
-  const int64_t tiles = (point_num + pts - 1) / pts;
-  *tinfo = (const int*)((uint8_t*)tplan + tile_plan_pts_bytes(tiles, pts));
-  if (point_num <= 0) return cudaSuccess;
-  if (cstride < point_num) cstride = point_num;
-  int* ti = (int*)*tinfo;
-  double* tp = (double*)tplan;
-  const size_t sm = sizeof(int) * (size_t)kblocks;
-  if (comps == 5)
-    tile_plan_kernel<BM / 5><<<(unsigned)tiles, 256, sm, s>>>(point_num, coord, cstride, perm, kblocks,
-                                                              (const uint8_t*)kskip, tp, ti, nullptr, 1);
-  else
-    tile_plan_kernel<BM><<<(unsigned)tiles, 256, sm, s>>>(point_num, coord, cstride, perm, kblocks,
-                                                          (const uint8_t*)kskip, tp, ti, nullptr, 1);
-  count_launch();
-  return cudaGetLastError();
-}
-
 size_t tc_kskip_bytes(int64_t ao_num, int64_t shell_num) {
   const int kb = (int)((ao_num + BK - 1) / BK);
-  return (size_t)kskip_sph_offset(kb) + sizeof(double4) * (size_t)shell_num;
+  return (size_t)kskip_kpos_offset(kb, (int)shell_num) + sizeof(int2) * (size_t)shell_num;
 }
 
 cudaError_t tc_encode_coef_map(const TcPlan& plan, const void* d_coef, CUtensorMap* map) {

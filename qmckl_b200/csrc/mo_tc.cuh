@@ -78,11 +78,6 @@ cudaError_t tc_run_fused(const DevTables& T, const TcPlan& plan, int64_t point_n
                          const fz::RowBound& rb, double* out, int* err, cudaStream_t s, int64_t cstride = -1,
                          const void* kskip = nullptr, unsigned long long* kstat = nullptr, void* tplan = nullptr);
 size_t tc_kskip_bytes(int64_t ao_num, int64_t shell_num);
-// The tile plan alone (for the tile-sparse FP64 contraction): tiles of
-// 128 / comps points in the order perm; *tinfo <- the K-block lists inside
-// tplan (tc_tile_plan_bytes of scratch).
-cudaError_t tc_launch_tile_plan(int64_t point_num, int comps, int kblocks, const double* coord, int64_t cstride,
-                                const int* perm, const void* kskip, void* tplan, const int** tinfo, cudaStream_t s);
 size_t tc_tile_plan_bytes(const TcPlan& plan, int64_t point_num, int comps);
 // TMA map of a plan's coefficient pieces (box: 64 AOs x n_tile MOs x 1 piece,
 // 128B swizzle) and a launch of the fused kernel that does not wait for it
