@@ -54,8 +54,15 @@ def load_traffic():
                 continue
             parts = dict(kv.split("=", 1) for kv in line.split() if "=" in kv)
             if "kernel" in parts and "bytes_per_launch" in parts:
-                out[(parts["kernel"], parts.get("form", ""))] = float(parts["bytes_per_launch"])
+                out[(parts["kernel"], parts.get("form", ""))] = (float(parts.get("points", 0)),
+                                                                 float(parts["bytes_per_launch"]))
     return out
+
+
+def _scaled_traffic(kernel, form, P):
+    """Per-launch DRAM bytes of `kernel` at P points, from the capture in profiles/dram_traffic.txt."""
+    cap = load_traffic().get((kernel, form))
+    return cap[1] * P / cap[0] if cap and cap[0] > 0 else None
 
 
 class ClockSampler:
@@ -472,7 +479,7 @@ def main():
         times.append(e0.elapsed_time(e1))
     pq.b200_synchronize(ctx)   # also reports a bounded wait that gave up
     launches = pq.b200_kernel_launch_count() - launches0
-    kb_eval, kb_total = pq.b200_get_kblock_stats(ctx) if fused_path else (0, 0)
+    ks_eval, ks_total = pq.b200_get_kblock_stats(ctx) if fused_path else (0, 0)
     clocks = sampler.stop()
     ms = replicas.max_over_ranks(statistics.mean(times), device="cuda")
 
@@ -500,8 +507,10 @@ def main():
                  "ao_kernel": {"kernel": "ao_f64_kernel<5> (AO VGL, FP64)", "ms_per_launch": ao_ms,
                                "algorithmic_bytes_per_launch": ao_bytes,
                                "achieved_gbs": ao_bytes / (ao_ms * 1e-3) / 1e9,
-                               "hbm_frac": ao_bytes / (ao_ms * 1e-3) / 1e9 / hbm},
+                               "hbm_frac": ao_bytes / (ao_ms * 1e-3) / 1e9 / hbm,
+                               "traffic": _scaled_traffic("ao_f64_kernel", "fp64", P)},
                  "mo_gemm_ms": fp64_ms - ao_ms,
+                 "mo_gemm_traffic": _scaled_traffic("sparse_dgemm_kernel", "fp64", P),
                  "timing": f"CUDA events, median of {n64}, L2 flushed before each step"}
 
     # accuracy of the timed form: against the FP64 form on every point, and
@@ -555,12 +564,15 @@ def main():
         roofline = {"kernel": "ao_f64_kernel<5> (AO VGL, FP64)", "bound": "hbm",
                     "achieved": fp64_form["ao_kernel"]["achieved_gbs"], "peak": hbm, "unit": "GB/s",
                     "frac": fp64_form["ao_kernel"]["hbm_frac"], "peak_source": peak_src,
-                    "traffic": None, "ms_per_launch": ao_ms, "algorithmic_bytes_per_launch": ao_bytes,
-                    "other_kernel": {"kernel": "dgemm_kernel (MO VGL, FP64 mma.sync m8n8k4)",
+                    "traffic": _scaled_traffic("ao_f64_kernel", "fp64", P),
+                    "traffic_note": "ncu capture at fewer points (profiles/dram_traffic.txt) scaled by the point count",
+                    "ms_per_launch": ao_ms, "algorithmic_bytes_per_launch": ao_bytes,
+                    "other_kernel": {"kernel": "f64_plan_kernel + sparse_dgemm_kernel (MO VGL, FP64 mma.sync "
+                                               "m8n8k4 over each tile's live AOs)",
                                      "ms_per_launch": ms - ao_ms,
-                                     "tflops": 2.0 * 5 * P * A * M / ((ms - ao_ms) * 1e-3) / 1e12}}
+                                     "dense_equivalent_tflops": 2.0 * 5 * P * A * M / ((ms - ao_ms) * 1e-3) / 1e12}}
     else:
-        roofline = mixed_roofline(args, P, A, M, ms, kb_eval, kb_total, bf16, peak_src)
+        roofline = mixed_roofline(args, P, A, M, ms, ks_eval, ks_total, bf16, peak_src)
 
     value = world * P / (ms * 1e-3)
     line = {
@@ -595,13 +607,13 @@ def main():
         dist.destroy_process_group()
 
 
-def mixed_roofline(args, P, A, M, ms, kb_eval, kb_total, bf16, peak_src):
+def mixed_roofline(args, P, A, M, ms, ks_eval, ks_total, bf16, peak_src):
     """Roofline of the mixed step's dominant kernel against the bf16 tensor peak.
 
     The fused kernel evaluates 25 points x 5 components per 128-row MMA tile,
-    MOs in N tiles of n_tile columns, 64-AO K blocks (the blocks that vanish
-    over a tile are skipped: the kernel counts the blocks it evaluates);
-    6 split-BF16 products (3 for float16 x 2) per K step.  Reported two ways:
+    MOs in N tiles of n_tile columns, 16-AO k-steps (the k-steps that vanish
+    over a tile are skipped: the kernel counts the k-steps it issues);
+    6 split-BF16 products (3 for float16 x 2) per k-step.  Reported two ways:
     the issued MMA flops and the algorithmic split count (3 x 10 P A M)."""
     flops = 2.0 * 5 * P * A * M
     n_tiles = -(-M // 256)
@@ -610,7 +622,7 @@ def mixed_roofline(args, P, A, M, ms, kb_eval, kb_total, bf16, peak_src):
         n_tiles += 1
         n_tile = -(-(-(-M // n_tiles)) // 16) * 16
     nprod = 6 if args.pieces == 3 else 3
-    issued = 2.0 * (kb_eval / args.steps) * 128 * n_tile * 64 * nprod
+    issued = 2.0 * (ks_eval / args.steps) * 128 * n_tile * 16 * nprod
     kname = ("fused_mo_kernel<3,5> (AO -> split-BF16 tcgen05 MO VGL" if args.pieces == 3 else
              "fused_mo_kernel<2,5> (AO -> split-FP16 tcgen05 MO VGL") + "; step = 3 ordering kernels + tile plan + this)"
     if args.unfused:
@@ -619,17 +631,24 @@ def mixed_roofline(args, P, A, M, ms, kb_eval, kb_total, bf16, peak_src):
         kname = "ao_tile_kernel<3,5> + tc_gemm_kernel<3,2> (unfused mixed form; whole step)"
     split3 = 3.0 * flops
     achieved = issued / (ms * 1e-3) / 1e12
+    traffic, traffic_note = None, "no ncu capture of this kernel in profiles/dram_traffic.txt"
+    cap = load_traffic().get(("fused_mo_kernel", "mixed"))
+    if cap and cap[0] > 0 and not args.unfused and args.pieces == 3:
+        traffic = _scaled_traffic("fused_mo_kernel", "mixed", P)
+        traffic_note = (f"DRAM read + write bytes per launch: ncu capture at {int(cap[0])} points "
+                        f"(profiles/dram_traffic.txt) scaled by the point count; the algorithmic bytes "
+                        f"are the {40.0 * P * M / 1e9:.3f} GB of mo_vgl written + 24 P bytes of coordinates")
     return {"kernel": kname, "bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
             "frac": achieved / bf16, "peak_source": peak_src,
             "achieved_basis": "issued split-BF16 MMA flops per step / step time",
             "split3_count": {"flop_per_step": split3, "tflops": split3 / (ms * 1e-3) / 1e12,
                              "frac": split3 / (ms * 1e-3) / 1e12 / bf16,
                              "note": "3 x 10 P A M: the 3-term split of the dense contraction"},
-            "traffic": None,
-            "traffic_note": "DRAM bytes per launch: profiles/ (ncu capture); the algorithmic bytes are the mo_vgl output",
+            "traffic": traffic,
+            "traffic_note": traffic_note,
             "executed_tensor_flop_per_launch": issued,
             "dense_equivalent_tflops": flops / (ms * 1e-3) / 1e12,
-            "k_blocks_evaluated_fraction": (kb_eval / kb_total) if kb_total else None,
+            "k_steps_issued_fraction": (ks_eval / ks_total) if ks_total else None,
             "output_bytes_per_launch": 40.0 * P * M}
 
 

@@ -175,8 +175,9 @@ qmckl_exit_code qmckl_b200_batch_set_wait_limit(qmckl_b200_batch batch, const in
 qmckl_exit_code qmckl_b200_mo_vgl_device_noalloc(qmckl_context context, const int64_t point_num,
                                                  const double* d_coord, double* d_mo_vgl);
 
-/* Tile skipping of the fused mixed-form kernel: K blocks (64 AOs) it
- * evaluated and K blocks of the dense contraction, summed over its launches
+/* Tile skipping of the fused mixed-form kernel: the 16-AO k-steps (a
+ * quarter of a 64-AO K block) whose MMAs it issued, and the k-steps of the
+ * dense contraction, summed over its launches
  * (one count per CTA: tile of points x MO tile) since the context's first
  * fused evaluation or the last reset (reset != 0 clears them after reading).
  * Both 0 before any fused evaluation.  Synchronizes the context's stream. */

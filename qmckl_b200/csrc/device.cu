@@ -365,7 +365,7 @@ struct DeviceState {
   // fused kernel: K order (AO at each K position; the coefficient pieces of
   // the fused plan follow it), tile-skipping tables, cutoff they were built for
   std::vector<int64_t> fused_perm;
-  DevBuf kskip, kstat;   // kstat: K blocks evaluated / dense, summed over the fused launches
+  DevBuf kskip, kstat;   // kstat: 16-AO k-steps issued / dense, summed over the fused launches
   double krec_cutoff = -1.0;
   // error word of the mixed form's tensor-core kernels: a bounded barrier
   // wait that gives up writes its code here; it is read (and cleared) at the

@@ -223,7 +223,7 @@ __device__ __forceinline__ void tile_kblock_flags(const uint8_t* kskip, int kblo
   const int2* kpos = (kskip && ksteps) ? (const int2*)(kskip + kskip_kpos_offset(kblocks, kb_sh[kblocks - 1].y))
                                        : nullptr;
   for (int kb = warp; kb < kblocks; kb += nwarps) {
-    unsigned int mask = kskip == nullptr ? 1u : 0u;
+    unsigned int mask = kskip == nullptr ? (ksteps ? 0xFu : 1u) : 0u;
     if (kskip != nullptr) {
       const int2 r = kb_sh[kb];
       for (int q0 = r.x; q0 < r.y && (kpos != nullptr || mask == 0u); q0 += 32) {
@@ -251,6 +251,16 @@ __device__ __forceinline__ void tile_kblock_flags(const uint8_t* kskip, int kblo
     }
     if (lane == 0) flags[kb] = (int)mask;
   }
+}
+
+// One warp: the 16-AO k-steps that the MMAs of a tile issue, from the flags
+// of tile_kblock_flags (k-step masks): the sum of their bits, or the four
+// k-steps of the zero block that stands in when no block is alive.
+__device__ __forceinline__ int tile_kstep_count(const int* flags, int kblocks, int lane) {
+  int n = 0;
+  for (int kb = lane; kb < kblocks; kb += 32) n += __popc((unsigned int)flags[kb]);
+  n = __reduce_add_sync(0xffffffffu, n);
+  return n == 0 ? BK / UMMA_K : n;
 }
 
 // One warp: the flagged K blocks in order into act[], and cnt[0..3] = their

@@ -124,10 +124,13 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
                            true);
     __syncthreads();
     if (warp == 0) {
-      const int n = tile_kblock_list(kflag, kblocks, act, nact_p, lane, true);
-      if (kstat != nullptr && lane == 0) {   // K blocks evaluated / in the dense contraction, summed over CTAs
-        atomicAdd(&kstat[0], (unsigned long long)n);
-        atomicAdd(&kstat[1], (unsigned long long)kblocks);
+      tile_kblock_list(kflag, kblocks, act, nact_p, lane, true);
+      if (kstat != nullptr) {   // 16-AO k-steps issued / in the dense contraction, summed over CTAs
+        const int ks = tile_kstep_count(kflag, kblocks, lane);
+        if (lane == 0) {
+          atomicAdd(&kstat[0], (unsigned long long)ks);
+          atomicAdd(&kstat[1], (unsigned long long)kblocks * (BK / UMMA_K));
+        }
       }
     }
   }
@@ -266,10 +269,11 @@ tile_plan_kernel(const int64_t P, const double* __restrict__ coord, const int64_
   int* ti = tinfo + tile * (kblocks + 4);
   const int n = tile_kblock_list(sflag, kblocks, ti + 4, ti, lane, true);
   for (int t = n + lane; t < kblocks; t += 32) ti[4 + t] = 0;
-  if (lane == 0) {
-    if (kstat != nullptr) {   // counted per CTA of the fused kernel: once per MO tile
-      atomicAdd(&kstat[0], (unsigned long long)n * n_tiles);
-      atomicAdd(&kstat[1], (unsigned long long)kblocks * n_tiles);
+  if (kstat != nullptr) {   // counted per CTA of the fused kernel: once per MO tile
+    const int ks = tile_kstep_count(sflag, kblocks, lane);
+    if (lane == 0) {
+      atomicAdd(&kstat[0], (unsigned long long)ks * n_tiles);
+      atomicAdd(&kstat[1], (unsigned long long)kblocks * (BK / UMMA_K) * n_tiles);
     }
   }
 }

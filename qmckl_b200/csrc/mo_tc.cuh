@@ -69,7 +69,7 @@ cudaError_t tc_run(const DevTables& T, const TcPlan& plan, int64_t point_num, in
 // rb: the per-row scale bounds of 2-piece float16 operands (fused_common.cuh).
 // kskip (optional): the tile-skipping tables of the K blocks (fused_tc.cu),
 // tc_kskip_bytes long; kstat (optional): two device counters to which every
-// tile adds its evaluated K blocks and the dense count.  tplan (optional,
+// tile adds the 16-AO k-steps its MMAs issue and the dense count.  tplan (optional,
 // tc_tile_plan_bytes of scratch): a small kernel first gathers each tile's
 // coordinates and finds its K blocks, so that the fused kernel's CTAs start
 // on their pipeline at once (the same blocks, the same results).

@@ -364,7 +364,7 @@ def mo_basis_rescale(ctx, factor):
 
 
 def b200_get_kblock_stats(ctx, reset=False):
-    """(evaluated, total) K blocks of the fused kernel's launches since the last reset."""
+    """(issued, dense) 16-AO k-steps of the fused kernel's launches since the last reset."""
     ev, tot = C.c_int64(0), C.c_int64(0)
     _call("qmckl_b200_get_kblock_stats", ctx, C.byref(ev), C.byref(tot), C.c_int32(1 if reset else 0))
     return ev.value, tot.value

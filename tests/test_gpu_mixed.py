@@ -153,9 +153,9 @@ def test_fused_tile_skipping():
         res[name] = out.cpu().numpy()
         if name == "fused":
             ev, tot = pq.b200_get_kblock_stats(ctx, reset=True)
-            # one count per CTA: ceil(P / 25) tiles x 1 MO tile, 32 K blocks each; the
-            # far points' tiles evaluate one (zero) block
-            assert tot == -(-P // 25) * 32
+            # one count per CTA: ceil(P / 25) tiles x 1 MO tile, 32 K blocks of 4
+            # k-steps each; the far points' tiles issue one (zero) block
+            assert tot == -(-P // 25) * 32 * 4
             assert 0 < ev < tot
             assert pq.b200_get_kblock_stats(ctx) == (0, 0)
         pq.context_destroy(ctx)
