@@ -559,6 +559,25 @@ def main():
         e2e_times.append(e0.elapsed_time(e1))
     pq.context_destroy(ctx_e)
     e2e_ms = replicas.max_over_ranks(statistics.mean(e2e_times), device="cuda")
+    # the floor of the end-to-end step: one plain copy of the same bytes from
+    # the device into the same pinned buffer, and of the coordinates up
+    d_src = torch.empty(P * 5 * M, dtype=torch.float64, device="cuda")
+    d_crd = torch.empty(h_coord.numel(), dtype=torch.float64, device="cuda")
+    copy_times = []
+    for i in range(4):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        with torch.cuda.stream(stream):
+            d_crd.copy_(h_coord, non_blocking=True)
+            h_out.copy_(d_src, non_blocking=True)
+        e1.record(stream)
+        e1.synchronize()
+        if i > 0:
+            copy_times.append(e0.elapsed_time(e1))
+    copy_ms = min(copy_times)
+    del d_src, d_crd
 
     if form == pq.FORM_FP64:
         roofline = {"kernel": "ao_f64_kernel<5> (AO VGL, FP64)", "bound": "hbm",
@@ -584,7 +603,11 @@ def main():
         "form": args.form + (" (unfused)" if args.unfused else ""),
         "e2e": {"value": world * P / (e2e_ms * 1e-3), "unit": "electron-points/s",
                 "h2d_bytes_per_step": int(P * 3 * 8), "d2h_bytes_per_step": int(P * 5 * M * 8),
-                "ms_per_step": e2e_ms},
+                "ms_per_step": e2e_ms,
+                "copy_floor_ms": copy_ms,
+                "copy_floor_gbs": (P * 5 * M * 8 + P * 3 * 8) / (copy_ms * 1e-3) / 1e9,
+                "fraction_of_copy_floor": copy_ms / e2e_ms,
+                "note": "copy floor: the same H2D + D2H bytes as plain pinned copies on the device stream, no compute"},
         "gpu_launches": int(launches),
         "clocks": clocks,
         "roofline": roofline,

@@ -256,12 +256,24 @@ qmckl_exit_code qmckl_set_electron_coord(qmckl_context context, const char trans
   if (elec_num == 0)
     return qmckl_failwith(context, QMCKL_FAILURE, "qmckl_set_electron_coord", "elec_num is not set");
   // Swap the current and previous walker sets (org/qmckl_electron.org:356-366).
+  // The reference then copies the new current set's point record into the
+  // context's (sharing its coordinate array) and overwrites the coordinates;
+  // here the record's count and date are taken over and its buffer swapped
+  // in, so that the coordinates are copied once, not three times.
   std::swap(ctx->electron.walker, ctx->electron.walker_old);
-  ctx->point = ctx->electron.walker.point;
+  PointRec& wp = ctx->electron.walker.point;
+  std::swap(ctx->point.coord, wp.coord);
+  ctx->point.num = wp.num;
+  ctx->point.date = wp.date;
   qmckl_exit_code rc = qmckl_set_point(context, transp, walk_num * elec_num, coord, size_max);
-  if (rc != QMCKL_SUCCESS) return rc;
+  if (rc != QMCKL_SUCCESS) {
+    wp.coord = ctx->point.coord;   // the record keeps its coordinates, as in the reference
+    return rc;
+  }
   ctx->electron.walker.num = walk_num;
-  ctx->electron.walker.point = ctx->point;
+  wp.num = ctx->point.num;
+  wp.date = ctx->point.date;
+  wp.coord.assign(ctx->point.coord.begin(), ctx->point.coord.end());
   if (ctx->electron.walker_old.num == 0)
     return qmckl_set_electron_coord(context, transp, walk_num, coord, size_max);
   return QMCKL_SUCCESS;
