@@ -187,7 +187,9 @@ def run_reference(args):
     P = sysd["elec_coord"].shape[0] * sysd["elec_coord"].shape[1]
     vals = []
     base = None
-    per_step = max(2.0, 20.0 / max(1, args.warmup + args.steps))
+    # each step: up to the whole workload (about 0.8 s on 16 cores), so that
+    # the default 5 + 100 steps end in about three minutes
+    per_step = max(1.0, 20.0 / max(1, args.warmup + args.steps))
     for i in range(args.warmup + args.steps):
         base = cpu_baseline(sysd, seconds=per_step, single_thread_seconds=0.5 if i < args.warmup + args.steps - 1 else 3.0)
         if i >= args.warmup:
