@@ -380,38 +380,58 @@ __device__ __forceinline__ void produce_kblock(const uint8_t* rec, const double*
 
 // The split-BF16 MMA chain of one K block from the stage at shared address
 // `base` (A pieces, then B pieces): per 16-AO k-step the products of total
-// order <= 2 (corrections into accumulator 2, the leading product A1 B1 last,
-// into accumulator 0 for the first half of the K blocks and 1 for the
-// second, whatever blocks a tile skips, so that a row's sums never depend on
-// the other rows of its tile), with the k-steps that vanish over the tile
-// skipped.  kmask: bit kk
-// set when k-step kk (AOs [16 kk, 16 kk + 16) of the block) holds an AO of a
-// live shell (0: all four); a skipped k-step would add exact zeros, so the
-// sums are those of the full chain.  init[3]: whether accumulator 0 (leading
+// order <= 2, the leading product A1 B1 into accumulator 0 for the first
+// half of the K blocks and 1 for the second, whatever blocks a tile skips
+// (so that a row's sums never depend on the other rows of its tile), the
+// corrections into accumulator 2.  The products are issued A piece by A
+// piece, each piece read once into the tensor core's collector buffer and
+// kept for the products that follow with it (3 pieces: A1 B3, A1 B2, A1 B1,
+// A2 B2, A2 B1, A3 B1; 2 pieces: A1 B2, A1 B1, A2 B1), so the MMAs read 12 KB
+// less shared memory per k-step than with A read for every product.  The
+// k-steps that vanish over the tile are skipped.  kmask: bit kk set when
+// k-step kk (AOs [16 kk, 16 kk + 16) of the block) holds an AO of a live
+// shell (0: all four); a skipped k-step would add exact zeros, so the sums
+// are those of the full chain.  init[3]: whether accumulator 0 (leading
 // product, first half of K), 1 (leading product, second half) or 2
 // (corrections) holds a sum yet; the first MMA into each overwrites it.
+// One k-step kk of that chain.
+template <int PIECES>
+__device__ __forceinline__ void mma_kstep(uint32_t base, uint32_t a_bytes, uint32_t b_tile, uint32_t tmem, int n_tile,
+                                          uint32_t idesc, int li, int kk, bool (&init)[3]) {
+  const uint32_t dl = tmem + (uint32_t)(li * n_tile), dc = tmem + (uint32_t)(2 * n_tile);
+  const uint32_t a0 = base + kk * UMMA_K * 2, b0 = base + a_bytes + kk * UMMA_K * 2;
+  const uint64_t A1 = smem_desc(a0), A2 = smem_desc(a0 + A_TILE);
+  const uint64_t B1 = smem_desc(b0), B2 = smem_desc(b0 + b_tile);
+  const uint32_t ic = init[2] ? 1u : 0u, il = init[li] ? 1u : 0u;
+  if constexpr (PIECES == 3) {
+    const uint64_t A3 = smem_desc(a0 + 2 * A_TILE), B3 = smem_desc(b0 + 2 * b_tile);
+    umma_bf16_ca<1>(dc, A1, B3, idesc, ic);
+    umma_bf16_ca<2>(dc, A1, B2, idesc, 1u);
+    umma_bf16_ca<3>(dl, A1, B1, idesc, il);
+    umma_bf16_ca<1>(dc, A2, B2, idesc, 1u);
+    umma_bf16_ca<3>(dc, A2, B1, idesc, 1u);
+    umma_bf16(dc, A3, B1, idesc, 1u);
+  } else {
+    umma_bf16_ca<1>(dc, A1, B2, idesc, ic);
+    umma_bf16_ca<3>(dl, A1, B1, idesc, il);
+    umma_bf16(dc, A2, B1, idesc, 1u);
+  }
+  init[2] = true;
+  init[li] = true;
+}
+
+// Accumulator of the leading product for K block kb: 0 in the first half of
+// the blocks, 1 in the second.
+__device__ __forceinline__ int lead_acc(int kb, int kblocks) { return 2 * kb >= kblocks ? 1 : 0; }
+
 template <int PIECES>
 __device__ __forceinline__ void mma_kblock_masked(uint32_t base, uint32_t a_bytes, uint32_t b_tile, uint32_t tmem,
                                                   int n_tile, uint32_t idesc, int kb, int kblocks, uint32_t kmask,
                                                   bool (&init)[3]) {
   if (kmask == 0u) kmask = 0xFu;
-  constexpr int NPROD = PIECES == 3 ? 6 : 3;
-  constexpr int pa3[6] = {2, 1, 0, 1, 0, 0}, pb3[6] = {0, 1, 2, 0, 1, 0};
-  constexpr int pa2[3] = {1, 0, 0}, pb2[3] = {0, 1, 0};
-  const int li = 2 * kb >= kblocks ? 1 : 0;
-  for (int kk = 0; kk < BK / UMMA_K; ++kk) {
-    if (!((kmask >> kk) & 1u)) continue;
-#pragma unroll
-    for (int t = 0; t < NPROD; ++t) {
-      const int ia = PIECES == 3 ? pa3[t] : pa2[t];
-      const int ib = PIECES == 3 ? pb3[t] : pb2[t];
-      const uint32_t a_addr = base + ia * A_TILE + kk * UMMA_K * 2;
-      const uint32_t b_addr = base + a_bytes + ib * b_tile + kk * UMMA_K * 2;
-      const int acc = t == NPROD - 1 ? li : 2;   // the leading product comes last
-      umma_bf16(tmem + (uint32_t)(acc * n_tile), smem_desc(a_addr), smem_desc(b_addr), idesc, init[acc] ? 1u : 0u);
-      init[acc] = true;
-    }
-  }
+  const int li = lead_acc(kb, kblocks);
+  for (int kk = 0; kk < BK / UMMA_K; ++kk)
+    if ((kmask >> kk) & 1u) mma_kstep<PIECES>(base, a_bytes, b_tile, tmem, n_tile, idesc, li, kk, init);
 }
 
 // Whether producer warp `warp` (AOs [chunk * warp, chunk * warp + chunk) of

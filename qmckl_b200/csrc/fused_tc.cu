@@ -31,6 +31,7 @@ constexpr int kTmaWarp = kProdWarps;
 constexpr int kMmaWarp = kProdWarps + 1;
 constexpr int kThreadsF = (kProdWarps + 2) * 32;
 constexpr int STAGES = 2;
+constexpr int kKsteps = BK / UMMA_K;   // 16-AO k-steps per K block, 4 producer warps each
 
 // Tile skipping: kskip (optional; layout in fused_common.cuh) lists, per K
 // block, the screening spheres of its shells.  A K block whose shells are
@@ -55,8 +56,10 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
   const int A_BYTES = PIECES * A_TILE;
   const int STAGE = PIECES * (A_TILE + B_TILE);
   uint8_t* recs = smem + STAGES * STAGE;      // STAGES K-block records
+  // full[4 s + kk]: k-step kk of stage s produced (the producer warps of its
+  // AOs; for kk = 0 also the coefficient pieces landed)
   uint64_t* full = (uint64_t*)(recs + STAGES * rec_bytes);
-  uint64_t* empty = full + STAGES;
+  uint64_t* empty = full + STAGES * kKsteps;
   uint64_t* rec_full = empty + STAGES;
   uint64_t* acc_full = rec_full + STAGES;
   uint32_t* tmem_slot = (uint32_t*)(acc_full + 1);
@@ -66,6 +69,7 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
   int* act = rexp + 3 * PTS;                  // [kblocks] the K blocks of this tile, [kblocks] flags,
   int* kflag = act + kblocks;                 // then: count, first block of each half, first block
   int* nact_p = kflag + kblocks;
+  int* claim = nact_p + 4;                    // chunks claimed by the producer warps after their first
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int64_t p0 = (int64_t)blockIdx.x * PTS;
@@ -80,13 +84,13 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
     mbar_expect_tx(&rec_full[s], (uint32_t)rec_bytes);
     bulk_load(recs + s * rec_bytes, krec + (size_t)kb * rec_bytes, (uint32_t)rec_bytes, &rec_full[s]);
     uint8_t* st = smem + s * STAGE + A_BYTES;
-    mbar_expect_tx(&full[s], (uint32_t)(PIECES * B_TILE));
-    for (int q = 0; q < PIECES; ++q) tma_load_3d(st + q * B_TILE, &tmB, &full[s], kb * BK, n0, q);
+    mbar_expect_tx(&full[s * kKsteps], (uint32_t)(PIECES * B_TILE));
+    for (int q = 0; q < PIECES; ++q) tma_load_3d(st + q * B_TILE, &tmB, &full[s * kKsteps], kb * BK, n0, q);
   };
   int tma_pre = 0;   // K blocks whose loads the TMA thread issued during the prologue
   if (tid == kTmaWarp * 32) {
     for (int s = 0; s < STAGES; ++s) {
-      mbar_init(&full[s], kProd + 1);
+      for (int kk = 0; kk < kKsteps; ++kk) mbar_init(&full[s * kKsteps + kk], kProd / kKsteps + (kk == 0 ? 1 : 0));
       mbar_init(&empty[s], 1);
       mbar_init(&rec_full[s], 1);
     }
@@ -109,6 +113,7 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
     if (d == 0) pidx[i] = q;
     rexp[t] = PIECES == 2 ? kExpMin : 0;
   }
+  if (tid == 0) *claim = 0;
   if (tinfo != nullptr) {   // the tile's K-block list, made by tile_plan_kernel
     const int* ti = tinfo + (size_t)blockIdx.x * (kblocks + 4);
     for (int t = tid; t < kblocks + 4; t += kThreadsF) {
@@ -149,10 +154,19 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
   const int nact = *nact_p;
 
   if (warp < kProdWarps) {
-    // ---------------- AO producers: warp w owns AOs [4w, 4w+4) of each K block,
-    // its lanes are the tile's points (uniform control flow within the warp)
-    const int j = warp;
-    for (int it = 0; it < nact; ++it) {
+    // ---------------- AO producers.  The work comes in chunks of 4 AOs of a K
+    // block (chunk c: AOs [4c, 4c+4), lanes = the tile's points, so control
+    // flow is uniform within the warp), numbered block by block; each warp
+    // takes the next unclaimed chunk from a shared counter (its first one is
+    // chunk `warp` of the first block).  A warp done early goes on with the
+    // next chunks, into the next block's stage once that stage is free,
+    // instead of waiting for the slowest warp of its block.  Chunks are
+    // claimed in order, so every chunk of a block is taken before any chunk
+    // of a later block: a warp waiting for a stage waits only for blocks
+    // whose chunks are all in progress.
+    const int total = nact * kProdWarps;
+    for (int q = warp; q < total;) {
+      const int it = q / kProdWarps, c = q - it * kProdWarps;
       const int s = it & 1;
       const uint32_t phase = (uint32_t)(it >> 1) & 1u;
       // warp-uniform outcome: every lane must take the same path
@@ -160,10 +174,13 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
       ok = ok && mbar_wait(&rec_full[s], phase, err, 15);
       if (!__all_sync(0xffffffffu, ok)) break;
       const uint32_t a_base = smem_addr(smem + s * STAGE);
-      if (kstep_live(act[it], j, kChunk))
-        produce_kblock<PIECES, COMPS, kChunk>(recs + s * rec_bytes, pts, p0, P, cutoff, rexp, a_base, j, lane);
+      if (kstep_live(act[it], c, kChunk))
+        produce_kblock<PIECES, COMPS, kChunk>(recs + s * rec_bytes, pts, p0, P, cutoff, rexp, a_base, c, lane);
       fence_async_smem();
-      mbar_arrive(&full[s]);
+      mbar_arrive(&full[s * kKsteps + c / (kProdWarps / kKsteps)]);
+      int nq = 0;
+      if (lane == 0) nq = atomicAdd(claim, 1) + kProdWarps;
+      q = __shfl_sync(0xffffffffu, nq, 0);
     }
   } else if (warp == kTmaWarp) {
     // ---------------- coefficient pieces
@@ -183,10 +200,27 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
       for (int it = 0; it < nact; ++it) {
         const int s = it & 1;
         const uint32_t phase = (uint32_t)(it >> 1) & 1u;
-        if (!mbar_wait(&full[s], phase, err, 13)) break;
+        // each k-step's MMAs go out as soon as its four producer warps are done
+        if (!mbar_wait(&full[s * kKsteps], phase, err, 13)) break;
         tc_fence_after();
-        mma_kblock_masked<PIECES>(smem_addr(smem + s * STAGE), (uint32_t)A_BYTES, (uint32_t)B_TILE, tmem, n_tile,
-                                  idesc, act[it] & 0xFFFF, kblocks, (uint32_t)act[it] >> 16, init);
+        const int kb = act[it] & 0xFFFF;
+        uint32_t kmask = (uint32_t)act[it] >> 16;
+        if (kmask == 0u) kmask = 0xFu;
+        const int li = lead_acc(kb, kblocks);
+        bool ok = true;
+        for (int kk = 0; kk < kKsteps; ++kk) {
+          if (!((kmask >> kk) & 1u)) continue;
+          if (kk > 0) {
+            if (!mbar_wait(&full[s * kKsteps + kk], phase, err, 13)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+          }
+          mma_kstep<PIECES>(smem_addr(smem + s * STAGE), (uint32_t)A_BYTES, (uint32_t)B_TILE, tmem, n_tile, idesc, li,
+                            kk, init);
+        }
+        if (!ok) break;
         umma_commit(&empty[s]);
       }
       umma_commit(acc_full);
@@ -296,8 +330,9 @@ template <int PIECES, int COMPS>
 size_t fused_smem(int n_tile, int rec_bytes, int kblocks) {
   constexpr int PTS = BM / COMPS;
   const size_t stage = (size_t)PIECES * (A_TILE + (size_t)n_tile * BK * 2);
-  return 1024 + STAGES * stage + (size_t)STAGES * rec_bytes + (3 * STAGES + 2) * 8 + 4 * PTS * 8 + 3 * PTS * 4 +
-         (size_t)(2 * kblocks + 4) * 4 + 16;
+  return 1024 + STAGES * stage + (size_t)STAGES * rec_bytes + ((kKsteps + 2) * STAGES + 2) * 8 + 4 * PTS * 8 +
+         3 * PTS * 4 +
+         (size_t)(2 * kblocks + 5) * 4 + 16;
 }
 
 template <int PIECES, int COMPS>
