@@ -56,10 +56,14 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
   const int A_BYTES = PIECES * A_TILE;
   const int STAGE = PIECES * (A_TILE + B_TILE);
   uint8_t* recs = smem + STAGES * STAGE;      // STAGES K-block records
-  // full[4 s + kk]: k-step kk of stage s produced (the producer warps of its
-  // AOs; for kk = 0 also the coefficient pieces landed)
+  // Barriers: full[4 s + kk], k-step kk of the block in stage s produced (its
+  // four chunks, or the MMA thread in their place when the k-step is
+  // skipped); bfull[s], the block's coefficient pieces landed; empty[s], all
+  // the block's MMAs done (the stage and its record slot free); rec_full[s],
+  // its record landed.
   uint64_t* full = (uint64_t*)(recs + STAGES * rec_bytes);
-  uint64_t* empty = full + STAGES * kKsteps;
+  uint64_t* bfull = full + STAGES * kKsteps;
+  uint64_t* empty = bfull + STAGES;
   uint64_t* rec_full = empty + STAGES;
   uint64_t* acc_full = rec_full + STAGES;
   uint32_t* tmem_slot = (uint32_t*)(acc_full + 1);
@@ -79,18 +83,22 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
 
   // loads of K block kb (the it-th of the tile) into stage it % STAGES: the
   // block's record and its coefficient pieces
-  auto issue_loads = [&](int it, int kb) {
+  auto load_record = [&](int it, int kb) {
     const int s = it & 1;
     mbar_expect_tx(&rec_full[s], (uint32_t)rec_bytes);
     bulk_load(recs + s * rec_bytes, krec + (size_t)kb * rec_bytes, (uint32_t)rec_bytes, &rec_full[s]);
+  };
+  auto load_coef = [&](int it, int kb) {
+    const int s = it & 1;
     uint8_t* st = smem + s * STAGE + A_BYTES;
-    mbar_expect_tx(&full[s * kKsteps], (uint32_t)(PIECES * B_TILE));
-    for (int q = 0; q < PIECES; ++q) tma_load_3d(st + q * B_TILE, &tmB, &full[s * kKsteps], kb * BK, n0, q);
+    mbar_expect_tx(&bfull[s], (uint32_t)(PIECES * B_TILE));
+    for (int q = 0; q < PIECES; ++q) tma_load_3d(st + q * B_TILE, &tmB, &bfull[s], kb * BK, n0, q);
   };
   int tma_pre = 0;   // K blocks whose loads the TMA thread issued during the prologue
   if (tid == kTmaWarp * 32) {
     for (int s = 0; s < STAGES; ++s) {
-      for (int kk = 0; kk < kKsteps; ++kk) mbar_init(&full[s * kKsteps + kk], kProd / kKsteps + (kk == 0 ? 1 : 0));
+      for (int kk = 0; kk < kKsteps; ++kk) mbar_init(&full[s * kKsteps + kk], kProd / kKsteps);
+      mbar_init(&bfull[s], 1);
       mbar_init(&empty[s], 1);
       mbar_init(&rec_full[s], 1);
     }
@@ -102,7 +110,10 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
       const int* ti = tinfo + (size_t)blockIdx.x * (kblocks + 4);
       const int n = ti[0];
       tma_pre = n < STAGES ? n : STAGES;
-      for (int it = 0; it < tma_pre; ++it) issue_loads(it, ti[4 + it] & 0xFFFF);
+      for (int it = 0; it < tma_pre; ++it) {
+        load_record(it, ti[4 + it] & 0xFFFF);
+        load_coef(it, ti[4 + it] & 0xFFFF);
+      }
     }
   }
   for (int t = tid; t < 3 * PTS; t += kThreadsF) {
@@ -164,20 +175,32 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
     // claimed in order, so every chunk of a block is taken before any chunk
     // of a later block: a warp waiting for a stage waits only for blocks
     // whose chunks are all in progress.
+    // A chunk of a skipped k-step is never read by the MMAs: it waits for
+    // the stage only (so that every chunk of a block waits for the same
+    // barrier, which keeps any warp from claiming a chunk two blocks past a
+    // stage still in use) and does not arrive; the MMA thread arrives for
+    // the whole skipped k-step.
     const int total = nact * kProdWarps;
     for (int q = warp; q < total;) {
       const int it = q / kProdWarps, c = q - it * kProdWarps;
       const int s = it & 1;
       const uint32_t phase = (uint32_t)(it >> 1) & 1u;
-      // warp-uniform outcome: every lane must take the same path
+      const bool live = kstep_live(act[it], c, kChunk);
+      // warp-uniform outcome: every lane must take the same path.  A
+      // produced chunk also waits for the block's record.  Its arrival comes
+      // after the stage's release, that is after the MMA thread has waited
+      // for the same full[] barrier's phase of the block two back, so no
+      // phase of a barrier mixes the arrivals of two blocks and no parity
+      // wait falls two phases behind.
       bool ok = mbar_wait(&empty[s], phase ^ 1u, err, 11);
-      ok = ok && mbar_wait(&rec_full[s], phase, err, 15);
+      if (live) ok = ok && mbar_wait(&rec_full[s], phase, err, 15);
       if (!__all_sync(0xffffffffu, ok)) break;
-      const uint32_t a_base = smem_addr(smem + s * STAGE);
-      if (kstep_live(act[it], c, kChunk))
+      if (live) {
+        const uint32_t a_base = smem_addr(smem + s * STAGE);
         produce_kblock<PIECES, COMPS, kChunk>(recs + s * rec_bytes, pts, p0, P, cutoff, rexp, a_base, c, lane);
-      fence_async_smem();
-      mbar_arrive(&full[s * kKsteps + c / (kProdWarps / kKsteps)]);
+        fence_async_smem();
+        mbar_arrive(&full[s * kKsteps + c / (kProdWarps / kKsteps)]);
+      }
       int nq = 0;
       if (lane == 0) nq = atomicAdd(claim, 1) + kProdWarps;
       q = __shfl_sync(0xffffffffu, nq, 0);
@@ -188,8 +211,10 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
       for (int it = tma_pre; it < nact; ++it) {
         const int s = it & 1;
         const uint32_t phase = (uint32_t)(it >> 1) & 1u;
+        // the stage, its record slot included: every MMA of block it - 2 done
         if (!mbar_wait(&empty[s], phase ^ 1u, err, 12)) break;
-        issue_loads(it, act[it] & 0xFFFF);
+        load_record(it, act[it] & 0xFFFF);
+        load_coef(it, act[it] & 0xFFFF);
       }
     }
   } else {
@@ -200,23 +225,24 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
       for (int it = 0; it < nact; ++it) {
         const int s = it & 1;
         const uint32_t phase = (uint32_t)(it >> 1) & 1u;
-        // each k-step's MMAs go out as soon as its four producer warps are done
-        if (!mbar_wait(&full[s * kKsteps], phase, err, 13)) break;
-        tc_fence_after();
+        // each k-step's MMAs go out as soon as its four chunks are produced;
+        // for a skipped k-step this thread arrives in place of its chunks
+        // (it waited for that barrier's phase of the block two back itself)
+        if (!mbar_wait(&bfull[s], phase, err, 13)) break;
         const int kb = act[it] & 0xFFFF;
         uint32_t kmask = (uint32_t)act[it] >> 16;
         if (kmask == 0u) kmask = 0xFu;
         const int li = lead_acc(kb, kblocks);
         bool ok = true;
         for (int kk = 0; kk < kKsteps; ++kk) {
-          if (!((kmask >> kk) & 1u)) continue;
-          if (kk > 0) {
-            if (!mbar_wait(&full[s * kKsteps + kk], phase, err, 13)) {
-              ok = false;
-              break;
-            }
-            tc_fence_after();
+          const bool kl = ((kmask >> kk) & 1u) != 0u;
+          if (!kl) mbar_arrive_n(&full[s * kKsteps + kk], (uint32_t)(kProd / kKsteps));
+          if (!mbar_wait(&full[s * kKsteps + kk], phase, err, 13)) {
+            ok = false;
+            break;
           }
+          if (!kl) continue;
+          tc_fence_after();
           mma_kstep<PIECES>(smem_addr(smem + s * STAGE), (uint32_t)A_BYTES, (uint32_t)B_TILE, tmem, n_tile, idesc, li,
                             kk, init);
         }
@@ -330,7 +356,7 @@ template <int PIECES, int COMPS>
 size_t fused_smem(int n_tile, int rec_bytes, int kblocks) {
   constexpr int PTS = BM / COMPS;
   const size_t stage = (size_t)PIECES * (A_TILE + (size_t)n_tile * BK * 2);
-  return 1024 + STAGES * stage + (size_t)STAGES * rec_bytes + ((kKsteps + 2) * STAGES + 2) * 8 + 4 * PTS * 8 +
+  return 1024 + STAGES * stage + (size_t)STAGES * rec_bytes + ((kKsteps + 3) * STAGES + 2) * 8 + 4 * PTS * 8 +
          3 * PTS * 4 +
          (size_t)(2 * kblocks + 5) * 4 + 16;
 }
