@@ -752,7 +752,7 @@ qmckl_exit_code prepare_korder(qmckl_context context, DeviceState* ds, bool* ok)
   *ok = false;
   const int64_t A = ctx->ao_basis.ao_num, M = ctx->mo_basis.mo_num;
   const double cutoff = cutoff_of(ctx);
-  const TcPlan plan = tc_plan(A, M, ds->split_pieces);
+  const TcPlan plan = tc_plan_fused(A, M, ds->split_pieces);
   // the VGL kernel decides the order; the value kernel (128-point tiles) may
   // still not fit, which run_mo_mixed checks per call
   auto fits = [&](int rec) { return tc_fused_smem(plan, 5, rec) <= 232448; };
@@ -799,7 +799,7 @@ qmckl_exit_code prepare_fused(qmckl_context context, DeviceState* ds, bool* usab
   *usable = false;
   const int64_t A = ctx->ao_basis.ao_num, M = ctx->mo_basis.mo_num;
   const int pieces = ds->split_pieces;
-  const TcPlan plan = tc_plan(A, M, pieces);
+  const TcPlan plan = tc_plan_fused(A, M, pieces);
   bool ok = false;
   qmckl_exit_code rc0 = prepare_korder(context, ds, &ok);
   if (rc0 != QMCKL_SUCCESS || !ok) return rc0;
@@ -809,7 +809,8 @@ qmckl_exit_code prepare_fused(qmckl_context context, DeviceState* ds, bool* usab
     if (rc != QMCKL_SUCCESS) return rc;
     QB_CUDA(cudaMemsetAsync(ds->kstat.p, 0, 2 * sizeof(unsigned long long), ds->stream), fname);
   }
-  if (ds->tc_coef_version != ctx->mo_basis.coef_version || ds->tc_pieces != pieces || !ds->tc_coef.p) {
+  if (ds->tc_coef_version != ctx->mo_basis.coef_version || ds->tc_pieces != pieces || !ds->tc_coef.p ||
+      ds->tc.n_tile != plan.n_tile || ds->tc.nacc != plan.nacc) {
     // coefficient columns in the K order of the records
     std::vector<double> cp((size_t)(M * A));
     const std::vector<double>& c = ctx->mo_basis.coefficient;

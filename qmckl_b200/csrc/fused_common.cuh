@@ -394,15 +394,18 @@ __device__ __forceinline__ void produce_kblock(const uint8_t* rec, const double*
 // are those of the full chain.  init[3]: whether accumulator 0 (leading
 // product, first half of K), 1 (leading product, second half) or 2
 // (corrections) holds a sum yet; the first MMA into each overwrites it.
-// One k-step kk of that chain.
-template <int PIECES>
+// One k-step kk of that chain.  NACC = 3: the accumulators above; NACC = 2
+// (wide MO tiles): the leading product in accumulator 0 for all of K, the
+// corrections in accumulator 1 (li must be 0).
+template <int PIECES, int NACC = 3>
 __device__ __forceinline__ void mma_kstep(uint32_t base, uint32_t a_bytes, uint32_t b_tile, uint32_t tmem, int n_tile,
                                           uint32_t idesc, int li, int kk, bool (&init)[3]) {
-  const uint32_t dl = tmem + (uint32_t)(li * n_tile), dc = tmem + (uint32_t)(2 * n_tile);
+  static_assert(NACC == 2 || NACC == 3, "two or three accumulators");
+  const uint32_t dl = tmem + (uint32_t)(li * n_tile), dc = tmem + (uint32_t)((NACC - 1) * n_tile);
   const uint32_t a0 = base + kk * UMMA_K * 2, b0 = base + a_bytes + kk * UMMA_K * 2;
   const uint64_t A1 = smem_desc(a0), A2 = smem_desc(a0 + A_TILE);
   const uint64_t B1 = smem_desc(b0), B2 = smem_desc(b0 + b_tile);
-  const uint32_t ic = init[2] ? 1u : 0u, il = init[li] ? 1u : 0u;
+  const uint32_t ic = init[NACC - 1] ? 1u : 0u, il = init[li] ? 1u : 0u;
   if constexpr (PIECES == 3) {
     const uint64_t A3 = smem_desc(a0 + 2 * A_TILE), B3 = smem_desc(b0 + 2 * b_tile);
     umma_bf16_ca<1>(dc, A1, B3, idesc, ic);
@@ -416,7 +419,7 @@ __device__ __forceinline__ void mma_kstep(uint32_t base, uint32_t a_bytes, uint3
     umma_bf16_ca<3>(dl, A1, B1, idesc, il);
     umma_bf16(dc, A2, B1, idesc, 1u);
   }
-  init[2] = true;
+  init[NACC - 1] = true;
   init[li] = true;
 }
 
@@ -456,7 +459,7 @@ __device__ __forceinline__ uint32_t mma_idesc(int n_tile) {
 // (tile point i, component c) written to out[(pidx[i] * COMPS + c) * n_out +
 // col] for the MO columns [n0, n0 + n_tile).
 // stage: 32 x 16 doubles of shared scratch for this warp.
-template <int PIECES, int COMPS>
+template <int PIECES, int COMPS, int NACC = 3>
 __device__ __forceinline__ void epilogue_warp(uint32_t tmem, int n_tile, int n0, int n_out, bool has_second,
                                               const int64_t* pidx, const int* rexp, const double* scales,
                                               double* out, double* stage, int warp, int lane, int chunk0 = 0,
@@ -468,12 +471,17 @@ __device__ __forceinline__ void epilogue_warp(uint32_t tmem, int n_tile, int n0,
     const uint32_t ta = tmem + ((uint32_t)row_base << 16) + (uint32_t)c0;
     tmem_ld16(ta, r0);
     tmem_ld16(ta + (uint32_t)n_tile, r1);
-    tmem_ld16(ta + (uint32_t)(2 * n_tile), r2);
+    if (NACC == 3) tmem_ld16(ta + (uint32_t)(2 * n_tile), r2);
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
-      double v = has_first ? (double)__uint_as_float(r0[j]) + (double)__uint_as_float(r2[j])
-                           : (double)__uint_as_float(r2[j]);
-      if (has_second) v += (double)__uint_as_float(r1[j]);
+      double v;
+      if (NACC == 2) {   // leading product + corrections
+        v = (double)__uint_as_float(r0[j]) + (double)__uint_as_float(r1[j]);
+      } else {
+        v = has_first ? (double)__uint_as_float(r0[j]) + (double)__uint_as_float(r2[j])
+                      : (double)__uint_as_float(r2[j]);
+        if (has_second) v += (double)__uint_as_float(r1[j]);
+      }
       stage[lane * 16 + ((j + lane) & 15)] = v;
     }
     __syncwarp();
@@ -502,31 +510,40 @@ __device__ __forceinline__ void epilogue_warp(uint32_t tmem, int n_tile, int n0,
 // the tile goes to stg + r * ldst in the same arithmetic.  ldst = n_tile + 2
 // puts the 16-byte stores of a warp's 32 rows on 8 distinct bank groups.  The
 // caller copies each row to its place in global memory with one bulk copy.
-template <int PIECES, int COMPS>
+// Only the columns [col_lo, col_hi) of the tile (multiples of 16; column
+// col_lo lands at stg + r * ldst), so that a wide tile can go out in passes.
+template <int PIECES, int COMPS, int NACC = 3>
 __device__ __forceinline__ void epilogue_stage_warp(uint32_t tmem, int n_tile, int n0, int n_out, bool has_second,
                                                     const int* rexp, const double* scales, double* stg, int ldst,
-                                                    int warp, int lane, int chunk0, int chunk_step, bool has_first) {
+                                                    int warp, int lane, int chunk0, int chunk_step, bool has_first,
+                                                    int col_lo = 0, int col_hi = 1 << 30) {
   constexpr int PTS = BM / COMPS;
   const int row_base = (warp & 3) * 32;
   const int r = row_base + lane;
   const bool row_ok = r < PTS * COMPS;
   const double rs = (PIECES == 2 && row_ok) ? pow2d(rexp[comp_group<COMPS>(r % COMPS) * PTS + r / COMPS]) : 1.0;
-  for (int c0 = 16 * chunk0; c0 < n_tile; c0 += 16 * chunk_step) {
+  const int c_end = min(n_tile, col_hi);
+  for (int c0 = col_lo + 16 * chunk0; c0 < c_end; c0 += 16 * chunk_step) {
     uint32_t r0[16], r1[16], r2[16];
     const uint32_t ta = tmem + ((uint32_t)row_base << 16) + (uint32_t)c0;
     tmem_ld16(ta, r0);
     tmem_ld16(ta + (uint32_t)n_tile, r1);
-    tmem_ld16(ta + (uint32_t)(2 * n_tile), r2);
+    if (NACC == 3) tmem_ld16(ta + (uint32_t)(2 * n_tile), r2);
     if (row_ok) {
-      double* dst = stg + (size_t)r * ldst + c0;
+      double* dst = stg + (size_t)r * ldst + (c0 - col_lo);
 #pragma unroll
       for (int j = 0; j < 16; j += 2) {
         double v[2];
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-          double x = has_first ? (double)__uint_as_float(r0[j + h]) + (double)__uint_as_float(r2[j + h])
-                               : (double)__uint_as_float(r2[j + h]);
-          if (has_second) x += (double)__uint_as_float(r1[j + h]);
+          double x;
+          if (NACC == 2) {   // leading product + corrections
+            x = (double)__uint_as_float(r0[j + h]) + (double)__uint_as_float(r1[j + h]);
+          } else {
+            x = has_first ? (double)__uint_as_float(r0[j + h]) + (double)__uint_as_float(r2[j + h])
+                          : (double)__uint_as_float(r2[j + h]);
+            if (has_second) x += (double)__uint_as_float(r1[j + h]);
+          }
           if (PIECES == 2) {
             const int col = n0 + c0 + j + h;
             x *= (col < n_out ? scales[kScaleCols + col] : 1.0) * rs;

@@ -38,7 +38,14 @@ constexpr int kKsteps = BK / UMMA_K;   // 16-AO k-steps per K block, 4 producer 
 // all beyond their radius at every point of the tile contributes exact zeros
 // and is left out of the producer, TMA and MMA loops.
 
-template <int PIECES, int COMPS>
+// NACC = 3: three accumulators of n_tile <= 160 columns (the leading
+// product in two halves of K, the corrections), each stage holding its A
+// and coefficient tiles.  NACC = 2 (wide MO tiles, n_tile <= 256, with a tile
+// plan only): the leading product in one accumulator, the corrections in the
+// other, and a single coefficient tile after the two A stages, loaded for
+// block it once the MMAs of block it - 1 are done; the epilogue then writes
+// the tile in column passes that fit the idle stage memory.
+template <int PIECES, int COMPS, int NACC>
 __global__ void __launch_bounds__(kThreadsF, 1)
 fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, const int64_t P,
                 const double* __restrict__ coord, const double cutoff, const int n_out, const int n_tile,
@@ -54,8 +61,11 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
   uint8_t* smem = smem_raw + ((1024u - (tcx::smem_addr(smem_raw) & 1023u)) & 1023u);
   const int B_TILE = n_tile * BK * 2;
   const int A_BYTES = PIECES * A_TILE;
-  const int STAGE = PIECES * (A_TILE + B_TILE);
-  uint8_t* recs = smem + STAGES * STAGE;      // STAGES K-block records
+  const int STAGE = NACC == 3 ? PIECES * (A_TILE + B_TILE) : A_BYTES;
+  // offset of the coefficient tile from the start of stage s
+  auto b_off = [&](int s) { return NACC == 3 ? A_BYTES : (STAGES - s) * STAGE; };
+  const int STAGE_MEM = STAGES * STAGE + (NACC == 3 ? 0 : PIECES * B_TILE);
+  uint8_t* recs = smem + STAGE_MEM;           // STAGES K-block records
   // Barriers: full[4 s + kk], k-step kk of the block in stage s produced (its
   // four chunks, or the MMA thread in their place when the k-step is
   // skipped); bfull[s], the block's coefficient pieces landed; empty[s], all
@@ -79,7 +89,7 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
   const int64_t p0 = (int64_t)blockIdx.x * PTS;
   const int n0 = blockIdx.y * n_tile;
   uint32_t tmem_cols = 32;
-  while ((int)tmem_cols < 3 * n_tile) tmem_cols <<= 1;
+  while ((int)tmem_cols < NACC * n_tile) tmem_cols <<= 1;
 
   // loads of K block kb (the it-th of the tile) into stage it % STAGES: the
   // block's record and its coefficient pieces
@@ -90,7 +100,7 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
   };
   auto load_coef = [&](int it, int kb) {
     const int s = it & 1;
-    uint8_t* st = smem + s * STAGE + A_BYTES;
+    uint8_t* st = smem + s * STAGE + b_off(s);
     mbar_expect_tx(&bfull[s], (uint32_t)(PIECES * B_TILE));
     for (int q = 0; q < PIECES; ++q) tma_load_3d(st + q * B_TILE, &tmB, &bfull[s], kb * BK, n0, q);
   };
@@ -112,7 +122,7 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
       tma_pre = n < STAGES ? n : STAGES;
       for (int it = 0; it < tma_pre; ++it) {
         load_record(it, ti[4 + it] & 0xFFFF);
-        load_coef(it, ti[4 + it] & 0xFFFF);
+        if (NACC == 3 || it == 0) load_coef(it, ti[4 + it] & 0xFFFF);   // one coefficient tile (NACC 2)
       }
     }
   }
@@ -206,15 +216,28 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
       q = __shfl_sync(0xffffffffu, nq, 0);
     }
   } else if (warp == kTmaWarp) {
-    // ---------------- coefficient pieces
+    // ---------------- records and coefficient pieces
     if (lane == 0) {
-      for (int it = tma_pre; it < nact; ++it) {
-        const int s = it & 1;
-        const uint32_t phase = (uint32_t)(it >> 1) & 1u;
-        // the stage, its record slot included: every MMA of block it - 2 done
-        if (!mbar_wait(&empty[s], phase ^ 1u, err, 12)) break;
-        load_record(it, act[it] & 0xFFFF);
-        load_coef(it, act[it] & 0xFFFF);
+      if (NACC == 3) {
+        for (int it = tma_pre; it < nact; ++it) {
+          const int s = it & 1;
+          const uint32_t phase = (uint32_t)(it >> 1) & 1u;
+          // the stage, its record slot included: every MMA of block it - 2 done
+          if (!mbar_wait(&empty[s], phase ^ 1u, err, 12)) break;
+          load_record(it, act[it] & 0xFFFF);
+          load_coef(it, act[it] & 0xFFFF);
+        }
+      } else {
+        // the single coefficient tile of block it once the MMAs of block
+        // it - 1 are done; then the record of block it + 1, whose slot (block
+        // it - 1's) is free by the same wait (the prologue loaded records 0
+        // and 1 and the coefficients of block 0)
+        for (int it = 1; it < nact; ++it) {
+          const int b = it - 1;
+          if (!mbar_wait(&empty[b & 1], (uint32_t)(b >> 1) & 1u, err, 12)) break;
+          load_coef(it, act[it] & 0xFFFF);
+          if (it + 1 < nact && it + 1 >= tma_pre) load_record(it + 1, act[it + 1] & 0xFFFF);
+        }
       }
     }
   } else {
@@ -232,7 +255,7 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
         const int kb = act[it] & 0xFFFF;
         uint32_t kmask = (uint32_t)act[it] >> 16;
         if (kmask == 0u) kmask = 0xFu;
-        const int li = lead_acc(kb, kblocks);
+        const int li = NACC == 3 ? lead_acc(kb, kblocks) : 0;
         bool ok = true;
         for (int kk = 0; kk < kKsteps; ++kk) {
           const bool kl = ((kmask >> kk) & 1u) != 0u;
@@ -243,8 +266,8 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
           }
           if (!kl) continue;
           tc_fence_after();
-          mma_kstep<PIECES>(smem_addr(smem + s * STAGE), (uint32_t)A_BYTES, (uint32_t)B_TILE, tmem, n_tile, idesc, li,
-                            kk, init);
+          mma_kstep<PIECES, NACC>(smem_addr(smem + s * STAGE), (uint32_t)b_off(s), (uint32_t)B_TILE, tmem, n_tile,
+                                  idesc, li, kk, init);
         }
         if (!ok) break;
         umma_commit(&empty[s]);
@@ -263,14 +286,23 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
     bool ok = mbar_wait(acc_full, 0, err, 14);
     ok = __all_sync(0xffffffffu, ok && *(volatile int*)err == 0);
     tc_fence_after();
-    const int ldst = n_tile + 2;
-    const bool bulk = (size_t)BM * ldst * sizeof(double) <= (size_t)STAGES * STAGE && (n_out & 1) == 0 &&
+    // the tile goes out in column passes of `pw` columns (a multiple of 16),
+    // as few as the idle stage memory allows (one for NACC = 3)
+    int npass = 1, pw = n_tile;
+    if constexpr (NACC == 2) {
+      const int max_pw = ((int)(STAGE_MEM / (BM * sizeof(double))) - 2) / 16 * 16;
+      npass = max_pw >= 16 ? (n_tile + max_pw - 1) / max_pw : 0;
+      pw = npass > 0 ? ((n_tile + npass - 1) / npass + 15) / 16 * 16 : 0;
+    }
+    const int ldst = pw + 2;
+    const bool bulk = npass > 0 && (size_t)BM * ldst * sizeof(double) <= (size_t)STAGE_MEM && (n_out & 1) == 0 &&
                       (reinterpret_cast<uintptr_t>(out) & 15) == 0;
-    if (bulk) {
+    if (NACC == 3 && bulk) {
+      // one pass: the whole tile fits the idle stage memory
       double* stg = (double*)smem;
       if (ok)
-        epilogue_stage_warp<PIECES, COMPS>(tmem, n_tile, n0, n_out, nact_p[2] >= 0, rexp, scales, stg, ldst, warp,
-                                           lane, warp >> 2, kProdWarps / 4, nact_p[1] >= 0);
+        epilogue_stage_warp<PIECES, COMPS, NACC>(tmem, n_tile, n0, n_out, nact_p[2] >= 0, rexp, scales, stg, ldst,
+                                                 warp, lane, warp >> 2, kProdWarps / 4, nact_p[1] >= 0);
       fence_async_smem();
       named_bar_sync(1, kProd);   // all producer warps arrive, whatever their `ok`
       if (ok) {
@@ -283,10 +315,35 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
         bulk_commit();
         bulk_wait_read();
       }
+    } else if (bulk) {
+      double* stg = (double*)smem;
+      for (int c_lo = 0; c_lo < n_tile; c_lo += pw) {
+        if (c_lo > 0) named_bar_sync(1, kProd);   // the previous pass's rows have left the staging memory
+        if (ok)
+          epilogue_stage_warp<PIECES, COMPS, NACC>(tmem, n_tile, n0, n_out, nact_p[2] >= 0, rexp, scales, stg, ldst,
+                                                   warp, lane, warp >> 2, kProdWarps / 4, nact_p[1] >= 0, c_lo,
+                                                   c_lo + pw);
+        fence_async_smem();
+        named_bar_sync(1, kProd);   // all producer warps arrive, whatever their `ok`
+        if (ok) {
+          // even: n_out even, n0 and c_lo multiples of 16
+          const int ncols = min(min(pw, n_tile - c_lo), n_out - n0 - c_lo);
+          if (ncols > 0) {
+            for (int r = tid; r < PTS * COMPS; r += kProd) {
+              const int64_t pq = pidx[r / COMPS];
+              if (pq >= 0)
+                bulk_store(out + (pq * COMPS + r % COMPS) * n_out + n0 + c_lo, stg + (size_t)r * ldst,
+                           (uint32_t)ncols * 8u);
+            }
+          }
+          bulk_commit();
+          bulk_wait_read();
+        }
+      }
     } else if (ok) {
-      epilogue_warp<PIECES, COMPS>(tmem, n_tile, n0, n_out, nact_p[2] >= 0, pidx, rexp, scales, out,
-                                   (double*)smem + warp * 32 * 16, warp, lane, warp >> 2, kProdWarps / 4,
-                                   nact_p[1] >= 0);
+      epilogue_warp<PIECES, COMPS, NACC>(tmem, n_tile, n0, n_out, nact_p[2] >= 0, pidx, rexp, scales, out,
+                                         (double*)smem + warp * 32 * 16, warp, lane, warp >> 2, kProdWarps / 4,
+                                         nact_p[1] >= 0);
     }
   }
   tc_fence_before();
@@ -352,24 +409,27 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 size_t tile_plan_pts_bytes(int64_t tiles, int pts) { return ((size_t)tiles * 3 * pts * sizeof(double) + 255) / 256 * 256; }
 
-template <int PIECES, int COMPS>
+template <int PIECES, int COMPS, int NACC>
 size_t fused_smem(int n_tile, int rec_bytes, int kblocks) {
   constexpr int PTS = BM / COMPS;
-  const size_t stage = (size_t)PIECES * (A_TILE + (size_t)n_tile * BK * 2);
-  return 1024 + STAGES * stage + (size_t)STAGES * rec_bytes + ((kKsteps + 3) * STAGES + 2) * 8 + 4 * PTS * 8 +
+  const size_t b_tile = (size_t)PIECES * n_tile * BK * 2;
+  const size_t stage_mem = NACC == 3 ? STAGES * ((size_t)PIECES * A_TILE + b_tile)
+                                     : STAGES * (size_t)PIECES * A_TILE + b_tile;
+  return 1024 + stage_mem + (size_t)STAGES * rec_bytes + ((kKsteps + 3) * STAGES + 2) * 8 + 4 * PTS * 8 +
          3 * PTS * 4 +
          (size_t)(2 * kblocks + 5) * 4 + 16;
 }
 
-template <int PIECES, int COMPS>
+template <int PIECES, int COMPS, int NACC>
 cudaError_t launch_fused(const DevTables& T, const CUtensorMap& tb, int64_t P, const double* coord, double cutoff,
                          int n_out, int n_tile, int n_tiles, int kblocks, const uint8_t* krec, int rec_bytes,
                          const int* perm, const double* scales, const RowBound& rb, double* out, int* err,
                          int64_t cstride, const uint8_t* kskip, unsigned long long* kstat, void* tplan,
                          cudaStream_t s) {
   constexpr int PTS = BM / COMPS;
-  const size_t smem = fused_smem<PIECES, COMPS>(n_tile, rec_bytes, kblocks);
-  auto kern = fused_mo_kernel<PIECES, COMPS>;
+  const size_t smem = fused_smem<PIECES, COMPS, NACC>(n_tile, rec_bytes, kblocks);
+  auto kern = fused_mo_kernel<PIECES, COMPS, NACC>;
+  if (NACC == 2 && tplan == nullptr) return cudaErrorInvalidValue;   // the wide form needs a tile plan
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const int64_t tiles = (P + PTS - 1) / PTS;
@@ -394,9 +454,13 @@ cudaError_t launch_fused(const DevTables& T, const CUtensorMap& tb, int64_t P, c
 
 size_t tc_fused_smem(const TcPlan& plan, int comps, int rec_bytes) {
   const int kb = (int)((plan.ao_num + BK - 1) / BK);
+  if (plan.pieces == 3 && plan.nacc == 2)
+    return comps == 5 ? fused_smem<3, 5, 2>(plan.n_tile, rec_bytes, kb)
+                      : fused_smem<3, 1, 2>(plan.n_tile, rec_bytes, kb);
   if (plan.pieces == 3)
-    return comps == 5 ? fused_smem<3, 5>(plan.n_tile, rec_bytes, kb) : fused_smem<3, 1>(plan.n_tile, rec_bytes, kb);
-  return comps == 5 ? fused_smem<2, 5>(plan.n_tile, rec_bytes, kb) : fused_smem<2, 1>(plan.n_tile, rec_bytes, kb);
+    return comps == 5 ? fused_smem<3, 5, 3>(plan.n_tile, rec_bytes, kb)
+                      : fused_smem<3, 1, 3>(plan.n_tile, rec_bytes, kb);
+  return comps == 5 ? fused_smem<2, 5, 3>(plan.n_tile, rec_bytes, kb) : fused_smem<2, 1, 3>(plan.n_tile, rec_bytes, kb);
 }
 
 size_t tc_tile_plan_bytes(const TcPlan& plan, int64_t point_num, int comps) {
@@ -437,14 +501,19 @@ cudaError_t tc_launch_fused(const TcPlan& plan, int64_t point_num, int comps, co
   const int M = (int)plan.mo_num;
   const double* sc = tc_scales(plan, d_coef);
   const uint8_t* ks = (const uint8_t*)kskip;
+  if (plan.pieces == 3 && plan.nacc == 2)
+    return comps == 5 ? launch_fused<3, 5, 2>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks,
+                                              kr, rec_bytes, perm, sc, rb, out, err, cstride, ks, kstat, tplan, s)
+                      : launch_fused<3, 1, 2>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks,
+                                              kr, rec_bytes, perm, sc, rb, out, err, cstride, ks, kstat, tplan, s);
   if (plan.pieces == 3)
-    return comps == 5 ? launch_fused<3, 5>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
+    return comps == 5 ? launch_fused<3, 5, 3>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
                                            rec_bytes, perm, sc, rb, out, err, cstride, ks, kstat, tplan, s)
-                      : launch_fused<3, 1>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
+                      : launch_fused<3, 1, 3>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
                                            rec_bytes, perm, sc, rb, out, err, cstride, ks, kstat, tplan, s);
-  return comps == 5 ? launch_fused<2, 5>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
+  return comps == 5 ? launch_fused<2, 5, 3>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
                                          rec_bytes, perm, sc, rb, out, err, cstride, ks, kstat, tplan, s)
-                    : launch_fused<2, 1>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
+                    : launch_fused<2, 1, 3>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
                                          rec_bytes, perm, sc, rb, out, err, cstride, ks, kstat, tplan, s);
 }
 

@@ -31,6 +31,7 @@
 #include <cudaTypedefs.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -630,6 +631,24 @@ TcPlan tc_plan(int64_t ao_num, int64_t mo_num, int pieces) {
     const int64_t q = (mo_num + p.n_tiles - 1) / p.n_tiles;
     p.n_tile = (int)((q + 15) / 16 * 16);
   }
+  p.n_pad = (int64_t)p.n_tile * p.n_tiles;
+  p.scale_off = ((size_t)pieces * p.n_pad * p.k_pad * 2 + 255) / 256 * 256;
+  p.coef_bytes = p.scale_off + sizeof(double) * (kScaleCols + (size_t)p.n_pad);
+  return p;
+}
+
+TcPlan tc_plan_fused(int64_t ao_num, int64_t mo_num, int pieces) {
+  TcPlan p = tc_plan(ao_num, mo_num, pieces);
+  const char* env = std::getenv("QMCKL_B200_WIDE_TILES");
+  if (pieces != 3 || p.n_tiles < 2 || (env != nullptr && std::strcmp(env, "0") == 0)) return p;
+  // two accumulators of up to 256 columns fit TMEM (512); the single
+  // coefficient tile (3 x 128 B per MO) fits beside the two 48 KB A stages
+  const int n_tiles = (int)((mo_num + 255) / 256);
+  if (n_tiles >= p.n_tiles) return p;
+  const int64_t per = (mo_num + n_tiles - 1) / n_tiles;
+  p.n_tiles = n_tiles;
+  p.n_tile = (int)((per + 15) / 16 * 16);
+  p.nacc = 2;
   p.n_pad = (int64_t)p.n_tile * p.n_tiles;
   p.scale_off = ((size_t)pieces * p.n_pad * p.k_pad * 2 + 255) / 256 * 256;
   p.coef_bytes = p.scale_off + sizeof(double) * (kScaleCols + (size_t)p.n_pad);

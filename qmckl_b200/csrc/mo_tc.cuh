@@ -26,6 +26,7 @@ struct TcPlan {
   int n_tile = 0;
   size_t scale_off = 0;  // byte offset of the scale block (split.cuh) after the pieces
   size_t coef_bytes = 0; // pieces * n_pad * k_pad 16-bit values + the scale block
+  int nacc = 3;          // fused kernel: 3 accumulators (n_tile <= 160) or 2 (wide tiles, n_tile <= 256)
 };
 
 // Device pointer to the scale block of a plan's coefficient buffer.
@@ -34,6 +35,10 @@ inline const double* tc_scales(const TcPlan& plan, const void* d_coef) {
 }
 
 TcPlan tc_plan(int64_t ao_num, int64_t mo_num, int pieces);
+// The fused kernel's plan: tc_plan's, or, when that takes several MO tiles
+// and wider ones would take fewer, tiles of up to 256 MOs with two
+// accumulators (QMCKL_B200_WIDE_TILES=0: never).
+TcPlan tc_plan_fused(int64_t ao_num, int64_t mo_num, int pieces);
 size_t tc_a_bytes(const TcPlan& plan, int64_t rows);
 // coefficient [mo][ao] (host, FP64) -> split pieces and the scale block on
 // the device (per-MO scales for 2 pieces).

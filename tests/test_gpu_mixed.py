@@ -183,3 +183,39 @@ def test_fused_follows_precision_changes():
     ref30 = O.mo_vgl(d["mo_coef"], O.ao_vgl(basis, pts, d["nucl_coord"], precision=30))
     assert max(comp_error(second, ref30)) <= MIXED_TOL
     pq.context_destroy(ctx)
+
+
+@pytest.mark.parametrize("mos", [161, 330, 350])
+def test_wide_mo_tiles(mos, monkeypatch):
+    """Past 160 MOs the fused kernel takes MO tiles of up to 256 columns with
+    two accumulators (leading product, corrections) and a single coefficient
+    tile, so each AO is evaluated once per tile of 256 MOs rather than of
+    160: one tile for 161 MOs, two for 330 and 350.  The results stay within
+    the mixed-form bound of the FP64 form and of the three-accumulator tiling
+    (QMCKL_B200_WIDE_TILES=0), and the kernel's statistics count the tiles it
+    ran."""
+    import torch
+    d = gen.config(1, walk_num=2)
+    rng = np.random.default_rng(10000 + mos)
+    q, _ = np.linalg.qr(rng.standard_normal((d["ao_num"], mos)))
+    d = dict(d, mo_coef=np.ascontiguousarray(q.T), mo_num=mos)
+    pts = gen.points(d)
+    P = pts.shape[0]
+    dc = torch.tensor(np.ascontiguousarray(pts.T), dtype=torch.float64, device="cuda")
+    res, tiles = {}, {}
+    for name, form, wide in (("fp64", pq.FORM_FP64, "1"), ("wide", pq.FORM_MIXED, "1"), ("narrow", pq.FORM_MIXED, "0")):
+        monkeypatch.setenv("QMCKL_B200_WIDE_TILES", wide)
+        ctx = make_context(d, points=False, form=form)
+        out = torch.full((P * 5 * mos,), float("nan"), dtype=torch.float64, device="cuda")
+        pq.b200_mo_vgl_device(ctx, P, dc.data_ptr(), out.data_ptr())
+        pq.b200_synchronize(ctx)
+        res[name] = out.cpu().numpy().reshape(P, 5, mos)
+        if form == pq.FORM_MIXED:
+            _, tot = pq.b200_get_kblock_stats(ctx, reset=True)
+            tiles[name] = tot // (-(-P // 25) * 32 * 4)
+        pq.context_destroy(ctx)
+    assert tiles["wide"] == -(-mos // 256)
+    assert tiles["narrow"] == -(-mos // 160)
+    assert np.isfinite(res["wide"]).all()
+    assert max(comp_error(res["wide"], res["fp64"])) < MIXED_TOL
+    assert max(comp_error(res["wide"], res["narrow"])) < MIXED_TOL
