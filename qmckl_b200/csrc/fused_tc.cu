@@ -42,10 +42,11 @@ constexpr int kKsteps = BK / UMMA_K;   // 16-AO k-steps per K block, 4 producer 
 // product in two halves of K, the corrections), each stage holding its A
 // and coefficient tiles.  NACC = 2 (wide MO tiles, n_tile <= 256, with a tile
 // plan only): the leading product in one accumulator, the corrections in the
-// other, and a single coefficient tile after the two A stages, loaded for
-// block it once the MMAs of block it - 1 are done; the epilogue then writes
-// the tile in column passes that fit the idle stage memory.
-template <int PIECES, int COMPS, int NACC>
+// other, and a single coefficient tile after the NST A stages (three where
+// they fit, else two), loaded for block it once the MMAs of block it - 1 are
+// done; the epilogue writes the tile in column passes that fit the idle
+// stage memory.
+template <int PIECES, int COMPS, int NACC, int NST>
 __global__ void __launch_bounds__(kThreadsF, 1)
 fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, const int64_t P,
                 const double* __restrict__ coord, const double cutoff, const int n_out, const int n_tile,
@@ -55,6 +56,9 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
                 const uint8_t* __restrict__ kskip, unsigned long long* __restrict__ kstat,
                 const double* __restrict__ tpts, const int* __restrict__ tinfo) {
   constexpr int PTS = BM / COMPS;            // 25 points (VGL) or 128 (value)
+  // NST stages of the A tiles: 2 for NACC = 3 (each with its coefficient
+  // tile), 2 or 3 for wide MO tiles
+  static_assert(NACC == 2 || NST == STAGES, "three accumulators: two stages");
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   // 1024-byte aligned base, kept as pointer arithmetic on the __shared__
   // array so that accesses compile to shared-memory (not generic) loads
@@ -63,19 +67,19 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
   const int A_BYTES = PIECES * A_TILE;
   const int STAGE = NACC == 3 ? PIECES * (A_TILE + B_TILE) : A_BYTES;
   // offset of the coefficient tile from the start of stage s
-  auto b_off = [&](int s) { return NACC == 3 ? A_BYTES : (STAGES - s) * STAGE; };
-  const int STAGE_MEM = STAGES * STAGE + (NACC == 3 ? 0 : PIECES * B_TILE);
-  uint8_t* recs = smem + STAGE_MEM;           // STAGES K-block records
+  auto b_off = [&](int s) { return NACC == 3 ? A_BYTES : (NST - s) * STAGE; };
+  const int STAGE_MEM = NST * STAGE + (NACC == 3 ? 0 : PIECES * B_TILE);
+  uint8_t* recs = smem + STAGE_MEM;           // NST K-block records
   // Barriers: full[4 s + kk], k-step kk of the block in stage s produced (its
   // four chunks, or the MMA thread in their place when the k-step is
   // skipped); bfull[s], the block's coefficient pieces landed; empty[s], all
   // the block's MMAs done (the stage and its record slot free); rec_full[s],
   // its record landed.
-  uint64_t* full = (uint64_t*)(recs + STAGES * rec_bytes);
-  uint64_t* bfull = full + STAGES * kKsteps;
-  uint64_t* empty = bfull + STAGES;
-  uint64_t* rec_full = empty + STAGES;
-  uint64_t* acc_full = rec_full + STAGES;
+  uint64_t* full = (uint64_t*)(recs + NST * rec_bytes);
+  uint64_t* bfull = full + NST * kKsteps;
+  uint64_t* empty = bfull + NST;
+  uint64_t* rec_full = empty + NST;
+  uint64_t* acc_full = rec_full + NST;
   uint32_t* tmem_slot = (uint32_t*)(acc_full + 1);
   double* pts = (double*)(acc_full + 2);      // [3][PTS]
   int64_t* pidx = (int64_t*)(pts + 3 * PTS);  // [PTS] original index of each tile point
@@ -91,22 +95,22 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
   uint32_t tmem_cols = 32;
   while ((int)tmem_cols < NACC * n_tile) tmem_cols <<= 1;
 
-  // loads of K block kb (the it-th of the tile) into stage it % STAGES: the
+  // loads of K block kb (the it-th of the tile) into stage it % NST: the
   // block's record and its coefficient pieces
   auto load_record = [&](int it, int kb) {
-    const int s = it & 1;
+    const int s = it % NST;
     mbar_expect_tx(&rec_full[s], (uint32_t)rec_bytes);
     bulk_load(recs + s * rec_bytes, krec + (size_t)kb * rec_bytes, (uint32_t)rec_bytes, &rec_full[s]);
   };
   auto load_coef = [&](int it, int kb) {
-    const int s = it & 1;
+    const int s = it % NST;
     uint8_t* st = smem + s * STAGE + b_off(s);
     mbar_expect_tx(&bfull[s], (uint32_t)(PIECES * B_TILE));
     for (int q = 0; q < PIECES; ++q) tma_load_3d(st + q * B_TILE, &tmB, &bfull[s], kb * BK, n0, q);
   };
   int tma_pre = 0;   // K blocks whose loads the TMA thread issued during the prologue
   if (tid == kTmaWarp * 32) {
-    for (int s = 0; s < STAGES; ++s) {
+    for (int s = 0; s < NST; ++s) {
       for (int kk = 0; kk < kKsteps; ++kk) mbar_init(&full[s * kKsteps + kk], kProd / kKsteps);
       mbar_init(&bfull[s], 1);
       mbar_init(&empty[s], 1);
@@ -119,7 +123,7 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
       // (into stages not used yet, nothing to wait for) run under the prologue
       const int* ti = tinfo + (size_t)blockIdx.x * (kblocks + 4);
       const int n = ti[0];
-      tma_pre = n < STAGES ? n : STAGES;
+      tma_pre = n < NST ? n : NST;
       for (int it = 0; it < tma_pre; ++it) {
         load_record(it, ti[4 + it] & 0xFFFF);
         if (NACC == 3 || it == 0) load_coef(it, ti[4 + it] & 0xFFFF);   // one coefficient tile (NACC 2)
@@ -161,7 +165,7 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
     }
   }
   // rows PTS*COMPS .. 127 of the A tiles stay zero for the whole kernel
-  zero_pad_rows<PIECES, COMPS, STAGES>(smem, STAGE, tid, kThreadsF);
+  zero_pad_rows<PIECES, COMPS, NST>(smem, STAGE, tid, kThreadsF);
   if (warp == kMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
                  "r"(tmem_cols));
@@ -187,19 +191,19 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
     // whose chunks are all in progress.
     // A chunk of a skipped k-step is never read by the MMAs: it waits for
     // the stage only (so that every chunk of a block waits for the same
-    // barrier, which keeps any warp from claiming a chunk two blocks past a
+    // barrier, which keeps any warp from claiming a chunk NST blocks past a
     // stage still in use) and does not arrive; the MMA thread arrives for
     // the whole skipped k-step.
     const int total = nact * kProdWarps;
     for (int q = warp; q < total;) {
       const int it = q / kProdWarps, c = q - it * kProdWarps;
-      const int s = it & 1;
-      const uint32_t phase = (uint32_t)(it >> 1) & 1u;
+      const int s = it % NST;
+      const uint32_t phase = (uint32_t)(it / NST) & 1u;
       const bool live = kstep_live(act[it], c, kChunk);
       // warp-uniform outcome: every lane must take the same path.  A
       // produced chunk also waits for the block's record.  Its arrival comes
       // after the stage's release, that is after the MMA thread has waited
-      // for the same full[] barrier's phase of the block two back, so no
+      // for the same full[] barrier's phase of the block NST back, so no
       // phase of a barrier mixes the arrivals of two blocks and no parity
       // wait falls two phases behind.
       bool ok = mbar_wait(&empty[s], phase ^ 1u, err, 11);
@@ -220,23 +224,24 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
     if (lane == 0) {
       if (NACC == 3) {
         for (int it = tma_pre; it < nact; ++it) {
-          const int s = it & 1;
-          const uint32_t phase = (uint32_t)(it >> 1) & 1u;
-          // the stage, its record slot included: every MMA of block it - 2 done
+          const int s = it % NST;
+          const uint32_t phase = (uint32_t)(it / NST) & 1u;
+          // the stage, its record slot included: every MMA of block it - NST done
           if (!mbar_wait(&empty[s], phase ^ 1u, err, 12)) break;
           load_record(it, act[it] & 0xFFFF);
           load_coef(it, act[it] & 0xFFFF);
         }
       } else {
         // the single coefficient tile of block it once the MMAs of block
-        // it - 1 are done; then the record of block it + 1, whose slot (block
+        // it - 1 are done; then the record of block it + 2, whose slot (block
         // it - 1's) is free by the same wait (the prologue loaded records 0
-        // and 1 and the coefficients of block 0)
+        // to 2 and the coefficients of block 0)
         for (int it = 1; it < nact; ++it) {
           const int b = it - 1;
-          if (!mbar_wait(&empty[b & 1], (uint32_t)(b >> 1) & 1u, err, 12)) break;
+          if (!mbar_wait(&empty[b % NST], (uint32_t)(b / NST) & 1u, err, 12)) break;
           load_coef(it, act[it] & 0xFFFF);
-          if (it + 1 < nact && it + 1 >= tma_pre) load_record(it + 1, act[it + 1] & 0xFFFF);
+          const int r = it + NST - 1;   // its record slot is block it - 1's
+          if (r < nact && r >= tma_pre) load_record(r, act[r] & 0xFFFF);
         }
       }
     }
@@ -246,11 +251,11 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
       const uint32_t idesc = mma_idesc<PIECES>(n_tile);
       bool init[3] = {false, false, false};   // accumulators written so far
       for (int it = 0; it < nact; ++it) {
-        const int s = it & 1;
-        const uint32_t phase = (uint32_t)(it >> 1) & 1u;
+        const int s = it % NST;
+        const uint32_t phase = (uint32_t)(it / NST) & 1u;
         // each k-step's MMAs go out as soon as its four chunks are produced;
         // for a skipped k-step this thread arrives in place of its chunks
-        // (it waited for that barrier's phase of the block two back itself)
+        // (it waited for that barrier's phase of the block NST back itself)
         if (!mbar_wait(&bfull[s], phase, err, 13)) break;
         const int kb = act[it] & 0xFFFF;
         uint32_t kmask = (uint32_t)act[it] >> 16;
@@ -409,26 +414,25 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 size_t tile_plan_pts_bytes(int64_t tiles, int pts) { return ((size_t)tiles * 3 * pts * sizeof(double) + 255) / 256 * 256; }
 
-template <int PIECES, int COMPS, int NACC>
+template <int PIECES, int COMPS, int NACC, int NST>
 size_t fused_smem(int n_tile, int rec_bytes, int kblocks) {
   constexpr int PTS = BM / COMPS;
   const size_t b_tile = (size_t)PIECES * n_tile * BK * 2;
-  const size_t stage_mem = NACC == 3 ? STAGES * ((size_t)PIECES * A_TILE + b_tile)
-                                     : STAGES * (size_t)PIECES * A_TILE + b_tile;
-  return 1024 + stage_mem + (size_t)STAGES * rec_bytes + ((kKsteps + 3) * STAGES + 2) * 8 + 4 * PTS * 8 +
+  const size_t stage_mem = NACC == 3 ? NST * ((size_t)PIECES * A_TILE + b_tile) : NST * (size_t)PIECES * A_TILE + b_tile;
+  return 1024 + stage_mem + (size_t)NST * rec_bytes + ((kKsteps + 3) * NST + 2) * 8 + 4 * PTS * 8 +
          3 * PTS * 4 +
          (size_t)(2 * kblocks + 5) * 4 + 16;
 }
 
-template <int PIECES, int COMPS, int NACC>
+template <int PIECES, int COMPS, int NACC, int NST>
 cudaError_t launch_fused(const DevTables& T, const CUtensorMap& tb, int64_t P, const double* coord, double cutoff,
                          int n_out, int n_tile, int n_tiles, int kblocks, const uint8_t* krec, int rec_bytes,
                          const int* perm, const double* scales, const RowBound& rb, double* out, int* err,
                          int64_t cstride, const uint8_t* kskip, unsigned long long* kstat, void* tplan,
                          cudaStream_t s) {
   constexpr int PTS = BM / COMPS;
-  const size_t smem = fused_smem<PIECES, COMPS, NACC>(n_tile, rec_bytes, kblocks);
-  auto kern = fused_mo_kernel<PIECES, COMPS, NACC>;
+  const size_t smem = fused_smem<PIECES, COMPS, NACC, NST>(n_tile, rec_bytes, kblocks);
+  auto kern = fused_mo_kernel<PIECES, COMPS, NACC, NST>;
   if (NACC == 2 && tplan == nullptr) return cudaErrorInvalidValue;   // the wide form needs a tile plan
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -454,13 +458,14 @@ cudaError_t launch_fused(const DevTables& T, const CUtensorMap& tb, int64_t P, c
 
 size_t tc_fused_smem(const TcPlan& plan, int comps, int rec_bytes) {
   const int kb = (int)((plan.ao_num + BK - 1) / BK);
+  const int n = plan.n_tile;
+  if (plan.pieces == 3 && plan.nacc == 2 && plan.nst == 3)
+    return comps == 5 ? fused_smem<3, 5, 2, 3>(n, rec_bytes, kb) : fused_smem<3, 1, 2, 3>(n, rec_bytes, kb);
   if (plan.pieces == 3 && plan.nacc == 2)
-    return comps == 5 ? fused_smem<3, 5, 2>(plan.n_tile, rec_bytes, kb)
-                      : fused_smem<3, 1, 2>(plan.n_tile, rec_bytes, kb);
+    return comps == 5 ? fused_smem<3, 5, 2, 2>(n, rec_bytes, kb) : fused_smem<3, 1, 2, 2>(n, rec_bytes, kb);
   if (plan.pieces == 3)
-    return comps == 5 ? fused_smem<3, 5, 3>(plan.n_tile, rec_bytes, kb)
-                      : fused_smem<3, 1, 3>(plan.n_tile, rec_bytes, kb);
-  return comps == 5 ? fused_smem<2, 5, 3>(plan.n_tile, rec_bytes, kb) : fused_smem<2, 1, 3>(plan.n_tile, rec_bytes, kb);
+    return comps == 5 ? fused_smem<3, 5, 3, 2>(n, rec_bytes, kb) : fused_smem<3, 1, 3, 2>(n, rec_bytes, kb);
+  return comps == 5 ? fused_smem<2, 5, 3, 2>(n, rec_bytes, kb) : fused_smem<2, 1, 3, 2>(n, rec_bytes, kb);
 }
 
 size_t tc_tile_plan_bytes(const TcPlan& plan, int64_t point_num, int comps) {
@@ -501,20 +506,17 @@ cudaError_t tc_launch_fused(const TcPlan& plan, int64_t point_num, int comps, co
   const int M = (int)plan.mo_num;
   const double* sc = tc_scales(plan, d_coef);
   const uint8_t* ks = (const uint8_t*)kskip;
+  auto run = [&](auto launch) {
+    return launch(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr, rec_bytes, perm, sc, rb,
+                  out, err, cstride, ks, kstat, tplan, s);
+  };
+  if (plan.pieces == 3 && plan.nacc == 2 && plan.nst == 3)
+    return comps == 5 ? run(launch_fused<3, 5, 2, 3>) : run(launch_fused<3, 1, 2, 3>);
   if (plan.pieces == 3 && plan.nacc == 2)
-    return comps == 5 ? launch_fused<3, 5, 2>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks,
-                                              kr, rec_bytes, perm, sc, rb, out, err, cstride, ks, kstat, tplan, s)
-                      : launch_fused<3, 1, 2>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks,
-                                              kr, rec_bytes, perm, sc, rb, out, err, cstride, ks, kstat, tplan, s);
+    return comps == 5 ? run(launch_fused<3, 5, 2, 2>) : run(launch_fused<3, 1, 2, 2>);
   if (plan.pieces == 3)
-    return comps == 5 ? launch_fused<3, 5, 3>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
-                                           rec_bytes, perm, sc, rb, out, err, cstride, ks, kstat, tplan, s)
-                      : launch_fused<3, 1, 3>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
-                                           rec_bytes, perm, sc, rb, out, err, cstride, ks, kstat, tplan, s);
-  return comps == 5 ? launch_fused<2, 5, 3>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
-                                         rec_bytes, perm, sc, rb, out, err, cstride, ks, kstat, tplan, s)
-                    : launch_fused<2, 1, 3>(T, tb, point_num, coord, cutoff, M, plan.n_tile, plan.n_tiles, kblocks, kr,
-                                         rec_bytes, perm, sc, rb, out, err, cstride, ks, kstat, tplan, s);
+    return comps == 5 ? run(launch_fused<3, 5, 3, 2>) : run(launch_fused<3, 1, 3, 2>);
+  return comps == 5 ? run(launch_fused<2, 5, 3, 2>) : run(launch_fused<2, 1, 3, 2>);
 }
 
 cudaError_t tc_run_fused(const DevTables& T, const TcPlan& plan, int64_t point_num, int comps, const double* coord,

@@ -646,9 +646,19 @@ TcPlan tc_plan_fused(int64_t ao_num, int64_t mo_num, int pieces) {
   const int n_tiles = (int)((mo_num + 255) / 256);
   if (n_tiles >= p.n_tiles) return p;
   const int64_t per = (mo_num + n_tiles - 1) / n_tiles;
+  const int n_tile = (int)((per + 15) / 16 * 16);
+  // shared memory: the A stages (48 KB each), the coefficient tile
+  // (384 B per MO), room for a K-block record per stage (4 KB each) and
+  // the rest (alignment, barriers, points, lists: 3 KB)
+  auto bytes = [&](int nst) { return 1024 + (size_t)nst * (49152 + 4096) + (size_t)384 * n_tile + 3072; };
+  int nst = 0;
+  if (bytes(3) <= 232448) nst = 3;
+  else if (bytes(2) <= 232448) nst = 2;
+  if (nst == 0) return p;
   p.n_tiles = n_tiles;
-  p.n_tile = (int)((per + 15) / 16 * 16);
+  p.n_tile = n_tile;
   p.nacc = 2;
+  p.nst = nst;
   p.n_pad = (int64_t)p.n_tile * p.n_tiles;
   p.scale_off = ((size_t)pieces * p.n_pad * p.k_pad * 2 + 255) / 256 * 256;
   p.coef_bytes = p.scale_off + sizeof(double) * (kScaleCols + (size_t)p.n_pad);

@@ -27,6 +27,7 @@ struct TcPlan {
   size_t scale_off = 0;  // byte offset of the scale block (split.cuh) after the pieces
   size_t coef_bytes = 0; // pieces * n_pad * k_pad 16-bit values + the scale block
   int nacc = 3;          // fused kernel: 3 accumulators (n_tile <= 160) or 2 (wide tiles, n_tile <= 256)
+  int nst = 2;           // fused kernel: stages of the A tiles (3 for wide tiles when they fit)
 };
 
 // Device pointer to the scale block of a plan's coefficient buffer.
