@@ -639,12 +639,16 @@ TcPlan tc_plan(int64_t ao_num, int64_t mo_num, int pieces) {
 
 TcPlan tc_plan_fused(int64_t ao_num, int64_t mo_num, int pieces) {
   TcPlan p = tc_plan(ao_num, mo_num, pieces);
+  // QMCKL_B200_WIDE_TILES: unset, wide tiles when they take fewer MO tiles;
+  // "0", never; "1", whenever they fit
   const char* env = std::getenv("QMCKL_B200_WIDE_TILES");
-  if (pieces != 3 || p.n_tiles < 2 || (env != nullptr && std::strcmp(env, "0") == 0)) return p;
+  const bool never = env != nullptr && std::strcmp(env, "0") == 0;
+  const bool always = env != nullptr && std::strcmp(env, "1") == 0;
+  if (pieces != 3 || never || (p.n_tiles < 2 && !always)) return p;
   // two accumulators of up to 256 columns fit TMEM (512); the single
-  // coefficient tile (3 x 128 B per MO) fits beside the two 48 KB A stages
+  // coefficient tile (3 x 128 B per MO) fits beside the 48 KB A stages
   const int n_tiles = (int)((mo_num + 255) / 256);
-  if (n_tiles >= p.n_tiles) return p;
+  if (n_tiles >= p.n_tiles && !always) return p;
   const int64_t per = (mo_num + n_tiles - 1) / n_tiles;
   const int n_tile = (int)((per + 15) / 16 * 16);
   // shared memory: the A stages (48 KB each), the coefficient tile
