@@ -73,6 +73,7 @@ struct BatchCtl {                 // shared-memory control block of a CTA
   uint32_t tmem_slot;
   int item[4];
   int ok;
+  int claim;   // chunks of the current item claimed by the producer warps after their first
   double pts[3 * kPts];
   int64_t pidx[kPts];
   int rexp[3 * kPts];
@@ -265,21 +266,34 @@ batch_mo_kernel(const BatchDesc* __restrict__ desc, const CUtensorMap* __restric
                             NTHREADS / 32, true);
     __syncthreads();
     if (warp == 0) tile_kblock_list(kflag, kblocks, act, kcnt, lane, true);
+    if (tid == 0) C.claim = 0;
     __syncthreads();
     const int nact = kcnt[0];
     if (warp < PRODW) {
-      for (int it = 0; it < nact; ++it) {
+      // the item's PRODW chunks per K block, claimed in order from a shared
+      // counter (first: chunk `warp` of the first block), as in the
+      // single-system kernel (fused_tc.cu): a warp done early goes on with
+      // the next chunks instead of waiting for its block's slowest warp.
+      // Every chunk waits for its stage and record and arrives (one barrier
+      // per stage, as many chunks as warps), so no wait falls two phases
+      // behind.
+      const int total = nact * PRODW;
+      for (int q = warp; q < total;) {
+        const int it = q / PRODW, c = q - it * PRODW;
         const uint32_t g = kbase + (uint32_t)it;
         const int s = (int)(g & 1u);
         const uint32_t phase = (g >> 1) & 1u;
         bool ok = mbar_wait(&C.empty[s], phase ^ 1u, err, 21);
         ok = ok && mbar_wait(&C.rec_full[s], phase, err, 25);
         if (!__all_sync(0xffffffffu, ok)) break;
-        if (kstep_live(act[it], warp, CHUNK))
+        if (kstep_live(act[it], c, CHUNK))
           produce_kblock<PIECES, COMPS, CHUNK>(recs + s * rec_max, C.pts, p0, P, D.cutoff, C.rexp,
-                                               smem_addr(smem + s * STAGE), warp, lane);
+                                               smem_addr(smem + s * STAGE), c, lane);
         fence_async_smem();
         mbar_arrive(&C.full[s]);
+        int nq = 0;
+        if (lane == 0) nq = atomicAdd(&C.claim, 1) + PRODW;
+        q = __shfl_sync(0xffffffffu, nq, 0);
       }
     } else if (warp == TMA_WARP) {
       if (lane == 0) {
