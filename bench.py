@@ -660,9 +660,12 @@ def mixed_roofline(args, P, A, M, ms, ks_eval, ks_total, bf16, peak_src):
     cap = load_traffic().get(("fused_mo_kernel", "mixed"))
     if cap and cap[0] > 0 and not args.unfused and args.pieces == 3:
         traffic = _scaled_traffic("fused_mo_kernel", "mixed", P)
-        traffic_note = (f"DRAM read + write bytes per launch: ncu capture at {int(cap[0])} points "
-                        f"(profiles/dram_traffic.txt) scaled by the point count; the algorithmic bytes "
-                        f"are the {40.0 * P * M / 1e9:.3f} GB of mo_vgl written + 24 P bytes of coordinates")
+        scaled = "" if int(cap[0]) == P else " scaled by the point count"
+        traffic_note = (f"DRAM read + write bytes of one launch from an ncu capture at {int(cap[0])} points "
+                        f"(profiles/dram_traffic.txt){scaled}; the algorithmic bytes are the "
+                        f"{40.0 * P * M / 1e9:.3f} GB of mo_vgl written + 24 P bytes of coordinates, of which "
+                        f"~56 MB are still dirty in L2 when the kernel ends (written back afterwards, "
+                        f"uncounted in the launch)")
     return {"kernel": kname, "bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
             "frac": achieved / bf16, "peak_source": peak_src,
             "achieved_basis": "issued split-BF16 MMA flops per step / step time",
