@@ -219,3 +219,27 @@ def test_wide_mo_tiles(mos, monkeypatch):
     assert np.isfinite(res["wide"]).all()
     assert max(comp_error(res["wide"], res["fp64"])) < MIXED_TOL
     assert max(comp_error(res["wide"], res["narrow"])) < MIXED_TOL
+
+
+@pytest.mark.parametrize("mos", [224, 350])
+def test_wide_mo_tiles_value_form(mos):
+    """MO values alone (128-point tiles) with wide MO tiles: one tile of 224
+    (two A stages) or two of 176 (three A stages where they fit, else the
+    three-accumulator tiling), against the FP64 form, and the same values as
+    the VGL form's value component within the mixed bound."""
+    d = gen.config(1, walk_num=2)
+    rng = np.random.default_rng(11000 + mos)
+    q, _ = np.linalg.qr(rng.standard_normal((d["ao_num"], mos)))
+    d = dict(d, mo_coef=np.ascontiguousarray(q.T), mo_num=mos)
+    P = d["elec_coord"].shape[0] * d["elec_coord"].shape[1]
+    res = {}
+    for name, form in (("fp64", pq.FORM_FP64), ("mixed", pq.FORM_MIXED)):
+        ctx = make_context(d, form=form)
+        res[name] = pq.get_mo_basis_mo_value(ctx, P * mos).reshape(P, mos)
+        if name == "mixed":
+            res["vgl"] = pq.get_mo_basis_mo_vgl(ctx, P * 5 * mos).reshape(P, 5, mos)[:, 0, :]
+        pq.context_destroy(ctx)
+    scale = np.abs(res["fp64"]).max()
+    assert np.isfinite(res["mixed"]).all()
+    assert np.abs(res["mixed"] - res["fp64"]).max() / scale < MIXED_TOL
+    assert np.abs(res["mixed"] - res["vgl"]).max() / scale < MIXED_TOL
