@@ -197,6 +197,36 @@ qmckl_exit_code qmckl_get_forces_mo_g(qmckl_context context, double* const force
 qmckl_exit_code qmckl_get_forces_mo_g_inplace(qmckl_context context, double* const forces_mo_g, const int64_t size_max);
 qmckl_exit_code qmckl_get_forces_mo_l(qmckl_context context, double* const forces_mo_l, const int64_t size_max);
 
+/* ---- standalone AO helpers, one point, computed on the host ---- */
+/* P[i*ldp + k-1] = X[i]^k, k = 1..LMAX[i] (org/qmckl_ao.org:5971-6026; as there,
+ * n <= ldp is rejected with QMCKL_INVALID_ARG_2). */
+qmckl_exit_code qmckl_ao_power(const qmckl_context context, const int64_t n, const double* X, const int32_t* LMAX,
+                               double* const P, const int64_t ldp);
+/* VGL[c*ldv + i], c = value, d/dx, d/dy, d/dz, Laplacian of exp(-A[i] |X-R|^2)
+ * (org/qmckl_ao.org:3839-3910).  The reference's generated C prototype reads
+ * n, A and VGL as pointers; its bind(C) function takes n by value, A as input
+ * and VGL as output, which is the ABI declared here. */
+qmckl_exit_code qmckl_ao_gaussian_vgl(const qmckl_context context, const double* X, const double* R, const int64_t n,
+                                      const double* A, double* const VGL, const int64_t ldv);
+/* Cartesian monomials of X - R of degree <= lmax, L[m*ldl + {0,1,2}] their
+ * powers, *n their number (org/qmckl_ao.org:6195-6619, 6624-6914).
+ * Non-transposed forms: VGL[m*ldv + c]; transposed forms: VGL[c*ldv + m]. */
+qmckl_exit_code qmckl_ao_polynomial_vgl(const qmckl_context context, const double* X, const double* R,
+                                        const int32_t lmax, int64_t* n, int32_t* const L, const int64_t ldl,
+                                        double* const VGL, const int64_t ldv);
+qmckl_exit_code qmckl_ao_polynomial_vgl_doc(const qmckl_context context, const double* X, const double* R,
+                                            const int32_t lmax, int64_t* n, int32_t* const L, const int64_t ldl,
+                                            double* const VGL, const int64_t ldv);
+qmckl_exit_code qmckl_ao_polynomial_transp_vgl(const qmckl_context context, const double* X, const double* R,
+                                               const int32_t lmax, int64_t* n, int32_t* const L, const int64_t ldl,
+                                               double* const VGL, const int64_t ldv);
+qmckl_exit_code qmckl_ao_polynomial_transp_vgl_doc(const qmckl_context context, const double* X, const double* R,
+                                                   const int32_t lmax, int64_t* n, int32_t* const L,
+                                                   const int64_t ldl, double* const VGL, const int64_t ldv);
+qmckl_exit_code qmckl_ao_polynomial_transp_vgl_hpc(const qmckl_context context, const double* X, const double* R,
+                                                   const int32_t lmax, int64_t* n, int32_t* const L,
+                                                   const int64_t ldl, double* const VGL, const int64_t ldv);
+
 /* ---- MO basis: org/qmckl_mo.org:192-1747, 2362-2400, 3479 ---- */
 qmckl_exit_code qmckl_set_mo_basis_mo_num(qmckl_context context, const int64_t mo_num);
 qmckl_exit_code qmckl_set_mo_basis_coefficient(qmckl_context context, const double* coefficient, const int64_t size_max);

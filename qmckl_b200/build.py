@@ -20,7 +20,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 INC = ["-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
 CU_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", *ARCH, *INC]
-CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-I/usr/local/cuda/include", *INC]
+CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-ffp-contract=off", "-I/usr/local/cuda/include", *INC]
 
 
 def _sources():

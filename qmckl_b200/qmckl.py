@@ -326,6 +326,56 @@ get_forces_mo_g = _array_getter("qmckl_get_forces_mo_g")
 get_forces_mo_g_inplace = _array_getter("qmckl_get_forces_mo_g_inplace")
 get_forces_mo_l = _array_getter("qmckl_get_forces_mo_l")
 
+# ----------------------------------------------- standalone AO helpers
+
+
+def ao_power(ctx, X, LMAX, ldp):
+    """P[n][ldp], P[i][k-1] = X[i]**k for k = 1..LMAX[i] (entries past LMAX[i] are 0)."""
+    x, xp, n = _arr(X, np.float64)
+    lm, lp, _ = _arr(LMAX, np.int32)
+    P = np.zeros((x.size, ldp), dtype=np.float64)
+    _check(lib().qmckl_ao_power(C.c_int64(ctx), n, xp, lp, P.ctypes.data_as(C.c_void_p), C.c_int64(ldp)))
+    return P
+
+
+def ao_gaussian_vgl(ctx, X, R, A, ldv=None):
+    """VGL[5][ldv] of exp(-A[i] |X-R|^2): value, gradient, Laplacian."""
+    x, xp, _ = _arr(X, np.float64)
+    r, rp, _ = _arr(R, np.float64)
+    a, ap, n = _arr(A, np.float64)
+    ldv = a.size if ldv is None else ldv
+    VGL = np.zeros((5, max(ldv, 0)), dtype=np.float64)
+    _check(lib().qmckl_ao_gaussian_vgl(C.c_int64(ctx), xp, rp, n, ap, VGL.ctypes.data_as(C.c_void_p),
+                                       C.c_int64(ldv)))
+    return VGL
+
+
+def _polynomial(cname, transposed):
+    def f(ctx, X, R, lmax, ldl=3, ldv=None):
+        x, xp, _ = _arr(X, np.float64)
+        r, rp, _ = _arr(R, np.float64)
+        npoly = max(lmax + 1, 0) * (lmax + 2) * (lmax + 3) // 6
+        if ldv is None:
+            ldv = npoly if transposed else 5
+        L = np.zeros((max(npoly, 1), max(ldl, 0)), dtype=np.int32)
+        VGL = np.zeros((5, max(ldv, 0)) if transposed else (max(npoly, 1), max(ldv, 0)), dtype=np.float64)
+        n = C.c_int64(0)
+        _check(getattr(lib(), cname)(C.c_int64(ctx), xp, rp, C.c_int32(lmax), C.byref(n),
+                                     L.ctypes.data_as(C.c_void_p), C.c_int64(ldl),
+                                     VGL.ctypes.data_as(C.c_void_p), C.c_int64(ldv)))
+        return n.value, L, VGL
+    f.__name__ = cname[len("qmckl_"):]
+    f.__doc__ = (f"{cname}: (n, L[n][ldl], VGL) with VGL[5][ldv] (monomial m in column m)" if transposed else
+                 f"{cname}: (n, L[n][ldl], VGL) with VGL[n][ldv] (component c in column c)")
+    return f
+
+
+ao_polynomial_vgl = _polynomial("qmckl_ao_polynomial_vgl", False)
+ao_polynomial_vgl_doc = _polynomial("qmckl_ao_polynomial_vgl_doc", False)
+ao_polynomial_transp_vgl = _polynomial("qmckl_ao_polynomial_transp_vgl", True)
+ao_polynomial_transp_vgl_doc = _polynomial("qmckl_ao_polynomial_transp_vgl_doc", True)
+ao_polynomial_transp_vgl_hpc = _polynomial("qmckl_ao_polynomial_transp_vgl_hpc", True)
+
 # ------------------------------------------------------------- MO basis
 
 
