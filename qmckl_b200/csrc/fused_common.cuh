@@ -158,6 +158,23 @@ __device__ __forceinline__ void row_exponents(const RowBound& RB, const double* 
   }
 }
 
+// (c0, c1, c2, c3) with r^a = c0 + c1 r + c2 r^2 + c3 r^3, a = 0..3.
+static __constant__ float4 kAxisHot[4] = {{1.f, 0.f, 0.f, 0.f}, {0.f, 1.f, 0.f, 0.f}, {0.f, 0.f, 1.f, 0.f},
+                                          {0.f, 0.f, 0.f, 1.f}};
+
+// One axis of a cartesian monomial, exponent a <= 3 given by its one-hot
+// coefficients h: F0 = r^a, F1 = a r^(a-1), G = a (a-1) r^(a-2) / 2.  With
+// t2 = c3 r + c2 and t1 = t2 r + c1: F0 = t1 r + c0, F1 = (t2 + c3 r) r + t1,
+// G = 3 c3 r + c2.
+__device__ __forceinline__ void axis_factors(float r, float4 h, float& F0, float& F1, float& G) {
+  const float t2 = fmaf(h.w, r, h.z);
+  const float t1 = fmaf(t2, r, h.y);
+  F0 = fmaf(t1, r, h.x);
+  const float u = fmaf(h.w, r, t2);
+  F1 = fmaf(u, r, t1);
+  G = fmaf(h.w, r, u);
+}
+
 // Value, gradient and Laplacian of one AO from its shell's radial VGL (FP32).
 __device__ __forceinline__ void ao_product(int code, float f, const float (&s)[5], float x, float y, float z,
                                            float (&v)[5]) {
@@ -171,22 +188,23 @@ __device__ __forceinline__ void ao_product(int code, float f, const float (&s)[5
   if (l == 1) {
     P0 = ax ? x : (by ? y : z);
     P1 = (float)ax; P2 = (float)by; P3 = (float)cz; P4 = 0.f;
+  } else if (l <= 3) {
+    // Per axis, r^a and its first two derivatives as one cubic each, by
+    // Horner from the exponent's one-hot coefficients (a warp-uniform table
+    // lookup): no selects, no branches.
+    float X0, X1, XG, Y0, Y1, YG, Z0, Z1, ZG;
+    axis_factors(x, kAxisHot[ax & 3], X0, X1, XG);
+    axis_factors(y, kAxisHot[by & 3], Y0, Y1, YG);
+    axis_factors(z, kAxisHot[cz & 3], Z0, Z1, ZG);
+    const float xy = X0 * Y0, yz = Y0 * Z0, xz = X0 * Z0;
+    P0 = xy * Z0;
+    P1 = X1 * yz; P2 = Y1 * xz; P3 = Z1 * xy;
+    P4 = 2.f * (XG * yz + YG * xz + ZG * xy);
   } else {
     float pa = 1.f, pb = 1.f, pc = 1.f, pa1 = 1.f, pb1 = 1.f, pc1 = 1.f, pa2 = 1.f, pb2 = 1.f, pc2 = 1.f;
-    if (l <= 3) {   // branch-free powers
-      const float x2 = x * x, y2 = y * y, z2 = z * z;
-      const float xs[4] = {1.f, x, x2, x2 * x}, ys[4] = {1.f, y, y2, y2 * y}, zs[4] = {1.f, z, z2, z2 * z};
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        if (ax == q) { pa = xs[q]; pa1 = q >= 1 ? xs[q - 1] : 1.f; pa2 = q >= 2 ? xs[q - 2] : 1.f; }
-        if (by == q) { pb = ys[q]; pb1 = q >= 1 ? ys[q - 1] : 1.f; pb2 = q >= 2 ? ys[q - 2] : 1.f; }
-        if (cz == q) { pc = zs[q]; pc1 = q >= 1 ? zs[q - 1] : 1.f; pc2 = q >= 2 ? zs[q - 2] : 1.f; }
-      }
-    } else {
-      for (int i = 0; i < ax; ++i) { pa2 = pa1; pa1 = pa; pa *= x; }
-      for (int i = 0; i < by; ++i) { pb2 = pb1; pb1 = pb; pb *= y; }
-      for (int i = 0; i < cz; ++i) { pc2 = pc1; pc1 = pc; pc *= z; }
-    }
+    for (int i = 0; i < ax; ++i) { pa2 = pa1; pa1 = pa; pa *= x; }
+    for (int i = 0; i < by; ++i) { pb2 = pb1; pb1 = pb; pb *= y; }
+    for (int i = 0; i < cz; ++i) { pc2 = pc1; pc1 = pc; pc *= z; }
     float xy = pa * pb, yz = pb * pc, xz = pa * pc;
     P0 = xy * pc;
     xy *= (float)cz; xz *= (float)by; yz *= (float)ax;
