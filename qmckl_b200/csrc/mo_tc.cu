@@ -639,16 +639,16 @@ TcPlan tc_plan(int64_t ao_num, int64_t mo_num, int pieces) {
 
 TcPlan tc_plan_fused(int64_t ao_num, int64_t mo_num, int pieces) {
   TcPlan p = tc_plan(ao_num, mo_num, pieces);
-  // QMCKL_B200_WIDE_TILES: unset, wide tiles when they take fewer MO tiles;
-  // "0", never; "1", whenever they fit
+  // QMCKL_B200_WIDE_TILES: unset, wide tiles when they take fewer MO tiles,
+  // or as many with three A stages; "0", never; "1", whenever they fit
   const char* env = std::getenv("QMCKL_B200_WIDE_TILES");
   const bool never = env != nullptr && std::strcmp(env, "0") == 0;
   const bool always = env != nullptr && std::strcmp(env, "1") == 0;
-  if (pieces != 3 || never || (p.n_tiles < 2 && !always)) return p;
+  if (pieces != 3 || never) return p;
   // two accumulators of up to 256 columns fit TMEM (512); the single
   // coefficient tile (3 x 128 B per MO) fits beside the 48 KB A stages
   const int n_tiles = (int)((mo_num + 255) / 256);
-  if (n_tiles >= p.n_tiles && !always) return p;
+  if (n_tiles > p.n_tiles && !always) return p;
   const int64_t per = (mo_num + n_tiles - 1) / n_tiles;
   const int n_tile = (int)((per + 15) / 16 * 16);
   // shared memory: the A stages (48 KB each), the coefficient tile
@@ -659,6 +659,10 @@ TcPlan tc_plan_fused(int64_t ao_num, int64_t mo_num, int pieces) {
   if (bytes(3) <= 232448) nst = 3;
   else if (bytes(2) <= 232448) nst = 2;
   if (nst == 0) return p;
+  // As many tiles either way: the wide form wins only with its third stage
+  // (config-1 molecule, 160 MOs: 2.52 against 2.67 ms); with two it
+  // reloads its single coefficient tile between blocks for nothing.
+  if (n_tiles == p.n_tiles && nst < 3 && !always) return p;
   p.n_tiles = n_tiles;
   p.n_tile = n_tile;
   p.nacc = 2;

@@ -36,9 +36,10 @@ inline const double* tc_scales(const TcPlan& plan, const void* d_coef) {
 }
 
 TcPlan tc_plan(int64_t ao_num, int64_t mo_num, int pieces);
-// The fused kernel's plan: tc_plan's, or, when that takes several MO tiles
-// and wider ones would take fewer, tiles of up to 256 MOs with two
-// accumulators (QMCKL_B200_WIDE_TILES=0: never; =1: whenever they fit).
+// The fused kernel's plan (3 pieces): tiles of up to 256 MOs with two
+// accumulators when they take fewer MO tiles than tc_plan's, or as many with
+// three A stages (up to 176 MOs a tile); tc_plan's otherwise
+// (QMCKL_B200_WIDE_TILES=0: never; =1: whenever they fit).
 TcPlan tc_plan_fused(int64_t ao_num, int64_t mo_num, int pieces);
 size_t tc_a_bytes(const TcPlan& plan, int64_t rows);
 // coefficient [mo][ao] (host, FP64) -> split pieces and the scale block on
