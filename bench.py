@@ -632,6 +632,19 @@ def main():
         dist.destroy_process_group()
 
 
+def fused_n_tile(M):
+    """MO tile width of the fused kernel's plan with 3 pieces (mo_tc.cu
+    tc_plan_fused): tiles of up to 256 MOs when they take fewer tiles than
+    tiles of up to 160, or as many with three A stages (up to 176 MOs)."""
+    narrow = -(-M // 160)
+    nt = -(-M // 256)
+    n = -(-(-(-M // nt)) // 16) * 16
+    fits3 = 1024 + 3 * (49152 + 4096) + 384 * n + 3072 <= 232448
+    if nt < narrow or (nt == narrow and fits3):
+        return n
+    return -(-(-(-M // narrow)) // 16) * 16
+
+
 def mixed_roofline(args, P, A, M, ms, ks_eval, ks_total, bf16, peak_src):
     """Roofline of the mixed step's dominant kernel against the bf16 tensor peak.
 
@@ -641,18 +654,15 @@ def mixed_roofline(args, P, A, M, ms, ks_eval, ks_total, bf16, peak_src):
     6 split-BF16 products (3 for float16 x 2) per k-step.  Reported two ways:
     the issued MMA flops and the algorithmic split count (3 x 10 P A M)."""
     flops = 2.0 * 5 * P * A * M
-    n_tiles = -(-M // 256)
-    n_tile = -(-(-(-M // n_tiles)) // 16) * 16
-    while n_tile > 160:
-        n_tiles += 1
-        n_tile = -(-(-(-M // n_tiles)) // 16) * 16
+    n_tile = fused_n_tile(M) if args.pieces == 3 else -(-(-(-M // -(-M // 160))) // 16) * 16
     nprod = 6 if args.pieces == 3 else 3
     issued = 2.0 * (ks_eval / args.steps) * 128 * n_tile * 16 * nprod
     kname = ("fused_mo_kernel<3,5> (AO -> split-BF16 tcgen05 MO VGL" if args.pieces == 3 else
              "fused_mo_kernel<2,5> (AO -> split-FP16 tcgen05 MO VGL") + "; step = 3 ordering kernels + tile plan + this)"
     if args.unfused:
         # AO pieces to HBM, then 128-row tiles of the 5P x A pieces matrix x 6 products
-        issued = 2.0 * (-(-5 * P // 128) * 128) * (n_tile * n_tiles) * (-(-A // 64) * 64) * 6
+        nt = -(-M // 160)
+        issued = 2.0 * (-(-5 * P // 128) * 128) * (nt * (-(-(-(-M // nt)) // 16) * 16)) * (-(-A // 64) * 64) * 6
         kname = "ao_tile_kernel<3,5> + tc_gemm_kernel<3,2> (unfused mixed form; whole step)"
     split3 = 3.0 * flops
     achieved = issued / (ms * 1e-3) / 1e12
@@ -664,7 +674,7 @@ def mixed_roofline(args, P, A, M, ms, ks_eval, ks_total, bf16, peak_src):
         traffic_note = (f"DRAM read + write bytes of one launch from an ncu capture at {int(cap[0])} points "
                         f"(profiles/dram_traffic.txt){scaled}; the algorithmic bytes are the "
                         f"{40.0 * P * M / 1e9:.3f} GB of mo_vgl written + 24 P bytes of coordinates, of which "
-                        f"~56 MB are still dirty in L2 when the kernel ends (written back afterwards, "
+                        f"~59 MB are still dirty in L2 when the kernel ends (written back afterwards, "
                         f"uncounted in the launch)")
     return {"kernel": kname, "bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
             "frac": achieved / bf16, "peak_source": peak_src,
