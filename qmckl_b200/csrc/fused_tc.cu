@@ -24,8 +24,9 @@ using namespace tcx;
 
 using namespace fz;
 
-constexpr int kProdWarps = 16;   // one warp per 4-AO chunk of the 64-AO K block
-constexpr int kChunk = BK / kProdWarps;
+constexpr int kChunks = 16;      // 4-AO chunks of a 64-AO K block, 4 per 16-AO k-step
+constexpr int kChunk = BK / kChunks;
+constexpr int kProdWarps = 16;   // producer warps (a multiple of 4: the epilogue splits them by TMEM quadrant)
 constexpr int kProd = kProdWarps * 32;
 constexpr int kTmaWarp = kProdWarps;
 constexpr int kMmaWarp = kProdWarps + 1;
@@ -88,6 +89,7 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
   int* kflag = act + kblocks;                 // then: count, first block of each half, first block
   int* nact_p = kflag + kblocks;
   int* claim = nact_p + 4;                    // chunks claimed by the producer warps after their first
+  int* released = claim + 1;                  // K blocks whose MMAs the TMA thread has seen done
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int64_t p0 = (int64_t)blockIdx.x * PTS;
@@ -111,7 +113,7 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
   int tma_pre = 0;   // K blocks whose loads the TMA thread issued during the prologue
   if (tid == kTmaWarp * 32) {
     for (int s = 0; s < NST; ++s) {
-      for (int kk = 0; kk < kKsteps; ++kk) mbar_init(&full[s * kKsteps + kk], kProd / kKsteps);
+      for (int kk = 0; kk < kKsteps; ++kk) mbar_init(&full[s * kKsteps + kk], kChunks / kKsteps * 32);
       mbar_init(&bfull[s], 1);
       mbar_init(&empty[s], 1);
       mbar_init(&rec_full[s], 1);
@@ -138,7 +140,10 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
     if (d == 0) pidx[i] = q;
     rexp[t] = PIECES == 2 ? kExpMin : 0;
   }
-  if (tid == 0) *claim = 0;
+  if (tid == 0) {
+    *claim = 0;
+    *released = 0;
+  }
   if (tinfo != nullptr) {   // the tile's K-block list, made by tile_plan_kernel
     const int* ti = tinfo + (size_t)blockIdx.x * (kblocks + 4);
     for (int t = tid; t < kblocks + 4; t += kThreadsF) {
@@ -189,14 +194,20 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
     // claimed in order, so every chunk of a block is taken before any chunk
     // of a later block: a warp waiting for a stage waits only for blocks
     // whose chunks are all in progress.
-    // A chunk of a skipped k-step is never read by the MMAs: it waits for
-    // the stage only (so that every chunk of a block waits for the same
-    // barrier, which keeps any warp from claiming a chunk NST blocks past a
-    // stage still in use) and does not arrive; the MMA thread arrives for
-    // the whole skipped k-step.
-    const int total = nact * kProdWarps;
+    // A chunk of a skipped k-step is never read by the MMAs: it waits only
+    // until the MMAs of the block NST back are done (as every chunk does,
+    // which keeps any warp from claiming a chunk NST blocks past a stage
+    // still in use) and does not arrive; the MMA thread arrives for the
+    // whole skipped k-step.  Since the block's MMAs need none of its
+    // arrivals, they may finish before such a warp reaches its wait: a
+    // parity wait on the stage barrier alone would then read the barrier a
+    // phase late and wait for the stage's next use.  So its wait also ends
+    // when the count of blocks released (published by the TMA thread after
+    // its own waits on the same barriers, and only growing) shows the block
+    // NST back done.
+    const int total = nact * kChunks;
     for (int q = warp; q < total;) {
-      const int it = q / kProdWarps, c = q - it * kProdWarps;
+      const int it = q / kChunks, c = q - it * kChunks;
       const int s = it % NST;
       const uint32_t phase = (uint32_t)(it / NST) & 1u;
       const bool live = kstep_live(act[it], c, kChunk);
@@ -206,14 +217,17 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
       // for the same full[] barrier's phase of the block NST back, so no
       // phase of a barrier mixes the arrivals of two blocks and no parity
       // wait falls two phases behind.
-      bool ok = mbar_wait(&empty[s], phase ^ 1u, err, 11);
-      if (live) ok = ok && mbar_wait(&rec_full[s], phase, err, 15);
+      bool ok;
+      if (live)
+        ok = mbar_wait(&empty[s], phase ^ 1u, err, 11) && mbar_wait(&rec_full[s], phase, err, 15);
+      else
+        ok = mbar_wait_or_count(&empty[s], phase ^ 1u, released, it - NST + 1, err, 16);
       if (!__all_sync(0xffffffffu, ok)) break;
       if (live) {
         const uint32_t a_base = smem_addr(smem + s * STAGE);
         produce_kblock<PIECES, COMPS, kChunk>(recs + s * rec_bytes, pts, p0, P, cutoff, rexp, a_base, c, lane);
         fence_async_smem();
-        mbar_arrive(&full[s * kKsteps + c / (kProdWarps / kKsteps)]);
+        mbar_arrive(&full[s * kKsteps + c / (kChunks / kKsteps)]);
       }
       int nq = 0;
       if (lane == 0) nq = atomicAdd(claim, 1) + kProdWarps;
@@ -228,6 +242,7 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
           const uint32_t phase = (uint32_t)(it / NST) & 1u;
           // the stage, its record slot included: every MMA of block it - NST done
           if (!mbar_wait(&empty[s], phase ^ 1u, err, 12)) break;
+          if (it >= NST) *(volatile int*)released = it - NST + 1;
           load_record(it, act[it] & 0xFFFF);
           load_coef(it, act[it] & 0xFFFF);
         }
@@ -239,6 +254,7 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
         for (int it = 1; it < nact; ++it) {
           const int b = it - 1;
           if (!mbar_wait(&empty[b % NST], (uint32_t)(b / NST) & 1u, err, 12)) break;
+          *(volatile int*)released = it;
           load_coef(it, act[it] & 0xFFFF);
           const int r = it + NST - 1;   // its record slot is block it - 1's
           if (r < nact && r >= tma_pre) load_record(r, act[r] & 0xFFFF);
@@ -264,7 +280,7 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
         bool ok = true;
         for (int kk = 0; kk < kKsteps; ++kk) {
           const bool kl = ((kmask >> kk) & 1u) != 0u;
-          if (!kl) mbar_arrive_n(&full[s * kKsteps + kk], (uint32_t)(kProd / kKsteps));
+          if (!kl) mbar_arrive_n(&full[s * kKsteps + kk], (uint32_t)(kChunks / kKsteps * 32));
           if (!mbar_wait(&full[s * kKsteps + kk], phase, err, 13)) {
             ok = false;
             break;
@@ -421,7 +437,7 @@ size_t fused_smem(int n_tile, int rec_bytes, int kblocks) {
   const size_t stage_mem = NACC == 3 ? NST * ((size_t)PIECES * A_TILE + b_tile) : NST * (size_t)PIECES * A_TILE + b_tile;
   return 1024 + stage_mem + (size_t)NST * rec_bytes + ((kKsteps + 3) * NST + 2) * 8 + 4 * PTS * 8 +
          3 * PTS * 4 +
-         (size_t)(2 * kblocks + 5) * 4 + 16;
+         (size_t)(2 * kblocks + 6) * 4 + 16;
 }
 
 template <int PIECES, int COMPS, int NACC, int NST>

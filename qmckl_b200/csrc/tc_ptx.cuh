@@ -156,6 +156,33 @@ __device__ __forceinline__ void mbar_arrive_n(uint64_t* bar, uint32_t count) {
 
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
+// Bounded wait for the phase of parity `parity` of `bar`, or for the counter
+// `cnt` (shared memory, written by another thread of the CTA) to reach
+// `target`, whichever is seen first.  A parity wait alone cannot tell a
+// phase that completed from the one after it; a counter that only grows,
+// published when that phase completed, can.  The counter is read every 16th
+// poll only: it decides the rare wait that started a phase late, and the
+// barrier's own suspending wait stays the common path.  false, with `code`
+// recorded, when the deadline passes or the grid already failed.
+__device__ __forceinline__ bool mbar_wait_or_count(uint64_t* bar, uint32_t parity, const int* cnt, int target,
+                                                   int* err, int code) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer();
+  uint32_t spins = 0;
+  while (true) {
+    if (mbar_try_wait(bar, parity)) return true;
+    ++spins;
+    if ((spins & 15u) == 0 && *(const volatile int*)cnt >= target) return true;
+    if ((spins & 255u) == 0) {
+      if (*(volatile int*)err != 0) return false;
+      if (globaltimer() - t0 > kWaitNs) {
+        atomicCAS(err, 0, code);
+        return false;
+      }
+    }
+  }
+}
+
 __device__ __forceinline__ void st_shared_v2(uint32_t addr, uint32_t a, uint32_t b) {
   asm volatile("st.shared.v2.b32 [%0], {%1, %2};" ::"r"(addr), "r"(a), "r"(b) : "memory");
 }

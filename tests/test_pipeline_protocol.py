@@ -18,12 +18,19 @@ adversarial schedules and checks, for every schedule:
   block no longer needs it.
 
 Forms: three accumulators (two stages, a coefficient tile per stage) and
-wide MO tiles (a single coefficient tile, two or three stages).  A variant
+wide MO tiles (a single coefficient tile, two or three stages).  Schedules:
+random, adversarial (each actor moves with probability 0.15 a step), and
+with one producer warp held back until nothing else can move.  Two variants
 known to be wrong must be caught: chunks of skipped k-steps arriving
 themselves without waiting for the record, while each record is loaded as
 soon as every chunk of the block two back has arrived (a skipped chunk of a
 later block can then arrive before the TMA thread's parity wait for the
-earlier phase, which falls two phases behind).
+earlier phase, which falls two phases behind); and chunks of skipped
+k-steps waiting on the stage barrier's parity alone (the block's MMAs need
+none of their arrivals, so a warp held back can reach its wait after the
+phase it waits for and the next have completed, and waits for the stage's
+next use; the kernel's wait also ends on the count of released blocks that
+the TMA thread publishes).
 """
 import random
 
@@ -64,17 +71,20 @@ class Bar:
             self.phase += 1
             self.pending, self.tags = self.count, []
 
-    def wait(self, k):
-        """A parity wait for phase k (k < 0: the phase before the first)."""
+    def wait(self, k, late_ok=False):
+        """A parity wait for phase k (k < 0: the phase before the first).
+        late_ok: the caller also ends its wait by other means (a counter),
+        so a parity wait that reads the barrier a phase late is no fault."""
         passed = (self.phase & 1) != (k & 1)
         if passed and self.phase <= k:
             raise ProtocolViolation(f"{self.name}: wait for phase {k} passed in phase {self.phase}")
-        if not passed and self.phase > k:
+        if not passed and self.phase > k and not late_ok:
             raise ProtocolViolation(f"{self.name}: wait for completed phase {k} blocked in phase {self.phase}")
         return passed
 
 
-def run(masks, seed, nst=2, wide=False, adversarial=False, bad_variant=False):
+def run(masks, seed, nst=2, wide=False, adversarial=False, bad_variant=False, warps=WARPS, dead_parity=False,
+        late=None):
     rng = random.Random(seed)
     n = len(masks)
     full = [[Bar(f"full[{s}][{k}]", PER_K) for k in range(KSTEPS)] for s in range(nst)]
@@ -85,8 +95,9 @@ def run(masks, seed, nst=2, wide=False, adversarial=False, bad_variant=False):
     b_tile = {}                                    # coefficient buffer -> block
     rec_slot = [None] * nst
     mma_done, produced = set(), {}
-    pending, claim = [], [WARPS]
+    pending, claim = [], [warps]
     clock = [0]
+    released = [0]   # blocks whose MMAs the TMA thread has seen done (a counter in shared memory)
 
     def live(it, c):
         m = masks[it] or 0xF
@@ -120,7 +131,10 @@ def run(masks, seed, nst=2, wide=False, adversarial=False, bad_variant=False):
         while q < n * CHUNKS:
             it, c = divmod(q, CHUNKS)
             s, k = it % nst, it // nst
-            yield lambda: empty[s].wait(k - 1)
+            if live(it, c) or dead_parity or bad_variant:
+                yield lambda: empty[s].wait(k - 1)
+            else:   # a chunk of a skipped k-step: the stage barrier, or the count of released blocks
+                yield lambda: empty[s].wait(k - 1, late_ok=True) or released[0] >= it - nst + 1
             if live(it, c):
                 yield lambda: rec[s].wait(k)
                 if it >= nst and (it - nst) not in mma_done:
@@ -151,6 +165,7 @@ def run(masks, seed, nst=2, wide=False, adversarial=False, bad_variant=False):
                         yield lambda kk=kk: full[s][kk].wait(k - 1)
                     load_record(it)
                 yield lambda: empty[s].wait(k - 1)
+                released[0] = it - nst + 1
                 if not bad_variant:
                     load_record(it)
                 load_coef(it)
@@ -158,6 +173,7 @@ def run(masks, seed, nst=2, wide=False, adversarial=False, bad_variant=False):
             for it in range(1, n):
                 b = it - 1
                 yield lambda: empty[b % nst].wait(b // nst)
+                released[0] = it
                 load_coef(it)
                 r = it + nst - 1
                 if pre <= r < n:
@@ -181,7 +197,7 @@ def run(masks, seed, nst=2, wide=False, adversarial=False, bad_variant=False):
                 empty[s].arrive()
             pending.append((clock[0] + rng.randint(1, 10), done))
 
-    actors = [producer(w) for w in range(WARPS)] + [tma(), mma()]
+    actors = [producer(w) for w in range(warps)] + [tma(), mma()]
     cur = [next(a, None) for a in actors]
     while True:
         clock[0] += 1
@@ -190,7 +206,7 @@ def run(masks, seed, nst=2, wide=False, adversarial=False, bad_variant=False):
         for _, f in due:
             f()
         moved = False
-        order = list(range(len(actors)))
+        order = [i for i in range(len(actors)) if i != late]
         rng.shuffle(order)
         for i in order:
             if adversarial and rng.random() > 0.15:
@@ -200,6 +216,10 @@ def run(masks, seed, nst=2, wide=False, adversarial=False, bad_variant=False):
                 moved = True
                 if rng.random() < 0.5:
                     break
+        if late is not None and not moved and not pending:   # the late warp runs only when all else waits
+            while cur[late] is not None and cur[late]():
+                cur[late] = next(actors[late], None)
+                moved = True
         if all(c is None for c in cur) and not pending:
             return
         if not moved and not pending and not any(c is not None and c() for c in cur):
@@ -217,11 +237,29 @@ def test_protocol_holds(nst, wide, adversarial):
         run(_masks(random.Random(seed)), seed, nst=nst, wide=wide, adversarial=adversarial)
 
 
+@pytest.mark.parametrize("nst,wide", [(2, False), (2, True), (3, True)])
+@pytest.mark.parametrize("late", [0, 3, 9])
+def test_protocol_holds_with_a_warp_held_back(nst, wide, late):
+    for seed in range(40):
+        run(_masks(random.Random(seed)), seed, nst=nst, wide=wide, adversarial=seed % 2 == 0, late=late)
+
+
 def test_known_bad_variant_is_caught():
     failures = 0
     for seed in range(150):
         try:
             run(_masks(random.Random(seed)), seed, nst=2, bad_variant=True)
         except ProtocolViolation:
+            failures += 1
+    assert failures > 0
+
+
+def test_parity_only_wait_of_skipped_chunks_is_caught():
+    failures = 0
+    for seed in range(40):
+        try:
+            run(_masks(random.Random(seed)), seed, nst=3, wide=True, dead_parity=True, late=0)
+        except ProtocolViolation as e:
+            assert "blocked" in str(e)
             failures += 1
     assert failures > 0
