@@ -190,6 +190,14 @@ qmckl_exit_code qmckl_b200_get_kblock_stats(qmckl_context context, int64_t* eval
  * evaluation of the context first (QMCKL_NOT_PROVIDED otherwise). */
 qmckl_exit_code qmckl_b200_inject_wait_failure(qmckl_context context, const int32_t code);
 
+/* Test hook: in the fused mixed-form VGL kernel (3 pieces) launched after
+ * this call, in this process, every producer warp holding a chunk of a
+ * skipped 16-AO k-step sleeps `ns` nanoseconds (0 <= ns <= 1e7; 0 = off, the
+ * default, which launches the kernel without the sleep) before it waits for
+ * its pipeline stage, so that its block's MMAs can complete before that wait
+ * starts.  The results must not change. */
+qmckl_exit_code qmckl_b200_inject_late_warps(const int64_t ns);
+
 /* Number of kernels this library launched since the process started. */
 int64_t qmckl_b200_kernel_launch_count(void);
 

@@ -1577,6 +1577,11 @@ qmckl_exit_code qmckl_b200_inject_wait_failure(qmckl_context context, const int3
   return QMCKL_SUCCESS;
 }
 
+qmckl_exit_code qmckl_b200_inject_late_warps(const int64_t ns) {
+  if (ns < 0 || ns > 10000000) return QMCKL_INVALID_ARG_1;
+  return tc_set_late_warps((unsigned int)ns) == cudaSuccess ? QMCKL_SUCCESS : QMCKL_FAILURE;
+}
+
 static qmckl_exit_code device_entry(qmckl_context context, const char* fname, int64_t point_num,
                                     const double* d_coord, void* d_out, bool need_mo) {
   if (qmckl_context_check(context) == QMCKL_NULL_CONTEXT) return QMCKL_INVALID_CONTEXT;

@@ -39,6 +39,12 @@ constexpr int kKsteps = BK / UMMA_K;   // 16-AO k-steps per K block, 4 producer 
 // all beyond their radius at every point of the tile contributes exact zeros
 // and is left out of the producer, TMA and MMA loops.
 
+// Test hook (qmckl_b200_inject_late_warps): nanoseconds that every producer
+// warp holding a chunk of a skipped k-step sleeps before its stage wait, so
+// that the MMAs of its block can complete first.  Non-zero selects the LATE
+// instantiation of the kernel (3 pieces, VGL); the others compile it out.
+unsigned int g_late_warp_ns = 0u;
+
 // NACC = 3: three accumulators of n_tile <= 160 columns (the leading
 // product in two halves of K, the corrections), each stage holding its A
 // and coefficient tiles.  NACC = 2 (wide MO tiles, n_tile <= 256, with a tile
@@ -47,7 +53,7 @@ constexpr int kKsteps = BK / UMMA_K;   // 16-AO k-steps per K block, 4 producer 
 // they fit, else two), loaded for block it once the MMAs of block it - 1 are
 // done; the epilogue writes the tile in column passes that fit the idle
 // stage memory.
-template <int PIECES, int COMPS, int NACC, int NST>
+template <int PIECES, int COMPS, int NACC, int NST, bool LATE = false>
 __global__ void __launch_bounds__(kThreadsF, 1)
 fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, const int64_t P,
                 const double* __restrict__ coord, const double cutoff, const int n_out, const int n_tile,
@@ -55,7 +61,7 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
                 const int* __restrict__ perm, const double* __restrict__ scales, const RowBound rb,
                 double* __restrict__ out, int* __restrict__ err, const int64_t cstride,
                 const uint8_t* __restrict__ kskip, unsigned long long* __restrict__ kstat,
-                const double* __restrict__ tpts, const int* __restrict__ tinfo) {
+                const double* __restrict__ tpts, const int* __restrict__ tinfo, const unsigned int late_ns) {
   constexpr int PTS = BM / COMPS;            // 25 points (VGL) or 128 (value)
   // NST stages of the A tiles: 2 for NACC = 3 (each with its coefficient
   // tile), 2 or 3 for wide MO tiles
@@ -218,10 +224,13 @@ fused_mo_kernel(const DevTables T, const __grid_constant__ CUtensorMap tmB, cons
       // phase of a barrier mixes the arrivals of two blocks and no parity
       // wait falls two phases behind.
       bool ok;
-      if (live)
+      if (live) {
         ok = mbar_wait(&empty[s], phase ^ 1u, err, 11) && mbar_wait(&rec_full[s], phase, err, 15);
-      else
+      } else {
+        if constexpr (LATE)
+          for (unsigned int t = 0; t < late_ns; t += 1000u) __nanosleep(1000u);
         ok = mbar_wait_or_count(&empty[s], phase ^ 1u, released, it - NST + 1, err, 16);
+      }
       if (!__all_sync(0xffffffffu, ok)) break;
       if (live) {
         const uint32_t a_base = smem_addr(smem + s * STAGE);
@@ -449,6 +458,9 @@ cudaError_t launch_fused(const DevTables& T, const CUtensorMap& tb, int64_t P, c
   constexpr int PTS = BM / COMPS;
   const size_t smem = fused_smem<PIECES, COMPS, NACC, NST>(n_tile, rec_bytes, kblocks);
   auto kern = fused_mo_kernel<PIECES, COMPS, NACC, NST>;
+  const unsigned int late_ns = g_late_warp_ns;
+  if constexpr (PIECES == 3 && COMPS == 5)
+    if (late_ns != 0u) kern = fused_mo_kernel<PIECES, COMPS, NACC, NST, true>;
   if (NACC == 2 && tplan == nullptr) return cudaErrorInvalidValue;   // the wide form needs a tile plan
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -465,7 +477,7 @@ cudaError_t launch_fused(const DevTables& T, const CUtensorMap& tb, int64_t P, c
   }
   dim3 grid((unsigned)tiles, (unsigned)n_tiles);
   kern<<<grid, kThreadsF, smem, s>>>(T, tb, P, coord, cutoff, n_out, n_tile, kblocks, krec, rec_bytes, perm, scales,
-                                     rb, out, err, cstride, kskip, kstat, tpts, tinfo);
+                                     rb, out, err, cstride, kskip, kstat, tpts, tinfo, late_ns);
   count_launch();
   return cudaGetLastError();
 }
@@ -548,6 +560,11 @@ cudaError_t tc_run_fused(const DevTables& T, const TcPlan& plan, int64_t point_n
   // a timed-out barrier wait stays in *err for the caller's next synchronization
   return tc_launch_fused(plan, point_num, comps, coord, cutoff, tb, krec, rec_bytes, perm, d_coef, rb, out, err, s,
                          cstride, kskip, kstat, tplan);
+}
+
+cudaError_t tc_set_late_warps(unsigned int ns) {
+  g_late_warp_ns = ns;
+  return cudaSuccess;
 }
 
 }  // namespace qb

@@ -94,6 +94,10 @@ cudaError_t tc_launch_fused(const TcPlan& plan, int64_t point_num, int comps, co
                             const CUtensorMap& map, const void* krec, int rec_bytes, const int* perm, const void* d_coef,
                             const fz::RowBound& rb, double* out, int* err, cudaStream_t s, int64_t cstride = -1,
                             const void* kskip = nullptr, unsigned long long* kstat = nullptr, void* tplan = nullptr);
+// Test hook of the fused kernel (3 pieces, VGL), for the launches that follow
+// in this process: producer warps holding a chunk of a skipped k-step sleep
+// `ns` nanoseconds before their stage wait (0: off, the kernel without it).
+cudaError_t tc_set_late_warps(unsigned int ns);
 // Spatial order of points (32^3 cells over [box_lo, box_hi], Morton order) by
 // a counting sort: perm[P]; keys[P] and counts[kSortCells + 1] are scratch.
 // cstride: distance between the x, y and z blocks of coord (default

@@ -500,6 +500,12 @@ def b200_inject_alloc_failure(n):
     lib().qmckl_b200_inject_alloc_failure(C.c_int64(n))
 
 
+def b200_inject_late_warps(ns):
+    f = lib().qmckl_b200_inject_late_warps
+    f.restype = C.c_int32
+    _check(f(C.c_int64(ns)))
+
+
 def b200_inject_wait_failure(ctx, code):
     """Test hook: mark the context's tensor-core error word as a bounded wait that gave up."""
     _call("qmckl_b200_inject_wait_failure", ctx, C.c_int32(code))

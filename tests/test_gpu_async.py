@@ -79,3 +79,36 @@ def test_wait_failure_is_reported_by_the_host_getter():
         pq.get_mo_basis_mo_vgl(ctx, P * 5 * M)
     assert np.array_equal(pq.get_mo_basis_mo_vgl(ctx, P * 5 * M), good)
     pq.context_destroy(ctx)
+
+
+@pytest.mark.parametrize("cfg", [0, 1])
+def test_late_warps_leave_the_results_unchanged(cfg):
+    """Producer warps holding a chunk of a skipped 16-AO k-step sleep before
+    their stage wait (test hook), so the MMAs of their block, and on the
+    two-block tiles of config 0 (three stages) every MMA of the tile, can
+    complete before that wait starts: a parity wait alone would then wait for
+    a stage use that never comes.  The fused kernel ends such waits on the
+    count of released blocks: no wait gives up and the results are the same
+    to the last bit."""
+    import torch
+    d = gen.config(0) if cfg == 0 else gen.config(1, walk_num=2)
+    P = d["elec_coord"].shape[0] * d["elec_coord"].shape[1]
+    M = d["mo_num"]
+    ctx = make_context(d, points=False, form=pq.FORM_MIXED)
+    dc = torch.tensor(np.ascontiguousarray(gen.points(d).T), dtype=torch.float64, device="cuda")
+    out = torch.full((P * 5 * M,), float("nan"), dtype=torch.float64, device="cuda")
+    pq.b200_mo_vgl_device(ctx, P, dc.data_ptr(), out.data_ptr())
+    pq.b200_synchronize(ctx)
+    good = out.clone()
+    evaluated, total = pq.b200_get_kblock_stats(ctx, reset=True)
+    assert 0 < evaluated < total   # some k-steps are skipped
+    pq.b200_inject_late_warps(100_000)
+    try:
+        for _ in range(3):
+            out.fill_(float("nan"))
+            pq.b200_mo_vgl_device(ctx, P, dc.data_ptr(), out.data_ptr())
+            pq.b200_synchronize(ctx)   # raises if a bounded wait gave up
+            assert torch.equal(out, good)
+    finally:
+        pq.b200_inject_late_warps(0)
+    pq.context_destroy(ctx)
