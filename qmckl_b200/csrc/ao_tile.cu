@@ -15,6 +15,7 @@
 #include <cuda_bf16.h>
 
 #include "ao_tile.cuh"
+#include "monomial.cuh"
 #include "split.cuh"
 
 namespace qb {
@@ -94,6 +95,13 @@ __device__ __forceinline__ void ao_vgl_one(int code, R f, const R* s, R x, R y, 
   if (l == 1) {
     P[0] = (a ? x : (b ? y : z)) + shift;
     P[1] = R(a); P[2] = R(b); P[3] = R(c); P[4] = R(0);
+  } else if (std::is_same<R, float>::value && l <= 3) {
+    // FP32 (mixed form): the three cubics by Horner of monomial.cuh
+    float Pf[5];
+    monomial_horner(a, b, c, (float)x, (float)y, (float)z, Pf);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) P[q] = (R)Pf[q];
+    P[0] += shift;
   } else {
     monomial<R>(a, b, c, x, y, z, shift, P);
   }

@@ -21,6 +21,7 @@
 #include <cuda.h>
 #include <cuda_bf16.h>
 
+#include "monomial.cuh"
 #include "split.cuh"
 #include "tc_ptx.cuh"
 
@@ -158,23 +159,6 @@ __device__ __forceinline__ void row_exponents(const RowBound& RB, const double* 
   }
 }
 
-// (c0, c1, c2, c3) with r^a = c0 + c1 r + c2 r^2 + c3 r^3, a = 0..3.
-static __constant__ float4 kAxisHot[4] = {{1.f, 0.f, 0.f, 0.f}, {0.f, 1.f, 0.f, 0.f}, {0.f, 0.f, 1.f, 0.f},
-                                          {0.f, 0.f, 0.f, 1.f}};
-
-// One axis of a cartesian monomial, exponent a <= 3 given by its one-hot
-// coefficients h: F0 = r^a, F1 = a r^(a-1), G = a (a-1) r^(a-2) / 2.  With
-// t2 = c3 r + c2 and t1 = t2 r + c1: F0 = t1 r + c0, F1 = (t2 + c3 r) r + t1,
-// G = 3 c3 r + c2.
-__device__ __forceinline__ void axis_factors(float r, float4 h, float& F0, float& F1, float& G) {
-  const float t2 = fmaf(h.w, r, h.z);
-  const float t1 = fmaf(t2, r, h.y);
-  F0 = fmaf(t1, r, h.x);
-  const float u = fmaf(h.w, r, t2);
-  F1 = fmaf(u, r, t1);
-  G = fmaf(h.w, r, u);
-}
-
 // Value, gradient and Laplacian of one AO from its shell's radial VGL (FP32).
 __device__ __forceinline__ void ao_product(int code, float f, const float (&s)[5], float x, float y, float z,
                                            float (&v)[5]) {
@@ -191,7 +175,7 @@ __device__ __forceinline__ void ao_product(int code, float f, const float (&s)[5
   } else if (l <= 3) {
     // Per axis, r^a and its first two derivatives as one cubic each, by
     // Horner from the exponent's one-hot coefficients (a warp-uniform table
-    // lookup): no selects, no branches.
+    // lookup, monomial.cuh): no selects, no branches.
     float X0, X1, XG, Y0, Y1, YG, Z0, Z1, ZG;
     axis_factors(x, kAxisHot[ax & 3], X0, X1, XG);
     axis_factors(y, kAxisHot[by & 3], Y0, Y1, YG);
