@@ -209,7 +209,8 @@ qmckl_exit_code qmckl_ao_power(const qmckl_context context, const int64_t n, con
 qmckl_exit_code qmckl_ao_gaussian_vgl(const qmckl_context context, const double* X, const double* R, const int64_t n,
                                       const double* A, double* const VGL, const int64_t ldv);
 /* Cartesian monomials of X - R of degree <= lmax, L[m*ldl + {0,1,2}] their
- * powers, *n their number (org/qmckl_ao.org:6195-6619, 6624-6914).
+ * powers, *n their number (org/qmckl_ao.org:6195-6619, 6624-6914); lmax
+ * outside 0..1000 gives QMCKL_INVALID_ARG_4.
  * Non-transposed forms: VGL[m*ldv + c]; transposed forms: VGL[c*ldv + m]. */
 qmckl_exit_code qmckl_ao_polynomial_vgl(const qmckl_context context, const double* X, const double* R,
                                         const int32_t lmax, int64_t* n, int32_t* const L, const int64_t ldl,

@@ -25,6 +25,7 @@
 namespace {
 
 constexpr double kShift = 1.e-20;
+constexpr int32_t kMaxL = 1000;
 
 inline int64_t npoly(int32_t lmax) { return (int64_t)(lmax + 1) * (lmax + 2) * (lmax + 3) / 6; }
 
@@ -112,7 +113,10 @@ void monomials(const Form& f, const double* X, const double* R, int32_t lmax, in
 qmckl_exit_code check_poly(qmckl_context context, const double* X, const double* R, int32_t lmax, int64_t* n,
                            int32_t* L, int64_t ldl, double* VGL, int64_t ldv, int64_t ldv_min) {
   if (context == QMCKL_NULL_CONTEXT) return QMCKL_INVALID_CONTEXT;
-  if (lmax < 0) return QMCKL_INVALID_ARG_4;
+  // lmax above kMaxL (1.7e8 monomials) is refused rather than left to an
+  // allocation or, near 2e6, an overflowing count; the reference's own
+  // transposed doc form holds powers up to 21 only
+  if (lmax < 0 || lmax > kMaxL) return QMCKL_INVALID_ARG_4;
   if (ldl < 3) return QMCKL_INVALID_ARG_7;
   if (ldv < ldv_min) return QMCKL_INVALID_ARG_9;
   if (X == nullptr) return QMCKL_INVALID_ARG_2;
@@ -195,7 +199,8 @@ qmckl_exit_code qmckl_ao_polynomial_vgl(const qmckl_context context, const doubl
 qmckl_exit_code qmckl_ao_polynomial_transp_vgl_doc(const qmckl_context context, const double* X, const double* R,
                                                    const int32_t lmax, int64_t* n, int32_t* const L,
                                                    const int64_t ldl, double* const VGL, const int64_t ldv) {
-  const qmckl_exit_code rc = check_poly(context, X, R, lmax, n, L, ldl, VGL, ldv, lmax < 0 ? 0 : npoly(lmax));
+  const qmckl_exit_code rc =
+      check_poly(context, X, R, lmax, n, L, ldl, VGL, ldv, lmax < 0 || lmax > kMaxL ? 0 : npoly(lmax));
   if (rc != QMCKL_SUCCESS) return rc;
   monomials(Form{false, false, ldv, 1}, X, R, lmax, n, L, ldl, VGL);
   return QMCKL_SUCCESS;
@@ -204,7 +209,8 @@ qmckl_exit_code qmckl_ao_polynomial_transp_vgl_doc(const qmckl_context context, 
 qmckl_exit_code qmckl_ao_polynomial_transp_vgl_hpc(const qmckl_context context, const double* X, const double* R,
                                                    const int32_t lmax, int64_t* n, int32_t* const L,
                                                    const int64_t ldl, double* const VGL, const int64_t ldv) {
-  const qmckl_exit_code rc = check_poly(context, X, R, lmax, n, L, ldl, VGL, ldv, lmax < 0 ? 0 : npoly(lmax));
+  const qmckl_exit_code rc =
+      check_poly(context, X, R, lmax, n, L, ldl, VGL, ldv, lmax < 0 || lmax > kMaxL ? 0 : npoly(lmax));
   if (rc != QMCKL_SUCCESS) return rc;
   monomials(Form{false, true, ldv, 1}, X, R, lmax, n, L, ldl, VGL);
   return QMCKL_SUCCESS;

@@ -13,6 +13,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <atomic>
 
 #include "fused_common.cuh"
 #include "mo_tc.cuh"
@@ -43,7 +44,7 @@ constexpr int kKsteps = BK / UMMA_K;   // 16-AO k-steps per K block, 4 producer 
 // warp holding a chunk of a skipped k-step sleeps before its stage wait, so
 // that the MMAs of its block can complete first.  Non-zero selects the LATE
 // instantiation of the kernel (3 pieces, VGL); the others compile it out.
-unsigned int g_late_warp_ns = 0u;
+std::atomic<unsigned int> g_late_warp_ns{0u};
 
 // NACC = 3: three accumulators of n_tile <= 160 columns (the leading
 // product in two halves of K, the corrections), each stage holding its A
@@ -458,7 +459,7 @@ cudaError_t launch_fused(const DevTables& T, const CUtensorMap& tb, int64_t P, c
   constexpr int PTS = BM / COMPS;
   const size_t smem = fused_smem<PIECES, COMPS, NACC, NST>(n_tile, rec_bytes, kblocks);
   auto kern = fused_mo_kernel<PIECES, COMPS, NACC, NST>;
-  const unsigned int late_ns = g_late_warp_ns;
+  const unsigned int late_ns = g_late_warp_ns.load(std::memory_order_relaxed);
   if constexpr (PIECES == 3 && COMPS == 5)
     if (late_ns != 0u) kern = fused_mo_kernel<PIECES, COMPS, NACC, NST, true>;
   if (NACC == 2 && tplan == nullptr) return cudaErrorInvalidValue;   // the wide form needs a tile plan
@@ -563,7 +564,7 @@ cudaError_t tc_run_fused(const DevTables& T, const TcPlan& plan, int64_t point_n
 }
 
 cudaError_t tc_set_late_warps(unsigned int ns) {
-  g_late_warp_ns = ns;
+  g_late_warp_ns.store(ns, std::memory_order_relaxed);
   return cudaSuccess;
 }
 

@@ -190,6 +190,7 @@ def test_polynomial_error_codes(ctx):
         assert rc(name) == 0 and n.value == 10
         assert rc(name, c=0) == 103                 # QMCKL_INVALID_CONTEXT
         assert rc(name, lmax=-1) == 4
+        assert rc(name, lmax=1001) == 4
         assert rc(name, ldl=2) == 7
         assert rc(name, ldv=4) == 9                 # < 5 (doc) and < 10 monomials (transposed)
         assert rc(name, x=None) == 2
