@@ -2,12 +2,13 @@
 // leaves the SM.  One CTA per (tile of points, N tile of MOs); the shared
 // device pieces (AO production into swizzled split-BF16 tiles, MMA chain,
 // epilogue) and their arithmetic are described in fused_common.cuh.
-// Warp roles: warps 0..15 produce the AO pieces of each 64-AO K block (4 AOs
-// per warp, lanes = points); warp 16 bulk-copies the block's record and
-// TMA-loads the coefficient pieces; warp 17 owns TMEM and issues the MMAs;
-// the 16 producer warps then run the epilogue (4 per TMEM lane quadrant).  Every mbarrier wait is bounded (2 s of
-// %globaltimer); a timeout sets the error word and the CTA still releases its
-// TMEM.
+// Warp roles: warps 0..15 produce the AO pieces of the 64-AO K blocks (4-AO
+// chunks claimed in order from a shared counter, lanes = points); warp 16
+// bulk-copies the blocks' records, TMA-loads the coefficient pieces and
+// publishes the count of blocks whose MMAs are done; warp 17 owns TMEM and
+// issues the MMAs; the 16 producer warps then run the epilogue (4 per TMEM
+// lane quadrant).  Every wait is bounded (2 s of %globaltimer); a timeout
+// sets the error word and the CTA still releases its TMEM.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
@@ -33,7 +34,7 @@ constexpr int kTmaWarp = kProdWarps;
 constexpr int kMmaWarp = kProdWarps + 1;
 constexpr int kThreadsF = (kProdWarps + 2) * 32;
 constexpr int STAGES = 2;
-constexpr int kKsteps = BK / UMMA_K;   // 16-AO k-steps per K block, 4 producer warps each
+constexpr int kKsteps = BK / UMMA_K;   // 16-AO k-steps per K block, 4 chunks each
 
 // Tile skipping: kskip (optional; layout in fused_common.cuh) lists, per K
 // block, the screening spheres of its shells.  A K block whose shells are
