@@ -190,6 +190,15 @@ qmckl_exit_code qmckl_b200_get_kblock_stats(qmckl_context context, int64_t* eval
  * evaluation of the context first (QMCKL_NOT_PROVIDED otherwise). */
 qmckl_exit_code qmckl_b200_inject_wait_failure(qmckl_context context, const int32_t code);
 
+/* The MO tiling of the fused mixed-form kernel for ao_num AOs, mo_num MOs and
+ * `pieces` (2 or 3) split pieces: tile width, tile count, FP32 accumulators
+ * per tile (3, or 2 for wide tiles) and pipeline stages (2 or 3), as the
+ * library chooses them (QMCKL_B200_WIDE_TILES included).  Host only: needs
+ * no device and no context. */
+qmckl_exit_code qmckl_b200_get_fused_plan(const int64_t ao_num, const int64_t mo_num, const int32_t pieces,
+                                          int32_t* n_tile, int32_t* n_tiles, int32_t* accumulators,
+                                          int32_t* stages);
+
 /* Test hook: in the fused mixed-form VGL kernel (3 pieces) launched after
  * this call, in this process, every producer warp holding a chunk of a
  * skipped 16-AO k-step sleeps `ns` nanoseconds (0 <= ns <= 1e7; 0 = off, the

@@ -1577,6 +1577,21 @@ qmckl_exit_code qmckl_b200_inject_wait_failure(qmckl_context context, const int3
   return QMCKL_SUCCESS;
 }
 
+qmckl_exit_code qmckl_b200_get_fused_plan(const int64_t ao_num, const int64_t mo_num, const int32_t pieces,
+                                          int32_t* n_tile, int32_t* n_tiles, int32_t* accumulators,
+                                          int32_t* stages) {
+  if (ao_num <= 0) return QMCKL_INVALID_ARG_1;
+  if (mo_num <= 0) return QMCKL_INVALID_ARG_2;
+  if (pieces != 2 && pieces != 3) return QMCKL_INVALID_ARG_3;
+  if (!n_tile || !n_tiles || !accumulators || !stages) return QMCKL_INVALID_ARG_4;
+  const TcPlan p = tc_plan_fused(ao_num, mo_num, pieces);
+  *n_tile = p.n_tile;
+  *n_tiles = p.n_tiles;
+  *accumulators = p.nacc;
+  *stages = p.nst;
+  return QMCKL_SUCCESS;
+}
+
 qmckl_exit_code qmckl_b200_inject_late_warps(const int64_t ns) {
   if (ns < 0 || ns > 10000000) return QMCKL_INVALID_ARG_1;
   return tc_set_late_warps((unsigned int)ns) == cudaSuccess ? QMCKL_SUCCESS : QMCKL_FAILURE;

@@ -500,6 +500,15 @@ def b200_inject_alloc_failure(n):
     lib().qmckl_b200_inject_alloc_failure(C.c_int64(n))
 
 
+def b200_get_fused_plan(ao_num, mo_num, pieces=3):
+    """(n_tile, n_tiles, accumulators, stages) of the fused kernel's MO tiling."""
+    v = [C.c_int32() for _ in range(4)]
+    f = lib().qmckl_b200_get_fused_plan
+    f.restype = C.c_int32
+    _check(f(C.c_int64(ao_num), C.c_int64(mo_num), C.c_int32(pieces), *[C.byref(x) for x in v]))
+    return tuple(x.value for x in v)
+
+
 def b200_inject_late_warps(ns):
     f = lib().qmckl_b200_inject_late_warps
     f.restype = C.c_int32
